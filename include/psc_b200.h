@@ -1,0 +1,207 @@
+/*
+ * psc_b200.h -- C ABI of libpscb200.so: the D3Q19 partially-saturated-cell
+ * immersed-boundary (PSC-IMB) lattice-Boltzmann step on one NVIDIA B200
+ * (sm_100a).
+ *
+ * The reference implementation is pure NumPy (src/lbm_dem/psc3d.py of
+ * wangjianfttt/particuology_Hydraulic-penalty-) and has no FFI of its own.
+ * These entry points are what a ctypes binding of that module's hot path
+ * needs; each cites the reference function it replaces.  The Python package
+ * particuology_hydraulic_penalty_b200 binds them with ctypes.
+ *
+ * Conventions
+ *  - Every function returns PSC_OK (0) or a negative PSC_E* code; the message
+ *    of the last failure on the calling thread is psc_last_error().
+ *  - All array pointers are DEVICE pointers unless the parameter name starts
+ *    with "h_".  The caller allocates every buffer; no entry point here
+ *    allocates device memory.  Sizes come from the *_bytes / plan queries.
+ *  - "stream" is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    Work is enqueued asynchronously; nothing synchronises unless stated.
+ *  - Lattice layout: structure of arrays, population plane i of a window is
+ *    f[i * N + (ix * ny + iy) * nz + iz], N = nx * ny * nz, iz contiguous --
+ *    the reference's f[i, ix, iy, iz] (psc3d.py:140) flattened.
+ *  - The velocity set, its index order and weights are those of
+ *    psc3d.py:17-43 (rest, +-x, +-y, +-z, then 12 diagonals in +- pairs).
+ *  - Stored populations are POST-COLLISION values (pull streaming): a step
+ *    reads f*_i(x - c_i), collides at x and writes f*_i(x).  The reference's
+ *    post-stream state is recovered by psc_stream_push().
+ *  - Handles are not thread-safe; distinct windows / buffers are independent.
+ */
+#ifndef PSC_B200_H
+#define PSC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSC_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+#define PSC_OK 0
+#define PSC_E_INVALID -1     /* bad argument (null pointer, size, mode) */
+#define PSC_E_CUDA -2        /* a CUDA runtime call failed */
+#define PSC_E_UNSUPPORTED -3 /* valid but not supported by this build/device */
+#define PSC_E_CAPACITY -4    /* a caller buffer is too small (see plan queries) */
+
+/* ---- storage / arithmetic modes of the populations ---------------------- */
+#define PSC_STORE_F64_EXACT 0 /* absolute f in FP64, reference operation order: bit-exact */
+#define PSC_STORE_F64 1       /* deviation f - w*rho0 in FP64, FMA arithmetic */
+#define PSC_STORE_F32 2       /* deviation in FP32, FP32 arithmetic */
+#define PSC_STORE_F16 3       /* deviation * store_scale in FP16, FP32 arithmetic */
+#define PSC_STORE_BF16 4      /* deviation * store_scale in BF16, FP32 arithmetic */
+
+/* ---- per-step flags ----------------------------------------------------- */
+#define PSC_STEP_COLLIDE 1u /* collide and write f_dst; without it: moments only */
+#define PSC_STEP_IMB 2u     /* write the node IMB momentum (psc3d.py:234-236) */
+#define PSC_STEP_MOMENTS 4u /* write rho, ux, uy, uz of the pulled state */
+#define PSC_STEP_REDUCE 8u  /* write per-tile FP64 reduction partials */
+#define PSC_STEP_MOVING 16u /* some window has PSC_WIN_MOVING: compile in the u_s path */
+
+/* ---- per-window flags --------------------------------------------------- */
+#define PSC_WIN_MOVING 1 /* read the solid velocity field us (else u_s = 0) */
+
+/* Reduction slots written per tile with PSC_STEP_REDUCE and summed per window
+ * by psc_reduce_windows().  Velocities are the stored-moment velocities
+ * u = (m + F/2) / rho of the PULLED state (psc3d.py:211-214 / 243-246). */
+#define PSC_RED_RHO 0
+#define PSC_RED_UX 1
+#define PSC_RED_UY 2
+#define PSC_RED_UZ 3
+#define PSC_RED_FLUID_UX 4 /* sum (1 - solid) * ux */
+#define PSC_RED_FLUID_UY 5
+#define PSC_RED_FLUID_UZ 6
+#define PSC_RED_FLUID 7 /* sum (1 - solid) */
+#define PSC_RED_IMBX 8  /* sum of this step's IMB momentum (collide only) */
+#define PSC_RED_IMBY 9
+#define PSC_RED_IMBZ 10
+#define PSC_RED_NONFINITE 11 /* number of cells with a non-finite moment */
+#define PSC_RED_SOLID 12     /* sum of the clipped solid fraction (solid_volume_lu) */
+#define PSC_NRED 13
+
+/* Diagnostics written by psc_particle_loads() (psc3d.py:247-253). */
+#define PSC_DIAG_MOMENTUM_RESIDUAL 0
+#define PSC_DIAG_MAX_FORCE 1
+#define PSC_DIAG_MAX_TORQUE 2
+#define PSC_DIAG_FORCE_SUM_X 3
+#define PSC_DIAG_FORCE_SUM_Y 4
+#define PSC_DIAG_FORCE_SUM_Z 5
+#define PSC_NDIAG 6
+
+/* One lattice window of a (batched) launch.  Lives in device memory; the
+ * array of windows handed to psc_step() is a device pointer.  All windows of
+ * one launch share the storage mode. */
+typedef struct psc_window {
+    int32_t nx, ny, nz;    /* lattice extent (the reference's n, n, n) */
+    int32_t subsamples;    /* S: solid fraction from S^3 samples per cell */
+    int32_t flags;         /* PSC_WIN_* */
+    int32_t tile_cells;    /* cells per tile (set by psc_plan_tiles) */
+    int64_t tile_begin;    /* first global tile index of this window */
+    int64_t tile_count;    /* number of tiles of this window */
+    double tau;            /* BGK relaxation time */
+    double force[3];       /* body force; the reference is (0, 0, body_force_z) */
+    double store_scale;    /* F16/BF16: stored = deviation * store_scale; else 1 */
+    const void* f_src;     /* populations read this step [19][N] */
+    void* f_dst;           /* populations written this step [19][N] */
+    const double* solid;   /* PSC_STORE_F64_EXACT: clipped solid fraction [N] */
+    const uint8_t* level;  /* other modes: clipped inside-sample count [N] */
+    const void* us;        /* solid velocity [3][N] (double in F64 modes, float otherwise) */
+    void* imb;             /* IMB momentum [3][N] (double in F64 modes, float otherwise) */
+    void* moments;         /* rho, ux, uy, uz [4][N] (same element type as imb) */
+    double* partials;      /* [tile_count][PSC_NRED] */
+} psc_window;
+
+/* Particle-derived geometry of ONE window (device arrays, caller-owned).
+ * Particles are [P][10] float64: x, y, z, r, vx, vy, vz, wx, wy, wz in
+ * lattice units -- the fields of the reference's Particle3D (psc3d.py:46-57). */
+typedef struct psc_geometry {
+    int32_t nx, ny, nz;
+    int32_t subsamples;
+    int32_t nparticles;
+    int32_t chunk_entries;    /* bbox entries per load-reduction chunk (power of 2) */
+    int64_t capacity_entries; /* length of ent_cnt / cl_pid / cl_cnt */
+    int64_t capacity_chunks;  /* rows of the chunk partial buffer of psc_particle_loads */
+    const double* particles;  /* [P][10] */
+    int32_t* bbox;            /* [P][6]: x0, y0, z0, ex, ey, ez (clipped box) */
+    int64_t* ent_off;         /* [P+1] bbox-entry offsets */
+    int64_t* chunk_off;       /* [P+1] load-chunk offsets */
+    int64_t* totals;          /* [4]: entries, chunks, max particles per cell, overflow flag */
+    uint16_t* ent_cnt;        /* [capacity_entries] inside-sample count per bbox entry */
+    int32_t* cell_n;          /* [N] scratch counter */
+    int32_t* cell_off;        /* [N+1] cell -> particle list offsets */
+    int32_t* cl_pid;          /* [capacity_entries] particle ids per cell, ascending */
+    uint16_t* cl_cnt;         /* [capacity_entries] their sample counts */
+    double* alpha_sum;        /* [N] unclipped alpha sum (psc3d.py:174 / 339-341) */
+    double* solid;            /* [N] clip(alpha_sum, 0, 1) (psc3d.py:175 / 344) */
+    uint8_t* level;           /* [N] min(sum of counts, S^3), or NULL; needs S^3 <= 255 */
+    void* scan_tmp;           /* scratch of psc_scan_tmp_bytes(N + 1) bytes */
+} psc_geometry;
+
+/* ---- library ------------------------------------------------------------ */
+int psc_abi_version(void);
+const char* psc_last_error(void);
+/* sizeof(psc_window) and sizeof(psc_geometry) as compiled into the library,
+ * so bindings can check their struct layout. */
+size_t psc_window_size(void);
+size_t psc_geometry_size(void);
+/* Bytes of scan scratch needed for n elements. */
+size_t psc_scan_tmp_bytes(int64_t n);
+
+/* ---- tiles and windows -------------------------------------------------- */
+/* Fill tile_cells / tile_begin / tile_count of h_windows (HOST array) and
+ * return the total tile count in *h_total_tiles. */
+int psc_plan_tiles(struct psc_window* h_windows, int nwin, int tile_cells, int64_t* h_total_tiles);
+
+/* Equilibrium at rho = 1, u = 0 in the given storage mode
+ * (the reference's initial state, psc3d.py:136-140). */
+int psc_init_equilibrium(int store, double store_scale, void* f, int64_t ncells, void* stream);
+
+/* ---- geometry (psc3d.py:60-94, 151-179, 328-345) ------------------------ */
+/* Clipped bounding boxes, entry and chunk offsets, totals.  The caller reads
+ * totals[0] (entries) and totals[1] (chunks) to size ent_cnt / cl_* and the
+ * load partials before psc_geometry_build. */
+int psc_geometry_plan(const psc_geometry* h_geo, void* stream);
+/* Inside-sample counts, per-cell particle lists (ascending id), alpha_sum,
+ * solid and level.  Bit-exact with the reference (no FMA contraction). */
+int psc_geometry_build(const psc_geometry* h_geo, void* stream);
+/* alpha-weighted rigid-body velocity u_s = sum_p alpha_p (V_p + w_p x r) /
+ * sum alpha (psc3d.py:181-206 / 347-373), written as [3][N] of us_type
+ * (0 = float64, 1 = float32). */
+int psc_solid_velocity(const psc_geometry* h_geo, int us_type, void* us, void* stream);
+
+/* ---- the step (psc3d.py:208-246) ---------------------------------------- */
+/* One pull-stream + collide pass over every tile of every window.
+ * d_windows: device array of nwin windows; total_tiles from psc_plan_tiles;
+ * grid_ctas = 0 picks a persistent grid (a multiple of the SM count). */
+int psc_step(int store, const struct psc_window* d_windows, int nwin, int64_t total_tiles,
+             unsigned flags, int grid_ctas, void* stream);
+/* Sum the per-tile partials of each window in a fixed order (deterministic)
+ * into out[nwin][PSC_NRED] (device). */
+int psc_reduce_windows(const struct psc_window* d_windows, int nwin, double* out, void* stream);
+
+/* ---- particle loads (psc3d.py:255-281 / 375-407) ------------------------ */
+/* Per-particle force and torque from the node IMB momentum imb [3][N]
+ * (imb_type 0 = float64, 1 = float32), owner weights alpha_p / alpha_sum.
+ * chunk_partials: [capacity_chunks][6] scratch.  imb_sums: device [3] sum of
+ * the node IMB momentum (PSC_RED_IMB* of the same step).  Writes forces
+ * [P][3], torques [P][3] and diag [PSC_NDIAG]. */
+int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb, double* chunk_partials,
+                       const double* imb_sums, double* forces, double* torques, double* diag, void* stream);
+
+/* ---- population layout conversions -------------------------------------- */
+/* dst_i(x + c_i) = src_i(x): turns the stored post-collision populations into
+ * the reference's post-stream f (psc3d.py:239-242); returns absolute FP64
+ * populations for every storage mode. */
+int psc_stream_push(int store, double store_scale, const void* src, double* dst, int nx, int ny, int nz,
+                    void* stream);
+/* Inverse: absolute FP64 post-stream f -> stored representation. */
+int psc_stream_pull_store(int store, double store_scale, const double* src, void* dst, int nx, int ny, int nz,
+                          void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSC_B200_H */

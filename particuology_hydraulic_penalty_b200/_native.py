@@ -1,0 +1,149 @@
+"""ctypes binding of libpscb200.so (the C ABI in ``include/psc_b200.h``).
+
+This is the only module that talks to the shared library.  It fails loudly:
+a missing or stale library raises ``NativeLibraryError``; every non-zero
+status from the library raises ``PscError`` with the library's message.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_size_t, c_uint, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libpscb200.so"
+HEADER_PATH = Path(__file__).resolve().parents[1] / "include" / "psc_b200.h"
+
+ABI_VERSION = 1
+
+# status codes
+PSC_OK = 0
+PSC_E_INVALID = -1
+PSC_E_CUDA = -2
+PSC_E_UNSUPPORTED = -3
+PSC_E_CAPACITY = -4
+
+# storage modes
+STORE_F64_EXACT = 0
+STORE_F64 = 1
+STORE_F32 = 2
+STORE_F16 = 3
+STORE_BF16 = 4
+
+# step flags
+STEP_COLLIDE = 1
+STEP_IMB = 2
+STEP_MOMENTS = 4
+STEP_REDUCE = 8
+STEP_MOVING = 16
+
+WIN_MOVING = 1
+
+# reduction slots
+RED_RHO, RED_UX, RED_UY, RED_UZ = 0, 1, 2, 3
+RED_FLUID_UX, RED_FLUID_UY, RED_FLUID_UZ, RED_FLUID = 4, 5, 6, 7
+RED_IMBX, RED_IMBY, RED_IMBZ = 8, 9, 10
+RED_NONFINITE = 11
+RED_SOLID = 12
+NRED = 13
+
+DIAG_MOMENTUM_RESIDUAL, DIAG_MAX_FORCE, DIAG_MAX_TORQUE = 0, 1, 2
+DIAG_FORCE_SUM = (3, 4, 5)
+NDIAG = 6
+
+STEP_THREADS = 256
+
+
+class NativeLibraryError(RuntimeError):
+    """libpscb200.so is missing, stale or not loadable."""
+
+
+class PscError(RuntimeError):
+    """A library call returned a non-zero status."""
+
+    def __init__(self, code: int, func: str, message: str):
+        super().__init__(f"{func} failed ({code}): {message}")
+        self.code = code
+
+
+class PscWindow(ctypes.Structure):
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32),
+        ("subsamples", c_int32), ("flags", c_int32), ("tile_cells", c_int32),
+        ("tile_begin", c_int64), ("tile_count", c_int64),
+        ("tau", c_double), ("force", c_double * 3), ("store_scale", c_double),
+        ("f_src", c_void_p), ("f_dst", c_void_p), ("solid", c_void_p), ("level", c_void_p),
+        ("us", c_void_p), ("imb", c_void_p), ("moments", c_void_p), ("partials", c_void_p),
+    ]
+
+
+class PscGeometry(ctypes.Structure):
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32),
+        ("subsamples", c_int32), ("nparticles", c_int32), ("chunk_entries", c_int32),
+        ("capacity_entries", c_int64), ("capacity_chunks", c_int64),
+        ("particles", c_void_p), ("bbox", c_void_p), ("ent_off", c_void_p), ("chunk_off", c_void_p),
+        ("totals", c_void_p), ("ent_cnt", c_void_p), ("cell_n", c_void_p), ("cell_off", c_void_p),
+        ("cl_pid", c_void_p), ("cl_cnt", c_void_p), ("alpha_sum", c_void_p), ("solid", c_void_p),
+        ("level", c_void_p), ("scan_tmp", c_void_p),
+    ]
+
+
+# name -> (restype, argtypes); every function of include/psc_b200.h
+SIGNATURES = {
+    "psc_abi_version": (c_int, []),
+    "psc_last_error": (ctypes.c_char_p, []),
+    "psc_window_size": (c_size_t, []),
+    "psc_geometry_size": (c_size_t, []),
+    "psc_scan_tmp_bytes": (c_size_t, [c_int64]),
+    "psc_plan_tiles": (c_int, [POINTER(PscWindow), c_int, c_int, POINTER(c_int64)]),
+    "psc_init_equilibrium": (c_int, [c_int, c_double, c_void_p, c_int64, c_void_p]),
+    "psc_geometry_plan": (c_int, [POINTER(PscGeometry), c_void_p]),
+    "psc_geometry_build": (c_int, [POINTER(PscGeometry), c_void_p]),
+    "psc_solid_velocity": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p]),
+    "psc_step": (c_int, [c_int, c_void_p, c_int, c_int64, c_uint, c_int, c_void_p]),
+    "psc_reduce_windows": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "psc_particle_loads": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                   c_void_p, c_void_p, c_void_p]),
+    "psc_stream_push": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "psc_stream_pull_store": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
+}
+
+_lib = None
+
+
+def load(path: Path | None = None) -> ctypes.CDLL:
+    """Load (once) and type the shared library; raise if it is absent or stale."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise NativeLibraryError(
+            f"{p} not found: build it with `python -m particuology_hydraulic_penalty_b200.build`")
+    try:
+        lib = ctypes.CDLL(str(p))
+    except OSError as exc:  # pragma: no cover - depends on the host
+        raise NativeLibraryError(f"cannot load {p}: {exc}") from exc
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.psc_abi_version() != ABI_VERSION:
+        raise NativeLibraryError("libpscb200.so ABI version mismatch: rebuild the library")
+    if lib.psc_window_size() != ctypes.sizeof(PscWindow) or lib.psc_geometry_size() != ctypes.sizeof(PscGeometry):
+        raise NativeLibraryError("libpscb200.so struct layout mismatch: rebuild the library")
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(status: int, func: str) -> None:
+    if status != PSC_OK:
+        msg = load().psc_last_error()
+        raise PscError(status, func, msg.decode() if msg else "")
+
+
+def call(name: str, *args) -> None:
+    """Call a status-returning entry point and raise on failure."""
+    check(getattr(load(), name)(*args), name)

@@ -1,0 +1,188 @@
+// extern "C" entry points of libpscb200.so (declared in include/psc_b200.h).
+//
+// Every entry point validates its arguments on the host, enqueues work on the
+// caller's stream and returns a status code; no exception crosses the ABI and
+// nothing here allocates device memory.
+#include <cstdio>
+#include <string>
+
+#include "internal.cuh"
+
+namespace psc {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+    set_error(msg);
+    return code;
+}
+
+int cuda_fail(cudaError_t err, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(err) + " (" + cudaGetErrorString(err) + ")";
+    return fail(PSC_E_CUDA, m);
+}
+
+int sm_count() {
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    int& c = cache[dev & 63];
+    if (c == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        c = v;
+    }
+    return c;
+}
+
+static bool valid_store(int s) { return s >= PSC_STORE_F64_EXACT && s <= PSC_STORE_BF16; }
+
+static int check_extent(int nx, int ny, int nz, const char* who) {
+    if (nx <= 0 || ny <= 0 || nz <= 0) return fail(PSC_E_INVALID, std::string(who) + ": lattice extents must be > 0");
+    const long long n = (long long)nx * ny * nz;
+    if (n >= (1ll << 31)) return fail(PSC_E_UNSUPPORTED, std::string(who) + ": a window must have < 2^31 cells");
+    return PSC_OK;
+}
+
+static int check_geometry(const psc_geometry* g, const char* who) {
+    if (!g) return fail(PSC_E_INVALID, std::string(who) + ": null geometry");
+    int st = check_extent(g->nx, g->ny, g->nz, who);
+    if (st) return st;
+    if (g->subsamples < 1 || g->subsamples > 16)
+        return fail(PSC_E_INVALID, std::string(who) + ": subsamples must be in [1, 16]");
+    if (g->nparticles < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
+    if (g->chunk_entries <= 0) return fail(PSC_E_INVALID, std::string(who) + ": chunk_entries must be > 0");
+    if (g->capacity_entries < 0 || g->capacity_chunks < 0 || g->capacity_entries >= (1ll << 31))
+        return fail(PSC_E_INVALID, std::string(who) + ": capacities must be in [0, 2^31)");
+    if (g->nparticles > 0 && (!g->particles || !g->bbox))
+        return fail(PSC_E_INVALID, std::string(who) + ": null particle or bbox array");
+    if (!g->ent_off || !g->chunk_off || !g->totals)
+        return fail(PSC_E_INVALID, std::string(who) + ": null offsets/totals array");
+    return PSC_OK;
+}
+
+}  // namespace psc
+
+using namespace psc;
+
+extern "C" {
+
+int psc_abi_version(void) { return PSC_ABI_VERSION; }
+
+const char* psc_last_error(void) { return g_last_error.c_str(); }
+
+size_t psc_window_size(void) { return sizeof(psc_window); }
+
+size_t psc_geometry_size(void) { return sizeof(psc_geometry); }
+
+size_t psc_scan_tmp_bytes(int64_t n) { return scan_tmp_bytes(n < 0 ? 0 : n); }
+
+int psc_plan_tiles(psc_window* h_windows, int nwin, int tile_cells, int64_t* h_total_tiles) {
+    if (!h_windows || nwin <= 0 || !h_total_tiles) return fail(PSC_E_INVALID, "psc_plan_tiles: bad arguments");
+    if (tile_cells == 0) tile_cells = STEP_THREADS;
+    if (tile_cells != STEP_THREADS)
+        return fail(PSC_E_UNSUPPORTED, "psc_plan_tiles: tile_cells must be 0 or " + std::to_string(STEP_THREADS));
+    int64_t begin = 0;
+    for (int w = 0; w < nwin; ++w) {
+        psc_window& W = h_windows[w];
+        int st = check_extent(W.nx, W.ny, W.nz, "psc_plan_tiles");
+        if (st) return st;
+        const int64_t n = (int64_t)W.nx * W.ny * W.nz;
+        W.tile_cells = tile_cells;
+        W.tile_begin = begin;
+        W.tile_count = (n + tile_cells - 1) / tile_cells;
+        begin += W.tile_count;
+    }
+    *h_total_tiles = begin;
+    return PSC_OK;
+}
+
+int psc_init_equilibrium(int store, double store_scale, void* f, int64_t ncells, void* stream) {
+    if (!valid_store(store)) return fail(PSC_E_INVALID, "psc_init_equilibrium: unknown storage mode");
+    if (!f || ncells <= 0) return fail(PSC_E_INVALID, "psc_init_equilibrium: null buffer or empty lattice");
+    cudaError_t e = launch_init_equilibrium(store, store_scale, f, ncells, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_init_equilibrium");
+}
+
+int psc_geometry_plan(const psc_geometry* h_geo, void* stream) {
+    int st = check_geometry(h_geo, "psc_geometry_plan");
+    if (st) return st;
+    cudaError_t e = launch_geometry_plan(*h_geo, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_geometry_plan");
+}
+
+int psc_geometry_build(const psc_geometry* h_geo, void* stream) {
+    int st = check_geometry(h_geo, "psc_geometry_build");
+    if (st) return st;
+    const psc_geometry& g = *h_geo;
+    if (!g.cell_n || !g.cell_off || !g.alpha_sum || !g.solid || !g.scan_tmp)
+        return fail(PSC_E_INVALID, "psc_geometry_build: null cell array");
+    if (g.capacity_entries > 0 && (!g.ent_cnt || !g.cl_pid || !g.cl_cnt))
+        return fail(PSC_E_INVALID, "psc_geometry_build: null entry array");
+    if (g.level && g.subsamples * g.subsamples * g.subsamples > 255)
+        return fail(PSC_E_UNSUPPORTED, "psc_geometry_build: the uint8 level field needs subsamples <= 6");
+    cudaError_t e = launch_geometry_build(g, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_geometry_build");
+}
+
+int psc_solid_velocity(const psc_geometry* h_geo, int us_type, void* us, void* stream) {
+    int st = check_geometry(h_geo, "psc_solid_velocity");
+    if (st) return st;
+    if (!us || (us_type != 0 && us_type != 1)) return fail(PSC_E_INVALID, "psc_solid_velocity: bad output");
+    cudaError_t e = launch_solid_velocity(*h_geo, us_type, us, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_solid_velocity");
+}
+
+int psc_step(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags, int grid_ctas,
+             void* stream) {
+    if (!valid_store(store)) return fail(PSC_E_INVALID, "psc_step: unknown storage mode");
+    if (!d_windows || nwin <= 0 || total_tiles < 0) return fail(PSC_E_INVALID, "psc_step: bad window list");
+    if (grid_ctas < 0) return fail(PSC_E_INVALID, "psc_step: grid_ctas must be >= 0");
+    cudaError_t e = launch_step(store, d_windows, nwin, total_tiles, flags, (flags & PSC_STEP_MOVING) != 0,
+                                grid_ctas, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_step");
+}
+
+int psc_reduce_windows(const psc_window* d_windows, int nwin, double* out, void* stream) {
+    if (!d_windows || nwin <= 0 || !out) return fail(PSC_E_INVALID, "psc_reduce_windows: bad arguments");
+    cudaError_t e = launch_reduce_windows(d_windows, nwin, out, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_reduce_windows");
+}
+
+int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb, double* chunk_partials,
+                       const double* imb_sums, double* forces, double* torques, double* diag, void* stream) {
+    int st = check_geometry(h_geo, "psc_particle_loads");
+    if (st) return st;
+    if (imb_type != 0 && imb_type != 1) return fail(PSC_E_INVALID, "psc_particle_loads: imb_type must be 0 or 1");
+    if (!imb_sums || !diag) return fail(PSC_E_INVALID, "psc_particle_loads: null imb_sums / diag");
+    if (h_geo->nparticles > 0 && (!imb || !forces || !torques || !h_geo->ent_cnt || !h_geo->alpha_sum))
+        return fail(PSC_E_INVALID, "psc_particle_loads: null array");
+    if (h_geo->nparticles > 0 && h_geo->capacity_chunks > 0 && !chunk_partials)
+        return fail(PSC_E_INVALID, "psc_particle_loads: null chunk partials");
+    cudaError_t e = launch_particle_loads(*h_geo, imb_type, imb, chunk_partials, imb_sums, forces, torques, diag,
+                                          as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_particle_loads");
+}
+
+int psc_stream_push(int store, double store_scale, const void* src, double* dst, int nx, int ny, int nz,
+                    void* stream) {
+    if (!valid_store(store) || !src || !dst) return fail(PSC_E_INVALID, "psc_stream_push: bad arguments");
+    int st = check_extent(nx, ny, nz, "psc_stream_push");
+    if (st) return st;
+    if (store_scale == 0.0) return fail(PSC_E_INVALID, "psc_stream_push: zero store_scale");
+    cudaError_t e = launch_stream_push(store, store_scale, src, dst, nx, ny, nz, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_stream_push");
+}
+
+int psc_stream_pull_store(int store, double store_scale, const double* src, void* dst, int nx, int ny, int nz,
+                          void* stream) {
+    if (!valid_store(store) || !src || !dst) return fail(PSC_E_INVALID, "psc_stream_pull_store: bad arguments");
+    int st = check_extent(nx, ny, nz, "psc_stream_pull_store");
+    if (st) return st;
+    cudaError_t e = launch_stream_pull_store(store, store_scale, src, dst, nx, ny, nz, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_stream_pull_store");
+}
+
+}  // extern "C"

@@ -1,0 +1,236 @@
+// Per-node PSC-IMB collision: moments, Noble-Torczynski solid weighting, Guo
+// forcing and the node IMB momentum.  Host+device so that the exact variant
+// can be unit-tested on a CPU against the NumPy oracle.
+//
+// Two formulations of the same step (src/lbm_dem/psc3d.py:211-236):
+//  * exact   -- absolute FP64 populations, every rounding in the reference's
+//               order (NumPy evaluates one IEEE operation per ufunc call),
+//               no FMA: bit-identical to the reference.
+//  * fast<R> -- populations stored as deviations g_i = f_i - w_i (rho0 = 1),
+//               arithmetic in R (double or float) with FMAs and reciprocal
+//               multiplies.  The rest-weight offsets cancel in every
+//               difference the step takes, so small deviations keep full
+//               relative precision.
+//
+// Reference quirks reproduced by both (they are the method as published):
+//  * moment velocity u = (m + F/2) / rho, and the collision uses a second
+//    shift u_eff = u + F/(2 rho) = (m + F) / rho          (psc3d.py:214, 219)
+//  * Guo forcing added at every node, not weighted by 1 - B  (psc3d.py:230-232)
+//  * B = alpha / (alpha + tau (1 - alpha) + 1e-14)          (psc3d.py:229)
+#pragma once
+
+#include "d3q19.cuh"
+
+namespace psc {
+
+// ===========================================================================
+// exact FP64
+// ===========================================================================
+struct ExactMoments {
+    double rho, ux, uy, uz;
+};
+
+// rho and u = (m + F/2)/rho of absolute populations f, psc3d.py:211-214.
+PSC_HD ExactMoments moments_exact(const double* f, double hfx, double hfy, double hfz) {
+    ExactMoments m;
+    double rho = f[0];
+#pragma unroll
+    for (int i = 1; i < Q; ++i) rho = xadd(rho, f[i]);
+    m.rho = rho;
+    m.ux = xdiv(xadd(seq_moment_exact<0>(f), hfx), rho);
+    m.uy = xdiv(xadd(seq_moment_exact<1>(f), hfy), rho);
+    m.uz = xdiv(xadd(seq_moment_exact<2>(f), hfz), rho);
+    return m;
+}
+
+PSC_HD double cm(int c, double x) { return c == 0 ? 0.0 : (c > 0 ? x : -x); }
+
+// Collide f in place.  solid: clipped solid fraction.  moving: use (usx, usy,
+// usz), else the solid velocity is zero.  imb receives sum_i c_i B Omega_s,i in
+// the reference's sequential order (psc3d.py:234-236).
+PSC_HD void collide_exact(double* f, const ExactMoments& mo, double solid, bool moving, double usx, double usy,
+                          double usz, double tau, double fx, double fy, double fz, double hfx, double hfy,
+                          double hfz, double* imb) {
+    const double rho = mo.rho;
+    // u_eff = u + 0.5 F / rho   (psc3d.py:217-219)
+    const double uex = xadd(mo.ux, xdiv(hfx, rho));
+    const double uey = xadd(mo.uy, xdiv(hfy, rho));
+    const double uez = xadd(mo.uz, xdiv(hfz, rho));
+    // equilibrium pieces shared by all directions (psc3d.py:98, :102)
+    const double uu = xadd(xadd(xmul(uex, uex), xmul(uey, uey)), xmul(uez, uez));
+    const double ct = xdiv(xmul(0.5, uu), CS2);
+    double uus = 0.0, cts = 0.0;
+    if (moving) {
+        uus = xadd(xadd(xmul(usx, usx), xmul(usy, usy)), xmul(usz, usz));
+        cts = xdiv(xmul(0.5, uus), CS2);
+    }
+    // B (psc3d.py:228-229)
+    const double al = solid < 0.0 ? 0.0 : (solid > 1.0 ? 1.0 : solid);
+    const double B = xdiv(al, xadd(xadd(al, xmul(tau, xsub(1.0, al))), 1.0e-14));
+    const double omB = xsub(1.0, B);
+    // Guo prefactor and u.F (psc3d.py:108-109)
+    const double pref = xsub(1.0, xdiv(0.5, tau));
+    const double uf = xadd(xadd(xmul(uex, fx), xmul(uey, fy)), xmul(uez, fz));
+
+    double ix = 0.0, iy = 0.0, iz = 0.0;  // imb accumulators, index order from +0
+
+    // rest population: cu = 0, cf = 0
+    {
+        const double wr = xmul(W0, rho);
+        const double feqf = xmul(wr, xsub(1.0, ct));
+        const double feqs = moving ? xmul(wr, xsub(1.0, cts)) : wr;
+        const double f0 = f[0];
+        const double os = xsub(feqs, feqf);  // (f0 - f0) + feqs - feqf
+        const double obgk = -xdiv(xsub(f0, feqf), tau);
+        const double coll = xadd(xmul(omB, obgk), xmul(B, os));
+        const double g = xmul(xmul(pref, W0), xdiv(-uf, CS2));
+        f[0] = xadd(f0, xadd(coll, g));
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const int i = 2 * k + 1, j = i + 1;  // c_j = -c_i
+        const double w = wgt(i);
+        const double wr = xmul(w, rho);
+        // feq with u_eff: cu_j = -cu_i exactly, so q_j = -q_i and b_j = b_i
+        const double cu = xadd(xadd(cm(cxv(i), uex), cm(cyv(i), uey)), cm(czv(i), uez));
+        const double q = xdiv(cu, CS2);
+        const double b = xdiv(xmul(xmul(0.5, cu), cu), CS2SQ);
+        const double feqf_i = xmul(wr, xsub(xadd(xadd(1.0, q), b), ct));
+        const double feqf_j = xmul(wr, xsub(xadd(xadd(1.0, -q), b), ct));
+        double feqs_i = wr, feqs_j = wr;  // u_s = 0: feq = w rho exactly
+        if (moving) {
+            const double cus = xadd(xadd(cm(cxv(i), usx), cm(cyv(i), usy)), cm(czv(i), usz));
+            const double qs = xdiv(cus, CS2);
+            const double bs = xdiv(xmul(xmul(0.5, cus), cus), CS2SQ);
+            feqs_i = xmul(wr, xsub(xadd(xadd(1.0, qs), bs), cts));
+            feqs_j = xmul(wr, xsub(xadd(xadd(1.0, -qs), bs), cts));
+        }
+        const double fi = f[i], fj = f[j];
+        // Omega_s = f_opp - f + feq_s - feq_f[opp]   (psc3d.py:223-226)
+        const double os_i = xsub(xadd(xsub(fj, fi), feqs_i), feqf_j);
+        const double os_j = xsub(xadd(xsub(fi, fj), feqs_j), feqf_i);
+        // Omega_bgk = -(f - feq_f) / tau   (psc3d.py:221)
+        const double ob_i = -xdiv(xsub(fi, feqf_i), tau);
+        const double ob_j = -xdiv(xsub(fj, feqf_j), tau);
+        const double coll_i = xadd(xmul(omB, ob_i), xmul(B, os_i));
+        const double coll_j = xadd(xmul(omB, ob_j), xmul(B, os_j));
+        // Guo: pref W ((cf - uf)/cs2 + cu cf / cs2^2), cf_j = -cf_i   (psc3d.py:110-113)
+        const double cf = xadd(xadd(cm(cxv(i), fx), cm(cyv(i), fy)), cm(czv(i), fz));
+        const double pw = xmul(pref, w);
+        const double t2 = xdiv(xmul(cu, cf), CS2SQ);
+        const double g_i = xmul(pw, xadd(xdiv(xsub(cf, uf), CS2), t2));
+        const double g_j = xmul(pw, xadd(xdiv(xsub(-cf, uf), CS2), t2));
+        f[i] = xadd(fi, xadd(coll_i, g_i));
+        f[j] = xadd(fj, xadd(coll_j, g_j));
+        // node IMB momentum, sequential in index order (i then j)
+        const double bo_i = xmul(B, os_i), bo_j = xmul(B, os_j);
+        ix = cxv(i) > 0 ? xadd(ix, bo_i) : (cxv(i) < 0 ? xsub(ix, bo_i) : ix);
+        ix = cxv(j) > 0 ? xadd(ix, bo_j) : (cxv(j) < 0 ? xsub(ix, bo_j) : ix);
+        iy = cyv(i) > 0 ? xadd(iy, bo_i) : (cyv(i) < 0 ? xsub(iy, bo_i) : iy);
+        iy = cyv(j) > 0 ? xadd(iy, bo_j) : (cyv(j) < 0 ? xsub(iy, bo_j) : iy);
+        iz = czv(i) > 0 ? xadd(iz, bo_i) : (czv(i) < 0 ? xsub(iz, bo_i) : iz);
+        iz = czv(j) > 0 ? xadd(iz, bo_j) : (czv(j) < 0 ? xsub(iz, bo_j) : iz);
+    }
+    imb[0] = ix;
+    imb[1] = iy;
+    imb[2] = iz;
+}
+
+// ===========================================================================
+// fast deviation form, arithmetic type R
+// ===========================================================================
+template <typename R>
+struct FastMoments {
+    R drho, rho, mx, my, mz;
+};
+
+template <typename R>
+PSC_HD FastMoments<R> moments_fast(const R* g) {
+    FastMoments<R> m;
+    m.drho = (((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7]))) +
+             (((g[8] + g[9]) + (g[10] + g[11])) + ((g[12] + g[13]) + (g[14] + g[15]))) + ((g[16] + g[17]) + g[18]);
+    m.rho = R(1) + m.drho;
+    m.mx = ((g[1] - g[2]) + (g[7] - g[8])) + ((g[9] - g[10]) + (g[11] - g[12])) + (g[13] - g[14]);
+    m.my = ((g[3] - g[4]) + (g[7] - g[8])) + ((g[10] - g[9]) + (g[15] - g[16])) + (g[17] - g[18]);
+    m.mz = ((g[5] - g[6]) + (g[11] - g[12])) + ((g[14] - g[13]) + (g[15] - g[16])) + (g[18] - g[17]);
+    return m;
+}
+
+template <typename R>
+struct FastParams {
+    R inv_tau, pref, fx, fy, fz;
+};
+
+// c * x for a lattice component c in {-1, 0, 1} (folded once loops unroll).
+template <typename R>
+PSC_HD R csel(int c, R x) {
+    return c == 0 ? R(0) : (c > 0 ? x : -x);
+}
+
+// Collide deviations g in place; irho = 1 / rho; B solid weight.  imb gets
+// sum_i c_i B Omega_s,i.  Returns nothing else: the caller owns the moments.
+template <typename R, bool MOVING, bool IMB>
+PSC_HD void collide_fast(R* g, const FastMoments<R>& mo, R irho, R B, R usx, R usy, R usz,
+                         const FastParams<R>& p, R* imb) {
+    const R rho = mo.rho, drho = mo.drho;
+    const R uex = (mo.mx + p.fx) * irho;
+    const R uey = (mo.my + p.fy) * irho;
+    const R uez = (mo.mz + p.fz) * irho;
+    const R uu = uex * uex + uey * uey + uez * uez;
+    const R uf = uex * p.fx + uey * p.fy + uez * p.fz;
+    const R omB = R(1) - B;
+    const R kb = omB * p.inv_tau;  // (1 - B) / tau
+    R uus = R(0);
+    if (MOVING) uus = usx * usx + usy * usy + usz * usz;
+    const R r15 = R(1.5) * rho;
+    R ax = R(0), ay = R(0), az = R(0);
+    {
+        const R geq = R(W0) * (drho - r15 * uu);
+        const R os = R(W0) * r15 * (uu - uus);
+        const R G = R(-3) * p.pref * R(W0) * uf;
+        g[0] = g[0] - kb * (g[0] - geq) + B * os + G;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const int i = 2 * k + 1, j = i + 1;
+        const R w = R(wgt(i));
+        const R cu = csel(cxv(i), uex) + csel(cyv(i), uey) + csel(czv(i), uez);
+        const R cF = csel(cxv(i), p.fx) + csel(cyv(i), p.fy) + csel(czv(i), p.fz);
+        const R sym = w * (drho + rho * (R(4.5) * cu * cu - R(1.5) * uu));
+        const R asym = R(3) * w * rho * cu;
+        R ssym, sasym;
+        if (MOVING) {
+            const R cus = csel(cxv(i), usx) + csel(cyv(i), usy) + csel(czv(i), usz);
+            ssym = w * (drho + rho * (R(4.5) * cus * cus - R(1.5) * uus));
+            sasym = R(3) * w * rho * cus;
+        } else {
+            ssym = w * drho;
+            sasym = R(0);
+        }
+        const R gi = g[i], gj = g[j];
+        const R d = gj - gi;
+        const R e = ssym - sym;
+        const R h = sasym + asym;
+        const R os_i = d + e + h;
+        const R os_j = e - d - h;
+        const R pw = p.pref * w;
+        const R t9 = R(9) * cu * cF;
+        const R G_i = pw * (R(3) * (cF - uf) + t9);
+        const R G_j = pw * (R(3) * (-cF - uf) + t9);
+        g[i] = gi - kb * (gi - (sym + asym)) + B * os_i + G_i;
+        g[j] = gj - kb * (gj - (sym - asym)) + B * os_j + G_j;
+        if (IMB) {
+            const R dm = B * (os_i - os_j);  // c_i B os_i + c_j B os_j = c_i B (os_i - os_j)
+            ax += csel(cxv(i), dm);
+            ay += csel(cyv(i), dm);
+            az += csel(czv(i), dm);
+        }
+    }
+    if (IMB) {
+        imb[0] = ax;
+        imb[1] = ay;
+        imb[2] = az;
+    }
+}
+
+}  // namespace psc

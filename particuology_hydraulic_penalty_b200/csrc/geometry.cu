@@ -1,0 +1,545 @@
+// Particle geometry on the GPU: sub-sampled solid fraction (K1), solid
+// velocity, and per-particle IMB force / torque (K3).
+//
+// Reference: src/lbm_dem/psc3d.py
+//   bbox + S^3 inside count      :60-94 (sparse task), :151-173 (dense)
+//   alpha sum / solid             :174-175, :339-344
+//   solid velocity                :181-206, :347-373
+//   particle loads                :255-281, :375-407
+//
+// Data flow (all device-resident, no host round trip except the entry total
+// that sizes the caller's buffers):
+//   plan     one block: clipped bbox per particle, entry offsets (sum of bbox
+//            volumes) and load-chunk offsets by block scans
+//   count    one thread per (particle, bbox cell): S^3 inside tests in FP64
+//            with the reference's rounding (no FMA) -> uint16 count; bump the
+//            per-cell particle counter
+//   scan     counters -> per-cell list offsets
+//   fill     scatter (particle, count) into the cell lists
+//   final    per cell: sort its list by particle id, sum alpha = count / S^3 in
+//            that order from 0.0 (bit-identical to NumPy's sequential sums),
+//            clip to the solid fraction, clipped integer level
+//   loads    chunks of bbox entries per particle, deterministic block sums,
+//            then a fixed-order per-particle sum of the chunk partials
+#include "collide.cuh"
+#include "internal.cuh"
+
+namespace psc {
+
+constexpr int PF = 10;  // particle fields: x y z r vx vy vz wx wy wz
+
+// Clipped [lo, hi) box per axis: lo = max(0, floor(c - r - 1)),
+// hi = min(n, ceil(c + r + 1))  (psc3d.py:73-78).
+__device__ __forceinline__ void axis_box(double c, double r, int n, int32_t& lo, int32_t& ext) {
+    double a = floor(xsub(xsub(c, r), 1.0));
+    double b = ceil(xadd(xadd(c, r), 1.0));
+    if (!(a > 0.0)) a = 0.0;  // also maps NaN to 0 (rejected on the host)
+    if (!(b < (double)n)) b = (double)n;
+    if (a > (double)n) a = (double)n;
+    if (b < 0.0) b = 0.0;
+    lo = (int32_t)a;
+    const int32_t hi = (int32_t)b;
+    ext = hi > lo ? hi - lo : 0;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    T x = v;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, x, s);
+        if (lane >= s) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < nw ? s_warp[lane] : T(0);
+#pragma unroll
+        for (int s = 1; s < 32; s <<= 1) {
+            const T y = __shfl_up_sync(0xffffffffu, w, s);
+            if (lane >= s) w += y;
+        }
+        if (lane < nw) s_warp[lane] = w;
+    }
+    __syncthreads();
+    const T warp_prefix = warp > 0 ? s_warp[warp - 1] : T(0);
+    total = s_warp[nw - 1];
+    __syncthreads();
+    return warp_prefix + x - v;
+}
+
+// One block: boxes, entry offsets, chunk offsets, totals.
+__global__ void __launch_bounds__(1024) k_geometry_plan(psc_geometry g) {
+    __shared__ int64_t s_warp[32];
+    __shared__ int64_t s_carry[2];
+    const int P = g.nparticles;
+    if (threadIdx.x == 0) {
+        s_carry[0] = 0;
+        s_carry[1] = 0;
+    }
+    __syncthreads();
+    const int64_t ch = g.chunk_entries;
+    for (int base = 0; base < P; base += blockDim.x) {
+        const int p = base + threadIdx.x;
+        int64_t vol = 0;
+        if (p < P) {
+            const double* q = g.particles + (size_t)p * PF;
+            int32_t lo[3], ex[3];
+            axis_box(q[0], q[3], g.nx, lo[0], ex[0]);
+            axis_box(q[1], q[3], g.ny, lo[1], ex[1]);
+            axis_box(q[2], q[3], g.nz, lo[2], ex[2]);
+            int32_t* bb = g.bbox + (size_t)p * 6;
+            bb[0] = lo[0];
+            bb[1] = lo[1];
+            bb[2] = lo[2];
+            bb[3] = ex[0];
+            bb[4] = ex[1];
+            bb[5] = ex[2];
+            vol = (int64_t)ex[0] * ex[1] * ex[2];
+        }
+        const int64_t nch = (vol + ch - 1) / ch;
+        int64_t tot_e, tot_c;
+        const int64_t pe = block_exclusive_scan<int64_t>(vol, s_warp, tot_e);
+        const int64_t pc = block_exclusive_scan<int64_t>(nch, s_warp, tot_c);
+        if (p < P) {
+            g.ent_off[p] = s_carry[0] + pe;
+            g.chunk_off[p] = s_carry[1] + pc;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_carry[0] += tot_e;
+            s_carry[1] += tot_c;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        g.ent_off[P] = s_carry[0];
+        g.chunk_off[P] = s_carry[1];
+        g.totals[0] = s_carry[0];
+        g.totals[1] = s_carry[1];
+        g.totals[2] = 0;
+        g.totals[3] = (s_carry[0] > g.capacity_entries || s_carry[1] > g.capacity_chunks) ? 1 : 0;
+    }
+}
+
+// Largest p with off[p] <= e (off has P+1 non-decreasing entries, off[0] = 0).
+__device__ __forceinline__ int owner_of(const int64_t* off, int P, int64_t e) {
+    int lo = 0, hi = P - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= e) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct EntryCell {
+    int p;
+    int32_t ix, iy, iz;
+    uint32_t cell;
+};
+
+__device__ __forceinline__ EntryCell decode_entry(const psc_geometry& g, int64_t e) {
+    EntryCell c;
+    c.p = owner_of(g.ent_off, g.nparticles, e);
+    const int32_t* bb = g.bbox + (size_t)c.p * 6;
+    const int64_t local = e - g.ent_off[c.p];
+    const int64_t eyz = (int64_t)bb[4] * bb[5];
+    const int32_t a = (int32_t)(local / eyz);
+    const int64_t rem = local - (int64_t)a * eyz;
+    const int32_t b = (int32_t)(rem / bb[5]);
+    const int32_t k = (int32_t)(rem - (int64_t)b * bb[5]);
+    c.ix = bb[0] + a;
+    c.iy = bb[1] + b;
+    c.iz = bb[2] + k;
+    c.cell = ((uint32_t)c.ix * (uint32_t)g.ny + (uint32_t)c.iy) * (uint32_t)g.nz + (uint32_t)c.iz;
+    return c;
+}
+
+// Inside-sample count of one cell: offsets (k + 0.5)/S, d = (i + o) - c,
+// (dx*dx + dy*dy) + dz*dz <= r*r, every operation rounded once
+// (psc3d.py:72, :86-89).
+__device__ __forceinline__ int sample_count(int32_t ix, int32_t iy, int32_t iz, double px, double py, double pz,
+                                            double rr, int S) {
+    const double Sd = (double)S;
+    int cnt = 0;
+    for (int a = 0; a < S; ++a) {
+        const double dx = xsub(xadd((double)ix, xdiv((double)a + 0.5, Sd)), px);
+        const double dx2 = xmul(dx, dx);
+        for (int b = 0; b < S; ++b) {
+            const double dy = xsub(xadd((double)iy, xdiv((double)b + 0.5, Sd)), py);
+            const double dxy = xadd(dx2, xmul(dy, dy));
+            for (int c = 0; c < S; ++c) {
+                const double dz = xsub(xadd((double)iz, xdiv((double)c + 0.5, Sd)), pz);
+                cnt += xadd(dxy, xmul(dz, dz)) <= rr ? 1 : 0;
+            }
+        }
+    }
+    return cnt;
+}
+
+__global__ void k_geometry_count(psc_geometry g) {
+    const int64_t E = min(g.totals[0], g.capacity_entries);
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        const EntryCell c = decode_entry(g, e);
+        const double* q = g.particles + (size_t)c.p * PF;
+        const int cnt = sample_count(c.ix, c.iy, c.iz, q[0], q[1], q[2], xmul(q[3], q[3]), g.subsamples);
+        g.ent_cnt[e] = (uint16_t)cnt;
+        if (cnt > 0) atomicAdd(g.cell_n + c.cell, 1);
+    }
+}
+
+__global__ void k_geometry_fill(psc_geometry g) {
+    const int64_t E = min(g.totals[0], g.capacity_entries);
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        const uint16_t cnt = g.ent_cnt[e];
+        if (cnt == 0) continue;
+        const EntryCell c = decode_entry(g, e);
+        const int32_t pos = atomicAdd(g.cell_n + c.cell, 1);
+        const int64_t idx = (int64_t)g.cell_off[c.cell] + pos;
+        if (idx < g.capacity_entries) {
+            g.cl_pid[idx] = c.p;
+            g.cl_cnt[idx] = cnt;
+        }
+    }
+}
+
+__global__ void k_geometry_final(psc_geometry g) {
+    const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
+    const int S = g.subsamples;
+    const int S3 = S * S * S;
+    const double S3d = (double)S3;
+    int local_max = 0;
+    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < N; cell += gridDim.x * blockDim.x) {
+        const int32_t b = g.cell_off[cell], e = g.cell_off[cell + 1];
+        const int L = e - b;
+        local_max = max(local_max, L);
+        // insertion sort by particle id (lists are a handful long)
+        for (int i = b + 1; i < e; ++i) {
+            const int32_t kp = g.cl_pid[i];
+            const uint16_t kc = g.cl_cnt[i];
+            int j = i - 1;
+            while (j >= b && g.cl_pid[j] > kp) {
+                g.cl_pid[j + 1] = g.cl_pid[j];
+                g.cl_cnt[j + 1] = g.cl_cnt[j];
+                --j;
+            }
+            g.cl_pid[j + 1] = kp;
+            g.cl_cnt[j + 1] = kc;
+        }
+        double asum = 0.0;
+        int csum = 0;
+        for (int i = b; i < e; ++i) {
+            const int c = g.cl_cnt[i];
+            asum = xadd(asum, xdiv((double)c, S3d));
+            csum += c;
+        }
+        g.alpha_sum[cell] = asum;
+        g.solid[cell] = asum < 0.0 ? 0.0 : (asum > 1.0 ? 1.0 : asum);
+        if (g.level) g.level[cell] = (uint8_t)(csum < S3 ? csum : S3);
+    }
+    // warp max then one atomic per warp
+    for (int s = 16; s > 0; s >>= 1) local_max = max(local_max, __shfl_xor_sync(0xffffffffu, local_max, s));
+    if ((threadIdx.x & 31) == 0 && local_max > 0)
+        atomicMax(reinterpret_cast<unsigned long long*>(g.totals + 2), (unsigned long long)local_max);
+}
+
+template <typename O>
+__global__ void k_solid_velocity(psc_geometry g, O* us) {
+    const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
+    const double S3d = (double)(g.subsamples * g.subsamples * g.subsamples);
+    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < N; cell += gridDim.x * blockDim.x) {
+        const int32_t b = g.cell_off[cell], e = g.cell_off[cell + 1];
+        double ux = 0.0, uy = 0.0, uz = 0.0;
+        if (e > b) {
+            const uint32_t iz = cell % g.nz, rr = cell / g.nz, iy = rr % g.ny, ix = rr / g.ny;
+            const double xn = xadd((double)ix, 0.5), yn = xadd((double)iy, 0.5), zn = xadd((double)iz, 0.5);
+            for (int i = b; i < e; ++i) {
+                const double* q = g.particles + (size_t)g.cl_pid[i] * PF;
+                const double al = xdiv((double)g.cl_cnt[i], S3d);
+                const double rx = xsub(xn, q[0]), ry = xsub(yn, q[1]), rz = xsub(zn, q[2]);
+                // v = V + w x r in the reference's term order (psc3d.py:362-364)
+                const double vx = xsub(xadd(q[4], xmul(q[8], rz)), xmul(q[9], ry));
+                const double vy = xsub(xadd(q[5], xmul(q[9], rx)), xmul(q[7], rz));
+                const double vz = xsub(xadd(q[6], xmul(q[7], ry)), xmul(q[8], rx));
+                ux = xadd(ux, xmul(al, vx));
+                uy = xadd(uy, xmul(al, vy));
+                uz = xadd(uz, xmul(al, vz));
+            }
+            const double as = g.alpha_sum[cell];
+            if (as > 1.0e-14) {
+                ux = xdiv(ux, as);
+                uy = xdiv(uy, as);
+                uz = xdiv(uz, as);
+            }
+        }
+        us[cell] = (O)ux;
+        us[(size_t)N + cell] = (O)uy;
+        us[2 * (size_t)N + cell] = (O)uz;
+    }
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double (*s)[NV]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) s[warp][k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double acc = 0.0;
+            for (int w = 0; w < nw; ++w) acc += s[w][k];
+            v[k] = acc;
+        }
+    }
+    __syncthreads();
+}
+
+constexpr int LOAD_THREADS = 256;
+
+// One block per chunk of one particle's bbox entries.
+template <typename I>
+__global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, const I* imb, double* part) {
+    __shared__ double s[LOAD_THREADS / 32][6];
+    const int64_t C = g.totals[1];
+    const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
+    const double S3d = (double)(g.subsamples * g.subsamples * g.subsamples);
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {
+        const int p = owner_of(g.chunk_off, g.nparticles, chunk);
+        const int64_t e0 = g.ent_off[p] + (chunk - g.chunk_off[p]) * g.chunk_entries;
+        const int64_t e1 = min(e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
+        const double* q = g.particles + (size_t)p * PF;
+        const int32_t* bb = g.bbox + (size_t)p * 6;
+        const int64_t eyz = (int64_t)bb[4] * bb[5];
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+            const uint16_t cnt = g.ent_cnt[e];
+            if (cnt == 0) continue;
+            const int64_t local = e - g.ent_off[p];
+            const int32_t a = (int32_t)(local / eyz);
+            const int64_t rem = local - (int64_t)a * eyz;
+            const int32_t b = (int32_t)(rem / bb[5]);
+            const int32_t k = (int32_t)(rem - (int64_t)b * bb[5]);
+            const int32_t ix = bb[0] + a, iy = bb[1] + b, iz = bb[2] + k;
+            const uint32_t cell = ((uint32_t)ix * g.ny + iy) * g.nz + iz;
+            // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
+            const double al = xdiv((double)cnt, S3d);
+            const double as = g.alpha_sum[cell];
+            const double ow = xdiv(al, as > 1.0e-14 ? as : 1.0e-14);
+            const double nfx = -xmul(ow, (double)imb[cell]);
+            const double nfy = -xmul(ow, (double)imb[(size_t)N + cell]);
+            const double nfz = -xmul(ow, (double)imb[2 * (size_t)N + cell]);
+            // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
+            const double rx = xsub(xadd((double)ix, 0.5), q[0]);
+            const double ry = xsub(xadd((double)iy, 0.5), q[1]);
+            const double rz = xsub(xadd((double)iz, 0.5), q[2]);
+            acc[0] += nfx;
+            acc[1] += nfy;
+            acc[2] += nfz;
+            acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
+            acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
+            acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
+        }
+        block_sum<6>(acc, s);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
+        }
+    }
+}
+
+// One block: per-particle sums of chunk partials (fixed order), then the
+// closure residual |sum_p F_p + sum_x imb| and the max force / torque norms.
+__global__ void __launch_bounds__(1024) k_loads_final(psc_geometry g, const double* part, const double* imb_sums,
+                                                      double* forces, double* torques, double* diag) {
+    __shared__ double s[32][5];
+    const int P = g.nparticles;
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // sum Fx, Fy, Fz, max |F|^2, max |T|^2
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int64_t c = g.chunk_off[p]; c < g.chunk_off[p + 1]; ++c) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) F[k] += part[c * 6 + k];
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            forces[(size_t)p * 3 + k] = F[k];
+            torques[(size_t)p * 3 + k] = F[3 + k];
+        }
+        v[0] += F[0];
+        v[1] += F[1];
+        v[2] += F[2];
+        v[3] = fmax(v[3], F[0] * F[0] + F[1] * F[1] + F[2] * F[2]);
+        v[4] = fmax(v[4], F[3] * F[3] + F[4] * F[4] + F[5] * F[5]);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        double x = v[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = k < 3 ? x + y : fmax(x, y);
+        }
+        if (lane == 0) s[warp][k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int w = 0; w < nw; ++w) {
+            for (int k = 0; k < 3; ++k) r[k] += s[w][k];
+            r[3] = fmax(r[3], s[w][3]);
+            r[4] = fmax(r[4], s[w][4]);
+        }
+        const double cx = r[0] + imb_sums[0], cy = r[1] + imb_sums[1], cz = r[2] + imb_sums[2];
+        diag[PSC_DIAG_MOMENTUM_RESIDUAL] = sqrt(cx * cx + cy * cy + cz * cz);
+        diag[PSC_DIAG_MAX_FORCE] = sqrt(r[3]);
+        diag[PSC_DIAG_MAX_TORQUE] = sqrt(r[4]);
+        diag[PSC_DIAG_FORCE_SUM_X] = r[0];
+        diag[PSC_DIAG_FORCE_SUM_Y] = r[1];
+        diag[PSC_DIAG_FORCE_SUM_Z] = r[2];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scan (int32), three passes over blocks of SCAN_ITEMS elements
+// ---------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_PER_THREAD = 8;
+constexpr int SCAN_ITEMS = SCAN_THREADS * SCAN_PER_THREAD;
+
+size_t scan_tmp_bytes(int64_t n) {
+    const int64_t nb = (n + SCAN_ITEMS - 1) / SCAN_ITEMS;
+    return (size_t)(nb + 1) * sizeof(int32_t) + 256;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_partial(const int32_t* in, int64_t n, int32_t* bsum) {
+    __shared__ int32_t s_warp[32];
+    const int64_t base = (int64_t)blockIdx.x * SCAN_ITEMS + (int64_t)threadIdx.x * SCAN_PER_THREAD;
+    int32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; ++k)
+        if (base + k < n) acc += in[base + k];
+    int32_t total;
+    block_exclusive_scan<int32_t>(acc, s_warp, total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_top(int32_t* bsum, int64_t nb) {
+    __shared__ int32_t s_warp[32];
+    __shared__ int32_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < nb; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        const int32_t v = i < nb ? bsum[i] : 0;
+        int32_t total;
+        const int32_t ex = block_exclusive_scan<int32_t>(v, s_warp, total);
+        if (i < nb) bsum[i] = s_carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bsum[nb] = s_carry;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int32_t* in, int32_t* out, int64_t n,
+                                                             const int32_t* bsum, int64_t nb) {
+    __shared__ int32_t s_warp[32];
+    const int64_t base = (int64_t)blockIdx.x * SCAN_ITEMS + (int64_t)threadIdx.x * SCAN_PER_THREAD;
+    int32_t v[SCAN_PER_THREAD];
+    int32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        acc += v[k];
+    }
+    int32_t total;
+    int32_t run = block_exclusive_scan<int32_t>(acc, s_warp, total) + bsum[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = bsum[nb];
+}
+
+cudaError_t scan_exclusive_i32(const int32_t* in, int32_t* out, int64_t n, void* tmp, cudaStream_t stream) {
+    const int64_t nb = (n + SCAN_ITEMS - 1) / SCAN_ITEMS;
+    int32_t* bsum = reinterpret_cast<int32_t*>(tmp);
+    if (nb == 0) {
+        return cudaMemsetAsync(out, 0, sizeof(int32_t), stream);
+    }
+    k_scan_partial<<<(unsigned)nb, SCAN_THREADS, 0, stream>>>(in, n, bsum);
+    k_scan_top<<<1, 1024, 0, stream>>>(bsum, nb);
+    k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, stream>>>(in, out, n, bsum, nb);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static unsigned grid_cap(int64_t work, int threads) {
+    int64_t gsz = (work + threads - 1) / threads;
+    const int64_t cap = (int64_t)sm_count() * 32;
+    if (gsz > cap) gsz = cap;
+    if (gsz < 1) gsz = 1;
+    return (unsigned)gsz;
+}
+
+cudaError_t launch_geometry_plan(const psc_geometry& g, cudaStream_t stream) {
+    k_geometry_plan<<<1, 1024, 0, stream>>>(g);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_geometry_build(const psc_geometry& g, cudaStream_t stream) {
+    const int64_t N = (int64_t)g.nx * g.ny * g.nz;
+    cudaError_t e = cudaMemsetAsync(g.cell_n, 0, (size_t)N * sizeof(int32_t), stream);
+    if (e != cudaSuccess) return e;
+    if (g.capacity_entries > 0) {
+        k_geometry_count<<<grid_cap(g.capacity_entries, 256), 256, 0, stream>>>(g);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if ((e = scan_exclusive_i32(g.cell_n, g.cell_off, N, g.scan_tmp, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(g.cell_n, 0, (size_t)N * sizeof(int32_t), stream)) != cudaSuccess) return e;
+    if (g.capacity_entries > 0) {
+        k_geometry_fill<<<grid_cap(g.capacity_entries, 256), 256, 0, stream>>>(g);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    k_geometry_final<<<grid_cap(N, 256), 256, 0, stream>>>(g);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_solid_velocity(const psc_geometry& g, int us_type, void* us, cudaStream_t stream) {
+    const int64_t N = (int64_t)g.nx * g.ny * g.nz;
+    if (us_type == 0) k_solid_velocity<double><<<grid_cap(N, 256), 256, 0, stream>>>(g, reinterpret_cast<double*>(us));
+    else k_solid_velocity<float><<<grid_cap(N, 256), 256, 0, stream>>>(g, reinterpret_cast<float*>(us));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const void* imb, double* chunk_partials,
+                                  const double* imb_sums, double* forces, double* torques, double* diag,
+                                  cudaStream_t stream) {
+    if (g.capacity_chunks > 0 && g.nparticles > 0) {
+        const int64_t cap = (int64_t)sm_count() * 8;
+        const unsigned grid = (unsigned)(g.capacity_chunks < cap ? g.capacity_chunks : cap);
+        if (imb_type == 0)
+            k_loads_chunks<double><<<grid, LOAD_THREADS, 0, stream>>>(g, reinterpret_cast<const double*>(imb),
+                                                                      chunk_partials);
+        else
+            k_loads_chunks<float><<<grid, LOAD_THREADS, 0, stream>>>(g, reinterpret_cast<const float*>(imb),
+                                                                     chunk_partials);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    k_loads_final<<<1, 1024, 0, stream>>>(g, chunk_partials, imb_sums, forces, torques, diag);
+    return cudaGetLastError();
+}
+
+}  // namespace psc

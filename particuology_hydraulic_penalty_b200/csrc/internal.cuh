@@ -1,0 +1,48 @@
+// Internal declarations shared by the .cu translation units of libpscb200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+
+#include <string>
+
+#include "../../include/psc_b200.h"
+
+namespace psc {
+
+// Thread-local last-error slot behind psc_last_error().
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t err, const char* what);
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+constexpr int STEP_THREADS = 256;
+constexpr int MAX_SMEM_WINDOWS = 256;
+
+// launchers (return cudaError_t of the launch)
+cudaError_t launch_step(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
+                        bool moving, int grid_ctas, cudaStream_t stream);
+cudaError_t launch_reduce_windows(const psc_window* d_windows, int nwin, double* out, cudaStream_t stream);
+cudaError_t launch_init_equilibrium(int store, double scale, void* f, int64_t ncells, cudaStream_t stream);
+cudaError_t launch_stream_push(int store, double scale, const void* src, double* dst, int nx, int ny, int nz,
+                               cudaStream_t stream);
+cudaError_t launch_stream_pull_store(int store, double scale, const double* src, void* dst, int nx, int ny, int nz,
+                                     cudaStream_t stream);
+
+cudaError_t launch_geometry_plan(const psc_geometry& g, cudaStream_t stream);
+cudaError_t launch_geometry_build(const psc_geometry& g, cudaStream_t stream);
+cudaError_t launch_solid_velocity(const psc_geometry& g, int us_type, void* us, cudaStream_t stream);
+cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const void* imb, double* chunk_partials,
+                                  const double* imb_sums, double* forces, double* torques, double* diag,
+                                  cudaStream_t stream);
+
+// exclusive scan of int32 counts -> int32 offsets, out has n + 1 entries
+size_t scan_tmp_bytes(int64_t n);
+cudaError_t scan_exclusive_i32(const int32_t* in, int32_t* out, int64_t n, void* tmp, cudaStream_t stream);
+
+}  // namespace psc
