@@ -1,0 +1,454 @@
+#!/usr/bin/env python3
+"""Benchmark of the batched PSC-IMB step on B200 (one JSON line on rank 0).
+
+Workload ("batch24"): 24 seeded periodic pore windows, edges drawn from
+{48, 64, 96, 128, 160}, geometry type skeleton / passive fines / preloaded
+fines, 4^3 sub-samples, BGK tau = 0.8, body force 1e-6 along x; FP32
+deviation storage; every step is one persistent launch over all windows,
+replayed from a captured CUDA graph.  A step is one lattice update of every
+window; ``value`` is MLUPS over all ranks.  The populations (about 5 GB per
+GPU) exceed the 126 MB L2, so no flush is needed between steps.
+
+Also reported on the same line:
+  fp64_plain  -- the same windows solved one at a time in FP64 (deviation
+                 storage, one launch per step, no graph): MLUPS, windows/hour
+                 at 5000 steps, and the FP32/FP64 permeability difference
+                 after the same number of steps from rest
+  e2e         -- MLUPS through the drop-in SparsePscD3Q19.collide_stream_psc()
+                 (particle upload, step, loads, diagnostics read back per call)
+  roofline    -- achieved HBM GB/s of the step kernel vs the measured peak
+  cpu_baseline-- the NumPy oracle port on this host's cores (bounded sample)
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+NumPy oracle port, run on all host cores) on the same workload instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "PSC-IMB MLUPS & %HBM peak, FP32/batched vs plain FP64 at <=1e-4 perm. error"
+UNIT = "MLUPS"
+TAU = 0.8
+FORCE = (1.0e-6, 0.0, 0.0)
+SUBSAMPLES = 4
+NWIN = 24
+STEPS_PER_WINDOW = 5000
+# algorithmic bytes per lattice update: 19 populations read + 19 written,
+# plus the 1-byte solid level (static particles: no solid-velocity field)
+BYTES_PER_LUP = {"fp32": 2 * 19 * 4 + 1, "fp64": 2 * 19 * 8 + 1, "fp16": 2 * 19 * 2 + 1, "bf16": 2 * 19 * 2 + 1}
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle port) -- runs in spawned worker processes
+# ---------------------------------------------------------------------------
+def _oracle_worker(args):
+    n, parts, steps, warm = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from oracle import psc_oracle as orc
+
+    s = orc.OracleSolver(n, parts, tau=TAU, subsamples=SUBSAMPLES, force=FORCE, static_geometry=True)
+    for _ in range(warm):
+        s.collide_stream_psc()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.collide_stream_psc()
+    return n ** 3, steps, time.perf_counter() - t0
+
+
+def cpu_sample(windows, steps: int, warm: int, procs: int | None = None):
+    """Oracle steps on the smallest windows, one process per host core."""
+    procs = procs or os.cpu_count() or 1
+    small = sorted(windows, key=lambda w: w.n)
+    jobs = [(small[k % len(small)].n, small[k % len(small)].particles, steps, warm) for k in range(procs)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_oracle_worker, jobs)
+    wall = time.perf_counter() - t0
+    cells = sum(r[0] * r[1] for r in res)
+    slowest = max(r[2] for r in res)
+    return {
+        "value": cells / slowest / 1e6,
+        "unit": UNIT,
+        "cores": procs,
+        "sample": f"{procs} processes x {steps} oracle steps (after {warm} warm-up) on {len(set(j[0] for j in jobs))} "
+                  f"window size(s) {sorted(set(j[0] for j in jobs))}^3 of the batch; NumPy single-threaded per process",
+        "wall_s": round(wall, 2),
+    }
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.t_on = None
+        self.t_off = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_tag: str):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "k_step_batch24.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith(f"traffic_bytes_per_launch[{kernel_tag}]"):
+            try:
+                return float(line.split("=", 1)[1].split()[0])
+            except (IndexError, ValueError):
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+# ---------------------------------------------------------------------------
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def timed(fn, world):
+    import torch
+
+    barrier(world)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    fn()
+    b.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    return a.elapsed_time(b)
+
+
+def run_fp64_plain(windows, steps: int, warm: int):
+    """Each window alone in FP64 (one launch per step, no graph)."""
+    import torch
+
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    per_window = []
+    for w in windows:
+        b = PscBatch([WindowSpec(w.n, w.particles, TAU, FORCE, SUBSAMPLES)], precision="fp64", graph_steps=0)
+        b.run(warm)
+        ms = timed(lambda: b.run(steps), 1)
+        per_window.append(ms / steps)
+        del b
+        torch.cuda.empty_cache()
+    return per_window
+
+
+def run_e2e(windows, steps: int):
+    """MLUPS through the drop-in class (host particle upload + diagnostics read back per call)."""
+    import torch
+
+    from particuology_hydraulic_penalty_b200 import SparsePscD3Q19
+
+    solvers = [SparsePscD3Q19(w.n, w.particles, tau=TAU, subsamples=SUBSAMPLES, static_geometry=True,
+                              precision="fp32", force=FORCE) for w in windows]
+    for s in solvers:
+        s.collide_stream_psc()
+    torch.cuda.synchronize()
+    h2d = sum(int(w.particles.nbytes) for w in windows)
+    P = [w.particles.shape[0] for w in windows]
+    from particuology_hydraulic_penalty_b200 import _native as nat
+
+    d2h = sum((nat.NRED + nat.NDIAG + 6 * p) * 8 for p in P)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for s in solvers:
+            s.collide_stream_psc()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    cells = sum(w.n ** 3 for w in windows)
+    del solvers
+    torch.cuda.empty_cache()
+    return {"value": cells * steps / wall / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "api": "SparsePscD3Q19.collide_stream_psc() per window, precision=fp32, static geometry",
+            "steps": steps}
+
+
+WORKLOADS = {
+    "batch24": "batch24: 24 uneven periodic pore windows, edges {48,64,96,128,160}, S=4, BGK tau=0.8, "
+               "F=1e-6 x, {prec} deviation storage, one persistent launch per step, CUDA graph",
+    "window96x3": "window96x3: one seeded 96^3 window in its three geometries (skeleton, passive fines, "
+                  "preloaded fines), S=4, BGK tau=0.8, F=1e-6 x, {prec} deviation storage, one launch per step",
+}
+
+
+def make_windows(workload: str, rank: int):
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+
+    if workload == "batch24":
+        return wgen.batched_windows(NWIN, seed0=NWIN * rank)
+    seed = 1000 + rank
+    return [wgen.make_window(96, kind, seed) for kind in wgen.GEOMETRY_TYPES]
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup()
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    wins = make_windows(args.workload, rank)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(wins, steps=args.cpu_steps, warm=1)
+        cpu["cpu_model"] = cpu_model()
+
+    specs = [WindowSpec(w.n, w.particles, TAU, FORCE, SUBSAMPLES, name=w.kind) for w in wins]
+    batch = PscBatch(specs, precision=args.precision, graph_steps=args.graph_steps)
+    clocks = ClockSampler(local)
+    clocks.start()
+    batch.run(args.warmup)
+    torch.cuda.synchronize()
+    ms = timed(lambda: batch.run(args.steps), world)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms, world)
+    red = batch.observe()
+    k32 = batch.permeability(red)
+    nonfinite = bool(batch.nonfinite(red).any())
+    cells_rank = batch.total_cells
+    cells_all = sum_over_ranks(float(cells_rank), world)
+    value = cells_all * args.steps / (ms_max * 1e-3) / 1e6
+    lups_rank = cells_rank * args.steps / (ms * 1e-3)
+    bpl = BYTES_PER_LUP[args.precision]
+    peak, peak_kind = measured_peak_hbm()
+    achieved = bpl * lups_rank / 1e9
+    traffic = ncu_traffic(args.precision)
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else args.precision,
+        "data": "synthetic (seeded FCC skeleton / passive / preloaded pore windows; the reference's dumps are not shipped)",
+        "config": {"workload": WORKLOADS[args.workload].format(prec=args.precision.upper()),
+                   "windows_per_gpu": len(wins), "cells_per_gpu": cells_rank,
+                   "l2": "inputs (~5 GB/GPU) exceed the 126 MB L2; no flush", "parallelism": f"window-parallel x{world}",
+                   "graph_steps": args.graph_steps},
+        "gpu_launches": args.steps * batch.launches_per_step(),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": traffic, "bytes_per_lup": bpl,
+                     "kernel": "psc::k_step (fused pull-stream + PSC collide), avg launch = timed region / steps"},
+        "clocks": clk,
+        "nonfinite": nonfinite,
+    }
+    if rank == 0 and world == 1 and not args.no_fp64:
+        # FP32 vs FP64 permeability after the same number of steps from rest
+        del batch
+        torch.cuda.empty_cache()
+        b64 = PscBatch(specs, precision="fp64", graph_steps=args.graph_steps)
+        b64.run(args.warmup + args.steps)
+        k64 = b64.permeability()
+        del b64
+        torch.cuda.empty_cache()
+        err = np.abs(k32 - k64) / np.maximum(np.abs(k64), 1e-300)
+        per_ms = run_fp64_plain(wins, steps=args.fp64_steps, warm=3)
+        t_plain_h = sum(STEPS_PER_WINDOW * m * 1e-3 for m in per_ms) / 3600.0
+        t_batch_h = STEPS_PER_WINDOW * (ms / args.steps) * 1e-3 / 3600.0  # all windows advance together
+        out["fp64_plain"] = {
+            "mlups": round(sum(w.n ** 3 for w in wins) / (sum(per_ms) * 1e-3) / 1e6, 1),
+            "windows_per_hour": round(len(wins) / t_plain_h, 1),
+            "fp32_batched_windows_per_hour": round(len(wins) / t_batch_h, 1),
+            "windows_per_hour_ratio": round(t_plain_h / t_batch_h, 3),
+            "perm_rel_err_max_fp32_vs_fp64": float(err.max()),
+            "perm_rel_err_note": f"after {args.warmup + args.steps} steps from rest, same windows",
+            "steps_per_window_assumed": STEPS_PER_WINDOW,
+        }
+    if rank == 0 and world == 1 and not args.no_e2e:
+        out["e2e"] = run_e2e(wins, steps=args.e2e_steps)
+    elif rank == 0:
+        out["e2e"] = None
+    if cpu is not None:
+        out["cpu_baseline"] = {"value": round(cpu["value"], 4), "unit": UNIT, "cores": cpu["cores"], "kind": "port",
+                               "sample": cpu["sample"], "cpu_model": cpu["cpu_model"]}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference algorithm on the host cores (the oracle port), same workload and metric."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wins = make_windows(args.workload, 0)
+    procs = os.cpu_count() or 1
+    small = sorted(wins, key=lambda w: w.n)
+    jobs = [(small[k % len(small)].n, small[k % len(small)].particles, args.steps, args.warmup) for k in range(procs)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_oracle_worker, jobs)
+    cells = sum(r[0] * r[1] for r in res)
+    slowest = max(r[2] for r in res)
+    value = cells / slowest / 1e6
+    sample = (f"{procs} processes x {args.steps} timed steps (after {args.warmup} warm-up) of the NumPy oracle "
+              f"port on the batch's smallest window size(s) {sorted(set(j[0] for j in jobs))}^3; "
+              f"one NumPy thread per process")
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(slowest / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+        "data": "synthetic (seeded pore windows)",
+        "config": {"workload": args.workload + " sample (smallest windows), reference algorithm on host cores",
+                   "cpu_model": cpu_model()},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="batch24")
+    ap.add_argument("--precision", choices=["fp32", "fp64", "fp16", "bf16"], default="fp32")
+    ap.add_argument("--graph-steps", type=int, default=20)
+    ap.add_argument("--fp64-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

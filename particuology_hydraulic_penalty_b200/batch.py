@@ -1,0 +1,229 @@
+"""Many pore windows of uneven size stepped by one persistent launch.
+
+Every step is ONE ``psc_step`` launch whose persistent grid walks the tiles
+of all windows; the windows' descriptors sit in two device tables (even and
+odd step parity).  Step sequences are captured once in a CUDA graph and
+replayed, so a run issues no per-step host work.  Reductions (Darcy flux,
+porosity, NaN count) are taken only on reporting steps, in FP64, per window.
+
+This is the throughput path for permeability campaigns (the reference runs
+one NumPy solver per window and resolution,
+scripts/run_psc_permeability_resolution.py:122-192); the drop-in classes in
+``psc3d`` keep the reference's per-call semantics.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .engine import (DeviceGeometry, LatticeWindow, particles_array, require_cuda, store_mode, stream_handle,
+                     struct_to_device, vp)
+
+
+@dataclass
+class WindowSpec:
+    """One lattice window of a batch."""
+
+    n: int
+    particles: np.ndarray  # (P, 10)
+    tau: float = 0.8
+    force: tuple = (1.0e-6, 0.0, 0.0)
+    subsamples: int = 4
+    name: str = ""
+
+
+class PscBatch:
+    """A batch of independent periodic windows advanced together.
+
+    Parameters
+    ----------
+    specs : list of WindowSpec (or objects with ``n`` and ``particles``)
+    precision : storage mode ("fp64-exact", "fp64", "fp32", "fp16", "bf16")
+    graph_steps : steps per captured CUDA graph (0 disables graphs)
+    grid_ctas : persistent grid size (0 = SM count x occupancy)
+    """
+
+    def __init__(self, specs, precision: str = "fp32", store_scale: float | None = None, graph_steps: int = 20,
+                 grid_ctas: int = 0, device=None, tau=None, force=None, subsamples=None):
+        self.device = require_cuda(device)
+        self.store = store_mode(precision)
+        self.precision = precision
+        self.graph_steps = int(graph_steps)
+        if self.graph_steps % 2:
+            raise ValueError("graph_steps must be even (the graph must end on the buffer parity it started on)")
+        self.grid_ctas = int(grid_ctas)
+        self.specs = []
+        for s in specs:
+            if not isinstance(s, WindowSpec):
+                s = WindowSpec(n=int(s.n), particles=np.asarray(s.particles), name=getattr(s, "kind", ""))
+            if tau is not None:
+                s.tau = float(tau)
+            if force is not None:
+                s.force = tuple(float(v) for v in force)
+            if subsamples is not None:
+                s.subsamples = int(subsamples)
+            self.specs.append(s)
+        if not self.specs:
+            raise ValueError("a batch needs at least one window")
+        self.windows: list[LatticeWindow] = []
+        self.geoms: list[DeviceGeometry] = []
+        with torch.cuda.device(self.device):
+            for s in self.specs:
+                shape = (s.n, s.n, s.n)
+                win = LatticeWindow(shape, s.tau, s.force, s.subsamples, self.store, store_scale, self.device)
+                geo = DeviceGeometry(shape, s.subsamples, self.device, want_level=self.store != nat.STORE_F64_EXACT)
+                geo.set_particles(particles_array(s.particles))
+                geo.rebuild()
+                win.bind_geometry(geo)
+                self.windows.append(win)
+                self.geoms.append(geo)
+        self.cells = np.array([w.N for w in self.windows], dtype=np.int64)
+        self.parity = 0
+        self.steps_done = 0
+        self._tables = None
+        self._graphs: dict = {}
+        self._red = torch.zeros(len(self.windows) * nat.NRED, dtype=torch.float64, device=self.device)
+        self._build_tables()
+
+    # ------------------------------------------------------------------
+    def _build_tables(self) -> None:
+        nwin = len(self.windows)
+        tables = []
+        self.partials = None
+        for parity in (0, 1):
+            arr = (nat.PscWindow * nwin)()
+            for k, w in enumerate(self.windows):
+                arr[k] = w.struct(parity)
+            total = ctypes.c_int64(0)
+            nat.call("psc_plan_tiles", arr, nwin, 0, ctypes.byref(total))
+            if self.partials is None:
+                self.total_tiles = int(total.value)
+                self.partials = torch.zeros(self.total_tiles * nat.NRED, dtype=torch.float64, device=self.device)
+            base = self.partials.data_ptr()
+            for k in range(nwin):
+                arr[k].partials = base + int(arr[k].tile_begin) * nat.NRED * 8
+            tables.append(struct_to_device(arr, self.device))
+        self._tables = tables
+        self._graphs = {}
+
+    @property
+    def nwin(self) -> int:
+        return len(self.windows)
+
+    @property
+    def total_cells(self) -> int:
+        return int(self.cells.sum())
+
+    def _launch(self, flags: int) -> None:
+        nat.call("psc_step", self.store, vp(self._tables[self.parity]), self.nwin, self.total_tiles,
+                 flags, self.grid_ctas, stream_handle(self.device))
+
+    def step_once(self, flags: int = 0) -> None:
+        """One collide-stream step of every window (one kernel launch)."""
+        self._launch(flags | nat.STEP_COLLIDE)
+        self.parity ^= 1
+        for w in self.windows:
+            w.cur = self.parity
+        self.steps_done += 1
+
+    def _capture(self) -> None:
+        """Capture graph_steps launches starting at the current buffer parity."""
+        g = torch.cuda.CUDAGraph()
+        stream = torch.cuda.Stream(self.device)
+        stream.wait_stream(torch.cuda.current_stream(self.device))
+        parity0 = self.parity
+        with torch.cuda.stream(stream):
+            with torch.cuda.graph(g, stream=stream):
+                for _ in range(self.graph_steps):
+                    self._launch(nat.STEP_COLLIDE)
+                    self.parity ^= 1
+        torch.cuda.current_stream(self.device).wait_stream(stream)
+        self.parity = parity0
+        self._graphs[parity0] = g
+
+    def run(self, steps: int) -> None:
+        """Advance every window by ``steps`` steps (graph replays plus a remainder)."""
+        steps = int(steps)
+        with torch.cuda.device(self.device):
+            if self.graph_steps > 0 and steps >= self.graph_steps:
+                if self.steps_done == 0:
+                    self.step_once()  # warm the launch path before capture
+                    steps -= 1
+                if self.parity not in self._graphs:
+                    self._capture()
+                graph = self._graphs[self.parity]  # an even step count returns to this parity
+                reps = steps // self.graph_steps
+                for _ in range(reps):
+                    graph.replay()
+                self.steps_done += reps * self.graph_steps
+                steps -= reps * self.graph_steps
+                for w in self.windows:
+                    w.cur = self.parity
+            for _ in range(steps):
+                self.step_once()
+
+    def launches_per_step(self) -> int:
+        return 1
+
+    # ------------------------------------------------------------------
+    def observe(self) -> np.ndarray:
+        """FP64 reductions of every window's current post-stream state, (nwin, NRED) on the host."""
+        with torch.cuda.device(self.device):
+            self._launch(nat.STEP_REDUCE)
+            nat.call("psc_reduce_windows", vp(self._tables[self.parity]), self.nwin, vp(self._red),
+                     stream_handle(self.device))
+            return self._red.view(self.nwin, nat.NRED).cpu().numpy().copy()
+
+    def permeability(self, red: np.ndarray | None = None) -> np.ndarray:
+        """Darcy K per window along its body force, run_psc_permeability_resolution.py:144-150."""
+        red = self.observe() if red is None else red
+        out = np.zeros(self.nwin)
+        for k, s in enumerate(self.specs):
+            F = np.asarray(s.force, dtype=float)
+            fmag = float(np.linalg.norm(F))
+            d = F / max(fmag, 1e-300)
+            flux = d[0] * red[k, nat.RED_FLUID_UX] + d[1] * red[k, nat.RED_FLUID_UY] + d[2] * red[k, nat.RED_FLUID_UZ]
+            superficial = flux / float(self.cells[k])
+            nu = (s.tau - 0.5) / 3.0
+            out[k] = nu * superficial / max(fmag, 1e-300)
+        return out
+
+    def nonfinite(self, red: np.ndarray | None = None) -> np.ndarray:
+        red = self.observe() if red is None else red
+        return red[:, nat.RED_NONFINITE] > 0
+
+    def loads(self) -> list[tuple[np.ndarray, np.ndarray]]:
+        """Per-particle force and torque of every window from one extra collide step."""
+        out = []
+        with torch.cuda.device(self.device):
+            self._ensure_imb()
+            self.step_once(nat.STEP_IMB | nat.STEP_REDUCE)
+            nat.call("psc_reduce_windows", vp(self._tables[self.parity]), self.nwin, vp(self._red),
+                     stream_handle(self.device))
+            for k, (w, g) in enumerate(zip(self.windows, self.geoms)):
+                P = g.P
+                F = torch.zeros((P, 3), dtype=torch.float64, device=self.device)
+                T = torch.zeros((P, 3), dtype=torch.float64, device=self.device)
+                diag = torch.zeros(nat.NDIAG, dtype=torch.float64, device=self.device)
+                g.loads(w.imb, self._red[k * nat.NRED + nat.RED_IMBX:], F, T, diag)
+                out.append((F.cpu().numpy(), T.cpu().numpy()))
+        return out
+
+    def _ensure_imb(self) -> None:
+        if any(w.imb is None for w in self.windows):
+            for w in self.windows:
+                w.ensure_fields(imb=True, moments=False)
+            self._build_tables()
+
+    def velocity_field(self, k: int) -> np.ndarray:
+        """(4, n, n, n) rho, ux, uy, uz of window k's post-stream state (FP64 host copy)."""
+        w = self.windows[k]
+        with torch.cuda.device(self.device):
+            w.cur = self.parity
+            w.moments_pass(None, write_fields=True)
+            return w.moments.to(torch.float64).view(4, w.nx, w.ny, w.nz).cpu().numpy()

@@ -292,8 +292,8 @@ class LatticeWindow:
         N = self.N
         self.f = [torch.empty(Q * N, dtype=sd, device=device), torch.empty(Q * N, dtype=sd, device=device)]
         self.cur = 0
-        self.imb = torch.zeros(3 * N, dtype=fd, device=device)
-        self.moments = torch.zeros(4 * N, dtype=fd, device=device)
+        self.imb: torch.Tensor | None = None  # [3][N], allocated on first use
+        self.moments: torch.Tensor | None = None  # [4][N], allocated on first use
         self.us: torch.Tensor | None = None
         self.red = torch.zeros(nat.NRED, dtype=torch.float64, device=device)
         self.red_post = torch.zeros(nat.NRED, dtype=torch.float64, device=device)
@@ -312,6 +312,15 @@ class LatticeWindow:
         self.level_ptr = vp(geo.level)
         self._dirty = True
 
+    def ensure_fields(self, imb: bool = True, moments: bool = True) -> None:
+        fd = FIELD_DTYPE[self.store]
+        if imb and self.imb is None:
+            self.imb = torch.zeros(3 * self.N, dtype=fd, device=self.device)
+            self._dirty = True
+        if moments and self.moments is None:
+            self.moments = torch.zeros(4 * self.N, dtype=fd, device=self.device)
+            self._dirty = True
+
     def ensure_us(self) -> torch.Tensor:
         if self.us is None:
             self.us = torch.zeros(3 * self.N, dtype=FIELD_DTYPE[self.store], device=self.device)
@@ -322,6 +331,10 @@ class LatticeWindow:
         if moving != self.moving:
             self.moving = moving
             self._dirty = True
+
+    def struct(self, src: int) -> nat.PscWindow:
+        """The psc_window descriptor reading buffer ``src`` (tile fields unset)."""
+        return self._struct(src)
 
     def _struct(self, src: int) -> nat.PscWindow:
         w = nat.PscWindow()
@@ -359,6 +372,7 @@ class LatticeWindow:
     # kernels ----------------------------------------------------------------
     def step(self, flags: int) -> None:
         """One fused pull-stream + collide step; swaps the population buffers."""
+        self.ensure_fields(imb=bool(flags & nat.STEP_IMB), moments=bool(flags & nat.STEP_MOMENTS))
         if self.store == nat.STORE_F64_EXACT and self.solid_ptr is None:
             raise RuntimeError("geometry not bound")
         if self.store != nat.STORE_F64_EXACT and self.level_ptr is None:
@@ -373,6 +387,7 @@ class LatticeWindow:
 
     def moments_pass(self, reduce_out: torch.Tensor | None = None, write_fields: bool = True) -> None:
         """Moments (and reductions) of the current post-stream state, no collision."""
+        self.ensure_fields(imb=False, moments=write_fields)
         fl = (nat.STEP_MOMENTS if write_fields else 0) | (nat.STEP_REDUCE if reduce_out is not None else 0)
         nat.call("psc_step", self.store, vp(self.windows(self.cur)), 1, self.tiles, fl, 0,
                  stream_handle(self.device))

@@ -80,6 +80,7 @@ class PscD3Q19:
             self._geo = DeviceGeometry(shape, self.subsamples, self._device,
                                        want_level=self._store != nat.STORE_F64_EXACT)
             self._win.bind_geometry(self._geo)
+            self._win.ensure_fields(imb=True, moments=True)
             parr = particles_array(particles)
             self._geo.set_particles(parr)
             self._P = parr.shape[0]

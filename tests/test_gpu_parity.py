@@ -59,7 +59,8 @@ def test_exact_mode_matches_reference_bitwise(name):
     assert fe1 <= 1e-12 and te1 <= 1e-12, (fe1, te1)
     ref = data["diags"]
     assert np.allclose(diags[:, 0], ref[:, 0], rtol=1e-15, atol=0.0)
-    scale_u = max(np.abs(ref[:, 1]).max(), 1e-300)
+    # mean_uz can be pure round-off (flow along x): compare on the velocity scale
+    scale_u = max(np.abs(ref[:, 1]).max(), np.abs(np.stack([data["ux"], data["uy"], data["uz"]])).max(), 1e-300)
     assert np.abs(diags[:, 1] - ref[:, 1]).max() <= 1e-12 * scale_u
     fscale = max(float(np.abs(data["hydro_forces"]).sum()), 1e-30)
     assert np.all(diags[:, 2] <= 1e-12 * fscale + 1e-300)
@@ -151,7 +152,7 @@ def test_random_bed_against_oracle(seed):
     assert np.array_equal(g.uz, o.uz)
     fe, te = golden_io.load_errors(g.hydro_forces, g.hydro_torques, o.hydro_forces, o.hydro_torques, parts[:, 3])
     assert fe <= 1e-12 and te <= 1e-12
-    assert abs(dg["mean_uz"] - do["mean_uz"]) <= 1e-12 * abs(do["mean_uz"])
+    assert abs(dg["mean_uz"] - do["mean_uz"]) <= 1e-12 * max(abs(do["mean_uz"]), np.abs(o.uz).max())
 
 
 def test_particle_count_change_and_caller_arrays():
