@@ -291,7 +291,7 @@ def run_e2e(windows, steps: int):
 
 
 WORKLOADS = {
-    "batch24": "batch24: 24 uneven periodic pore windows, edges {48,64,96,128,160}, S=4, BGK tau=0.8, "
+    "batch24": "batch24: 24 uneven periodic pore windows, edges {{48,64,96,128,160}}, S=4, BGK tau=0.8, "
                "F=1e-6 x, {prec} deviation storage, one persistent launch per step, CUDA graph",
     "window96x3": "window96x3: one seeded 96^3 window in its three geometries (skeleton, passive fines, "
                   "preloaded fines), S=4, BGK tau=0.8, F=1e-6 x, {prec} deviation storage, one launch per step",

@@ -137,7 +137,31 @@ typedef struct psc_geometry {
     double* solid;            /* [N] clip(alpha_sum, 0, 1) (psc3d.py:175 / 344) */
     uint8_t* level;           /* [N] min(sum of counts, S^3), or NULL; needs S^3 <= 255 */
     void* scan_tmp;           /* scratch of psc_scan_tmp_bytes(N + 1) bytes */
+    /* Smooth solid fraction (the differentiable surrogate used by the
+     * adjoint): when smooth_eps > 0 every sample contributes
+     * sigma((r - |x_s - X|) / smooth_eps) instead of the 0/1 inside test. */
+    double smooth_eps;
+    double* ent_alpha;        /* [capacity_entries] smooth alpha per entry (smooth mode) */
+    int32_t* cl_ent;          /* [capacity_entries] entry index per cell-list slot (smooth mode) */
 } psc_geometry;
+
+/* Arguments of the adjoint kernels (one window, deviation storage F64/F32).
+ * The adjoint state lambda has the arithmetic type of the storage mode
+ * (double for PSC_STORE_F64, float for PSC_STORE_F32). */
+typedef struct psc_adjoint_args {
+    int32_t nx, ny, nz;
+    int32_t store;          /* PSC_STORE_F64 or PSC_STORE_F32 */
+    double tau;
+    double force[3];
+    double kappa;           /* nu / (|F| N): K = kappa * sum (1 - solid) u.dir */
+    double dir[3];          /* unit vector along the body force */
+    const void* state;      /* stored post-collision populations S_t [19][N] */
+    const double* solid;    /* clipped solid fraction [N] */
+    const void* lam_in;     /* dK/dS_{t+1} [19][N] */
+    void* lam_out;          /* dK/dS_t [19][N] (written, one store per element) */
+    double* dKdB;           /* [N] accumulated dK/dB */
+    double* dKdsolid;       /* [N] direct dK/dsolid (written by the seed) */
+} psc_adjoint_args;
 
 /* ---- library ------------------------------------------------------------ */
 int psc_abi_version(void);
@@ -146,6 +170,7 @@ const char* psc_last_error(void);
  * so bindings can check their struct layout. */
 size_t psc_window_size(void);
 size_t psc_geometry_size(void);
+size_t psc_adjoint_args_size(void);
 /* Bytes of scan scratch needed for n elements. */
 size_t psc_scan_tmp_bytes(int64_t n);
 
@@ -189,6 +214,18 @@ int psc_reduce_windows(const struct psc_window* d_windows, int nwin, double* out
  * [P][3], torques [P][3] and diag [PSC_NDIAG]. */
 int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb, double* chunk_partials,
                        const double* imb_sums, double* forces, double* torques, double* diag, void* stream);
+
+/* ---- adjoint of the permeability (no counterpart in the reference) ------- */
+/* Seed: lambda_T = dK/dS_T for K = kappa sum (1 - solid) u.dir of the
+ * post-stream state pull(S_T); also the direct term dK/dsolid. */
+int psc_adjoint_seed(const psc_adjoint_args* h_args, void* stream);
+/* One reverse step: lambda_t = pull^T (J_t^T lambda_{t+1}) with J_t the
+ * collision Jacobian at pull(S_t); dKdB += lambda_{t+1} . dC/dB. */
+int psc_adjoint_step(const psc_adjoint_args* h_args, void* stream);
+/* dK/d(x, y, z, r) per particle through the smooth solid fraction:
+ * grad[P][4]; chunk_partials [capacity_chunks][4] scratch. */
+int psc_adjoint_geometry_grad(const psc_geometry* h_geo, const psc_adjoint_args* h_args, double* chunk_partials,
+                              double* grad, void* stream);
 
 /* ---- population layout conversions -------------------------------------- */
 /* dst_i(x + c_i) = src_i(x): turns the stored post-collision populations into

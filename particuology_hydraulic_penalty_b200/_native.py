@@ -86,6 +86,16 @@ class PscGeometry(ctypes.Structure):
         ("totals", c_void_p), ("ent_cnt", c_void_p), ("cell_n", c_void_p), ("cell_off", c_void_p),
         ("cl_pid", c_void_p), ("cl_cnt", c_void_p), ("alpha_sum", c_void_p), ("solid", c_void_p),
         ("level", c_void_p), ("scan_tmp", c_void_p),
+        ("smooth_eps", c_double), ("ent_alpha", c_void_p), ("cl_ent", c_void_p),
+    ]
+
+
+class PscAdjointArgs(ctypes.Structure):
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32), ("store", c_int32),
+        ("tau", c_double), ("force", c_double * 3), ("kappa", c_double), ("dir", c_double * 3),
+        ("state", c_void_p), ("solid", c_void_p), ("lam_in", c_void_p), ("lam_out", c_void_p),
+        ("dKdB", c_void_p), ("dKdsolid", c_void_p),
     ]
 
 
@@ -95,6 +105,7 @@ SIGNATURES = {
     "psc_last_error": (ctypes.c_char_p, []),
     "psc_window_size": (c_size_t, []),
     "psc_geometry_size": (c_size_t, []),
+    "psc_adjoint_args_size": (c_size_t, []),
     "psc_scan_tmp_bytes": (c_size_t, [c_int64]),
     "psc_plan_tiles": (c_int, [POINTER(PscWindow), c_int, c_int, POINTER(c_int64)]),
     "psc_init_equilibrium": (c_int, [c_int, c_double, c_void_p, c_int64, c_void_p]),
@@ -105,6 +116,10 @@ SIGNATURES = {
     "psc_reduce_windows": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "psc_particle_loads": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),
+    "psc_adjoint_seed": (c_int, [POINTER(PscAdjointArgs), c_void_p]),
+    "psc_adjoint_step": (c_int, [POINTER(PscAdjointArgs), c_void_p]),
+    "psc_adjoint_geometry_grad": (c_int, [POINTER(PscGeometry), POINTER(PscAdjointArgs), c_void_p, c_void_p,
+                                          c_void_p]),
     "psc_stream_push": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "psc_stream_pull_store": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
 }
@@ -131,7 +146,8 @@ def load(path: Path | None = None) -> ctypes.CDLL:
         fn.argtypes = args
     if lib.psc_abi_version() != ABI_VERSION:
         raise NativeLibraryError("libpscb200.so ABI version mismatch: rebuild the library")
-    if lib.psc_window_size() != ctypes.sizeof(PscWindow) or lib.psc_geometry_size() != ctypes.sizeof(PscGeometry):
+    if (lib.psc_window_size() != ctypes.sizeof(PscWindow) or lib.psc_geometry_size() != ctypes.sizeof(PscGeometry)
+            or lib.psc_adjoint_args_size() != ctypes.sizeof(PscAdjointArgs)):
         raise NativeLibraryError("libpscb200.so struct layout mismatch: rebuild the library")
     if path is None:
         _lib = lib

@@ -77,6 +77,8 @@ size_t psc_window_size(void) { return sizeof(psc_window); }
 
 size_t psc_geometry_size(void) { return sizeof(psc_geometry); }
 
+size_t psc_adjoint_args_size(void) { return sizeof(psc_adjoint_args); }
+
 size_t psc_scan_tmp_bytes(int64_t n) { return scan_tmp_bytes(n < 0 ? 0 : n); }
 
 int psc_plan_tiles(psc_window* h_windows, int nwin, int tile_cells, int64_t* h_total_tiles) {
@@ -123,6 +125,12 @@ int psc_geometry_build(const psc_geometry* h_geo, void* stream) {
         return fail(PSC_E_INVALID, "psc_geometry_build: null entry array");
     if (g.level && g.subsamples * g.subsamples * g.subsamples > 255)
         return fail(PSC_E_UNSUPPORTED, "psc_geometry_build: the uint8 level field needs subsamples <= 6");
+    if (g.smooth_eps < 0.0 || !(g.smooth_eps == g.smooth_eps))
+        return fail(PSC_E_INVALID, "psc_geometry_build: smooth_eps must be >= 0");
+    if (g.smooth_eps > 0.0 && g.capacity_entries > 0 && (!g.ent_alpha || !g.cl_ent))
+        return fail(PSC_E_INVALID, "psc_geometry_build: smooth mode needs ent_alpha and cl_ent");
+    if (g.smooth_eps > 0.0 && g.level)
+        return fail(PSC_E_INVALID, "psc_geometry_build: smooth mode has no integer level (pass level = NULL)");
     cudaError_t e = launch_geometry_build(g, as_stream(stream));
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_geometry_build");
 }
@@ -164,6 +172,48 @@ int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb,
     cudaError_t e = launch_particle_loads(*h_geo, imb_type, imb, chunk_partials, imb_sums, forces, torques, diag,
                                           as_stream(stream));
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_particle_loads");
+}
+
+static int check_adjoint(const psc_adjoint_args* a, const char* who, bool need_in) {
+    if (!a) return fail(PSC_E_INVALID, std::string(who) + ": null args");
+    int st = check_extent(a->nx, a->ny, a->nz, who);
+    if (st) return st;
+    if (a->store != PSC_STORE_F64 && a->store != PSC_STORE_F32)
+        return fail(PSC_E_UNSUPPORTED, std::string(who) + ": the adjoint supports PSC_STORE_F64 and PSC_STORE_F32");
+    if (!(a->tau > 0.5)) return fail(PSC_E_INVALID, std::string(who) + ": tau must exceed 0.5");
+    if (!a->state || !a->solid || !a->lam_out || !a->dKdB || !a->dKdsolid || (need_in && !a->lam_in))
+        return fail(PSC_E_INVALID, std::string(who) + ": null array");
+    if (need_in && a->lam_in == a->lam_out)
+        return fail(PSC_E_INVALID, std::string(who) + ": lam_in and lam_out must differ (scattered stores)");
+    return PSC_OK;
+}
+
+int psc_adjoint_seed(const psc_adjoint_args* h_args, void* stream) {
+    int st = check_adjoint(h_args, "psc_adjoint_seed", false);
+    if (st) return st;
+    cudaError_t e = launch_adjoint_seed(*h_args, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_adjoint_seed");
+}
+
+int psc_adjoint_step(const psc_adjoint_args* h_args, void* stream) {
+    int st = check_adjoint(h_args, "psc_adjoint_step", true);
+    if (st) return st;
+    cudaError_t e = launch_adjoint_step(*h_args, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_adjoint_step");
+}
+
+int psc_adjoint_geometry_grad(const psc_geometry* h_geo, const psc_adjoint_args* h_args, double* chunk_partials,
+                              double* grad, void* stream) {
+    int st = check_geometry(h_geo, "psc_adjoint_geometry_grad");
+    if (st) return st;
+    if (!(h_geo->smooth_eps > 0.0))
+        return fail(PSC_E_INVALID, "psc_adjoint_geometry_grad: needs a smooth geometry (smooth_eps > 0)");
+    if (!h_args || !h_args->dKdB || !h_args->dKdsolid || !h_geo->alpha_sum)
+        return fail(PSC_E_INVALID, "psc_adjoint_geometry_grad: null array");
+    if (h_geo->nparticles > 0 && (!grad || (h_geo->capacity_chunks > 0 && !chunk_partials)))
+        return fail(PSC_E_INVALID, "psc_adjoint_geometry_grad: null output");
+    cudaError_t e = launch_adjoint_geometry_grad(*h_geo, *h_args, chunk_partials, grad, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_adjoint_geometry_grad");
 }
 
 int psc_stream_push(int store, double store_scale, const void* src, double* dst, int nx, int ny, int nz,

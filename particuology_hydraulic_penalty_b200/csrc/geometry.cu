@@ -179,12 +179,41 @@ __device__ __forceinline__ int sample_count(int32_t ix, int32_t iy, int32_t iz, 
     return cnt;
 }
 
+// Smooth surrogate of sample_count / S^3: every sample contributes
+// sigma((r - d_s) / eps) (logistic via tanh), the differentiable solid
+// fraction used by the adjoint.  Same boxes and sample offsets as the count.
+__device__ __forceinline__ double smooth_alpha(int32_t ix, int32_t iy, int32_t iz, double px, double py, double pz,
+                                               double r, int S, double eps) {
+    const double Sd = (double)S;
+    double acc = 0.0;
+    for (int a = 0; a < S; ++a) {
+        const double dx = ((double)ix + ((double)a + 0.5) / Sd) - px;
+        for (int b = 0; b < S; ++b) {
+            const double dy = ((double)iy + ((double)b + 0.5) / Sd) - py;
+            for (int c = 0; c < S; ++c) {
+                const double dz = ((double)iz + ((double)c + 0.5) / Sd) - pz;
+                const double d = sqrt(dx * dx + dy * dy + dz * dz);
+                acc += 0.5 * (1.0 + tanh(0.5 * (r - d) / eps));
+            }
+        }
+    }
+    return acc / (Sd * Sd * Sd);
+}
+
 __global__ void k_geometry_count(psc_geometry g) {
     const int64_t E = min(g.totals[0], g.capacity_entries);
+    const bool smooth = g.smooth_eps > 0.0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
         const EntryCell c = decode_entry(g, e);
         const double* q = g.particles + (size_t)c.p * PF;
-        const int cnt = sample_count(c.ix, c.iy, c.iz, q[0], q[1], q[2], xmul(q[3], q[3]), g.subsamples);
+        int cnt;
+        if (smooth) {
+            const double al = smooth_alpha(c.ix, c.iy, c.iz, q[0], q[1], q[2], q[3], g.subsamples, g.smooth_eps);
+            g.ent_alpha[e] = al;
+            cnt = al > 0.0 ? 1 : 0;  // membership of the cell list
+        } else {
+            cnt = sample_count(c.ix, c.iy, c.iz, q[0], q[1], q[2], xmul(q[3], q[3]), g.subsamples);
+        }
         g.ent_cnt[e] = (uint16_t)cnt;
         if (cnt > 0) atomicAdd(g.cell_n + c.cell, 1);
     }
@@ -201,6 +230,7 @@ __global__ void k_geometry_fill(psc_geometry g) {
         if (idx < g.capacity_entries) {
             g.cl_pid[idx] = c.p;
             g.cl_cnt[idx] = cnt;
+            if (g.cl_ent) g.cl_ent[idx] = (int32_t)e;
         }
     }
 }
@@ -216,23 +246,27 @@ __global__ void k_geometry_final(psc_geometry g) {
         const int L = e - b;
         local_max = max(local_max, L);
         // insertion sort by particle id (lists are a handful long)
+        const bool smooth = g.smooth_eps > 0.0;
         for (int i = b + 1; i < e; ++i) {
             const int32_t kp = g.cl_pid[i];
             const uint16_t kc = g.cl_cnt[i];
+            const int32_t ke = smooth ? g.cl_ent[i] : 0;
             int j = i - 1;
             while (j >= b && g.cl_pid[j] > kp) {
                 g.cl_pid[j + 1] = g.cl_pid[j];
                 g.cl_cnt[j + 1] = g.cl_cnt[j];
+                if (smooth) g.cl_ent[j + 1] = g.cl_ent[j];
                 --j;
             }
             g.cl_pid[j + 1] = kp;
             g.cl_cnt[j + 1] = kc;
+            if (smooth) g.cl_ent[j + 1] = ke;
         }
         double asum = 0.0;
         int csum = 0;
         for (int i = b; i < e; ++i) {
             const int c = g.cl_cnt[i];
-            asum = xadd(asum, xdiv((double)c, S3d));
+            asum = smooth ? asum + g.ent_alpha[g.cl_ent[i]] : xadd(asum, xdiv((double)c, S3d));
             csum += c;
         }
         g.alpha_sum[cell] = asum;

@@ -41,6 +41,11 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
                                   const double* imb_sums, double* forces, double* torques, double* diag,
                                   cudaStream_t stream);
 
+cudaError_t launch_adjoint_seed(const psc_adjoint_args& a, cudaStream_t stream);
+cudaError_t launch_adjoint_step(const psc_adjoint_args& a, cudaStream_t stream);
+cudaError_t launch_adjoint_geometry_grad(const psc_geometry& g, const psc_adjoint_args& a, double* part,
+                                         double* grad, cudaStream_t stream);
+
 // exclusive scan of int32 counts -> int32 offsets, out has n + 1 entries
 size_t scan_tmp_bytes(int64_t n);
 cudaError_t scan_exclusive_i32(const int32_t* in, int32_t* out, int64_t n, void* tmp, cudaStream_t stream);

@@ -219,7 +219,8 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restr
                 uz_d = (double)uz;
                 const int s = W.subsamples;
                 const int s3 = s * s * s;
-                const R al = (R)W.level[cell] / (R)s3;
+                // uint8 clipped sample level; without one (smooth geometry) the FP64 solid field
+                const R al = W.level ? (R)W.level[cell] / (R)s3 : (R)W.solid[cell];
                 solid_d = (double)al;
                 if (do_collide) {
                     const R tau = (R)W.tau;

@@ -124,7 +124,12 @@ class DeviceGeometry:
 
     CHUNK_ENTRIES = 4096
 
-    def __init__(self, shape, subsamples: int, device, want_level: bool):
+    def __init__(self, shape, subsamples: int, device, want_level: bool, smooth_eps: float = 0.0):
+        self.smooth_eps = float(smooth_eps)
+        if self.smooth_eps < 0.0:
+            raise ValueError("smooth_eps must be >= 0")
+        if self.smooth_eps > 0.0:
+            want_level = False  # a smooth solid fraction has no integer level
         self.nx, self.ny, self.nz = (int(v) for v in shape)
         self.subsamples = int(subsamples)
         if self.subsamples < 1 or self.subsamples > 16:
@@ -151,6 +156,8 @@ class DeviceGeometry:
         self.ent_cnt = torch.zeros(0, dtype=torch.int16, device=device)
         self.cl_pid = torch.zeros(0, dtype=i32, device=device)
         self.cl_cnt = torch.zeros(0, dtype=torch.int16, device=device)
+        self.ent_alpha = None
+        self.cl_ent = None
         self.chunk_partials = torch.zeros(0, dtype=f64, device=device)
         self.n_entries = 0
         self.n_chunks = 0
@@ -192,6 +199,9 @@ class DeviceGeometry:
         g.solid = vp(self.solid)
         g.level = vp(self.level)
         g.scan_tmp = vp(self.scan_tmp)
+        g.smooth_eps = self.smooth_eps
+        g.ent_alpha = vp(self.ent_alpha)
+        g.cl_ent = vp(self.cl_ent)
         return g
 
     def rebuild(self) -> None:
@@ -211,6 +221,9 @@ class DeviceGeometry:
             self.ent_cnt = torch.zeros(cap, dtype=torch.int16, device=self.device)
             self.cl_pid = torch.zeros(cap, dtype=torch.int32, device=self.device)
             self.cl_cnt = torch.zeros(cap, dtype=torch.int16, device=self.device)
+            if self.smooth_eps > 0.0:
+                self.ent_alpha = torch.zeros(cap, dtype=torch.float64, device=self.device)
+                self.cl_ent = torch.zeros(cap, dtype=torch.int32, device=self.device)
             self.cap_entries = cap
         if self.n_chunks > self.cap_chunks:
             cap = int(self.n_chunks * 1.25) + 16
@@ -373,9 +386,7 @@ class LatticeWindow:
     def step(self, flags: int) -> None:
         """One fused pull-stream + collide step; swaps the population buffers."""
         self.ensure_fields(imb=bool(flags & nat.STEP_IMB), moments=bool(flags & nat.STEP_MOMENTS))
-        if self.store == nat.STORE_F64_EXACT and self.solid_ptr is None:
-            raise RuntimeError("geometry not bound")
-        if self.store != nat.STORE_F64_EXACT and self.level_ptr is None:
+        if self.solid_ptr is None:
             raise RuntimeError("geometry not bound")
         fl = flags | nat.STEP_COLLIDE | (nat.STEP_MOVING if self.moving else 0)
         nat.call("psc_step", self.store, vp(self.windows(self.cur)), 1, self.tiles, fl, 0,

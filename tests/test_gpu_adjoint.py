@@ -1,0 +1,81 @@
+"""GPU adjoint of the permeability: vs the FP64 reference adjoint, vs central finite differences,
+FP32 vs FP64, checkpoint independence, and the torch.autograd wrapper."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import psc_adjoint as adj
+
+pytestmark = pytest.mark.gpu
+
+PARTS = np.array([[4.3, 5.1, 4.8, 2.2] + [0.0] * 6,
+                  [7.9, 3.2, 6.1, 1.7] + [0.0] * 6,
+                  [2.0, 8.5, 1.0, 1.9] + [0.0] * 6])
+N, S, EPS, TAU, F, STEPS = 10, 2, 0.05, 0.8, (1e-4, 0.0, 0.0), 25
+
+
+def problem(precision="fp64", every=7, steps=STEPS):
+    from particuology_hydraulic_penalty_b200.adjoint import PermeabilityProblem
+
+    return PermeabilityProblem(N, tau=TAU, force=F, subsamples=S, eps=EPS, steps=steps, checkpoint_every=every,
+                               precision=precision)
+
+
+def test_gpu_fp64_adjoint_matches_reference_adjoint():
+    Kref, gref, _ = adj.gradient(PARTS, N, S, EPS, TAU, F, STEPS)
+    pr = problem("fp64")
+    K = pr.forward(PARTS)
+    g = pr.backward()
+    assert abs(K - Kref) <= 1e-12 * abs(Kref)
+    assert np.linalg.norm(g - gref) <= 1e-9 * np.linalg.norm(gref)
+
+
+def test_gpu_adjoint_matches_central_differences():
+    pr = problem("fp64")
+    pr.forward(PARTS)
+    g = pr.backward()
+    h = 1e-3
+    worst = 0.0
+    for p in range(len(PARTS)):
+        for k in range(4):
+            pp = PARTS.copy()
+            pp[p, k] += h
+            pm = PARTS.copy()
+            pm[p, k] -= h
+            fd = (problem("fp64").forward(pp) - problem("fp64").forward(pm)) / (2 * h)
+            worst = max(worst, abs(fd - g[p, k]) / abs(fd))
+    assert worst <= 1e-3
+
+
+def test_fp32_adjoint_close_to_fp64():
+    p64 = problem("fp64")
+    p64.forward(PARTS)
+    g64 = p64.backward()
+    p32 = problem("fp32")
+    p32.forward(PARTS)
+    g32 = p32.backward()
+    assert np.linalg.norm(g32 - g64) <= 1e-3 * np.linalg.norm(g64)
+
+
+def test_checkpoint_interval_does_not_change_gradient():
+    a = problem("fp64", every=7)
+    a.forward(PARTS)
+    b = problem("fp64", every=STEPS)
+    b.forward(PARTS)
+    assert np.array_equal(a.backward(), b.backward())
+
+
+def test_autograd_function():
+    from particuology_hydraulic_penalty_b200.adjoint import permeability
+
+    pr = problem("fp64")
+    centres = torch.tensor(PARTS[:, 0:3], dtype=torch.float64, requires_grad=True)
+    radii = torch.tensor(PARTS[:, 3], dtype=torch.float64, requires_grad=True)
+    K = permeability(centres, radii, pr, template=PARTS)
+    (2.0 * K).backward()
+    ref = problem("fp64")
+    ref.forward(PARTS)
+    g = ref.backward()
+    assert np.allclose(centres.grad.numpy(), 2.0 * g[:, 0:3], rtol=1e-12, atol=0)
+    assert np.allclose(radii.grad.numpy(), 2.0 * g[:, 3], rtol=1e-12, atol=0)
