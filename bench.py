@@ -324,6 +324,7 @@ def run_ours(args):
     batch = PscBatch(specs, precision=args.precision, graph_steps=args.graph_steps)
     clocks = ClockSampler(local)
     clocks.start()
+    batch.prepare()  # graph capture of both buffer parities happens here, outside the timed region
     batch.run(args.warmup)
     torch.cuda.synchronize()
     ms = timed(lambda: batch.run(args.steps), world)

@@ -60,6 +60,19 @@ extern "C" {
 #define PSC_STEP_REDUCE 8u  /* write per-tile FP64 reduction partials */
 #define PSC_STEP_MOVING 16u /* some window has PSC_WIN_MOVING: compile in the u_s path */
 
+/* ---- kernel variants of the deviation modes ----------------------------- */
+#define PSC_KERNEL_AUTO 0   /* the library's choice */
+#define PSC_KERNEL_DIRECT 1 /* per-thread coalesced pulls (any window) */
+#define PSC_KERNEL_TMA 2    /* bulk-copy (TMA) row staging in shared memory */
+
+/* Launch configuration of psc_step_ex(). */
+typedef struct psc_launch {
+    int32_t grid_ctas;        /* persistent grid size; 0 = SM count x occupancy */
+    int32_t cells_per_thread; /* 1, 2 or 4; the windows must be planned with tile_cells = 256 x this */
+    int32_t kernel;           /* PSC_KERNEL_* (PSC_STORE_F64_EXACT always runs its own kernel) */
+    int32_t stages;           /* TMA pipeline depth (0 = default) */
+} psc_launch;
+
 /* ---- per-window flags --------------------------------------------------- */
 #define PSC_WIN_MOVING 1 /* read the solid velocity field us (else u_s = 0) */
 
@@ -176,7 +189,9 @@ size_t psc_scan_tmp_bytes(int64_t n);
 
 /* ---- tiles and windows -------------------------------------------------- */
 /* Fill tile_cells / tile_begin / tile_count of h_windows (HOST array) and
- * return the total tile count in *h_total_tiles. */
+ * return the total tile count in *h_total_tiles.  tile_cells: 0 (= 256),
+ * 256, 512 or 1024 (256 x cells per thread).  A window must hold fewer than
+ * 2^31 / 19 cells (32-bit population offsets). */
 int psc_plan_tiles(struct psc_window* h_windows, int nwin, int tile_cells, int64_t* h_total_tiles);
 
 /* Equilibrium at rho = 1, u = 0 in the given storage mode
@@ -202,6 +217,10 @@ int psc_solid_velocity(const psc_geometry* h_geo, int us_type, void* us, void* s
  * grid_ctas = 0 picks a persistent grid (a multiple of the SM count). */
 int psc_step(int store, const struct psc_window* d_windows, int nwin, int64_t total_tiles,
              unsigned flags, int grid_ctas, void* stream);
+/* psc_step with an explicit launch configuration (kernel variant, cells per
+ * thread, grid); cfg may be NULL for the defaults. */
+int psc_step_ex(int store, const struct psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
+                const psc_launch* cfg, void* stream);
 /* Sum the per-tile partials of each window in a fixed order (deterministic)
  * into out[nwin][PSC_NRED] (device). */
 int psc_reduce_windows(const struct psc_window* d_windows, int nwin, double* out, void* stream);

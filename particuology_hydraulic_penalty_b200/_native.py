@@ -99,6 +99,13 @@ class PscAdjointArgs(ctypes.Structure):
     ]
 
 
+KERNEL_AUTO, KERNEL_DIRECT, KERNEL_TMA = 0, 1, 2
+
+
+class PscLaunch(ctypes.Structure):
+    _fields_ = [("grid_ctas", c_int32), ("cells_per_thread", c_int32), ("kernel", c_int32), ("stages", c_int32)]
+
+
 # name -> (restype, argtypes); every function of include/psc_b200.h
 SIGNATURES = {
     "psc_abi_version": (c_int, []),
@@ -113,6 +120,7 @@ SIGNATURES = {
     "psc_geometry_build": (c_int, [POINTER(PscGeometry), c_void_p]),
     "psc_solid_velocity": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p]),
     "psc_step": (c_int, [c_int, c_void_p, c_int, c_int64, c_uint, c_int, c_void_p]),
+    "psc_step_ex": (c_int, [c_int, c_void_p, c_int, c_int64, c_uint, POINTER(PscLaunch), c_void_p]),
     "psc_reduce_windows": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "psc_particle_loads": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),

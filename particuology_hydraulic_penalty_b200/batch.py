@@ -49,10 +49,15 @@ class PscBatch:
     """
 
     def __init__(self, specs, precision: str = "fp32", store_scale: float | None = None, graph_steps: int = 20,
-                 grid_ctas: int = 0, device=None, tau=None, force=None, subsamples=None):
+                 grid_ctas: int = 0, device=None, tau=None, force=None, subsamples=None, cells_per_thread: int = 1,
+                 kernel: int = nat.KERNEL_AUTO):
         self.device = require_cuda(device)
         self.store = store_mode(precision)
         self.precision = precision
+        self.cells_per_thread = 1 if self.store == nat.STORE_F64_EXACT else int(cells_per_thread)
+        if self.cells_per_thread not in (1, 2, 4):
+            raise ValueError("cells_per_thread must be 1, 2 or 4")
+        self.kernel = int(kernel)
         self.graph_steps = int(graph_steps)
         if self.graph_steps % 2:
             raise ValueError("graph_steps must be even (the graph must end on the buffer parity it started on)")
@@ -100,7 +105,7 @@ class PscBatch:
             for k, w in enumerate(self.windows):
                 arr[k] = w.struct(parity)
             total = ctypes.c_int64(0)
-            nat.call("psc_plan_tiles", arr, nwin, 0, ctypes.byref(total))
+            nat.call("psc_plan_tiles", arr, nwin, nat.STEP_THREADS * self.cells_per_thread, ctypes.byref(total))
             if self.partials is None:
                 self.total_tiles = int(total.value)
                 self.partials = torch.zeros(self.total_tiles * nat.NRED, dtype=torch.float64, device=self.device)
@@ -120,8 +125,9 @@ class PscBatch:
         return int(self.cells.sum())
 
     def _launch(self, flags: int) -> None:
-        nat.call("psc_step", self.store, vp(self._tables[self.parity]), self.nwin, self.total_tiles,
-                 flags, self.grid_ctas, stream_handle(self.device))
+        cfg = nat.PscLaunch(self.grid_ctas, self.cells_per_thread, self.kernel, 0)
+        nat.call("psc_step_ex", self.store, vp(self._tables[self.parity]), self.nwin, self.total_tiles,
+                 flags, ctypes.byref(cfg), stream_handle(self.device))
 
     def step_once(self, flags: int = 0) -> None:
         """One collide-stream step of every window (one kernel launch)."""
@@ -146,16 +152,27 @@ class PscBatch:
         self.parity = parity0
         self._graphs[parity0] = g
 
+    def prepare(self) -> None:
+        """Warm the launch path and capture the step graphs of both buffer parities (no timed work)."""
+        with torch.cuda.device(self.device):
+            if self.steps_done == 0:
+                self.step_once()
+            if self.graph_steps > 0:
+                for _ in range(2):
+                    if self.parity not in self._graphs:
+                        self._capture()
+                    self.parity ^= 1  # capture does not run anything; visit the other parity
+                for w in self.windows:
+                    w.cur = self.parity
+
     def run(self, steps: int) -> None:
         """Advance every window by ``steps`` steps (graph replays plus a remainder)."""
         steps = int(steps)
         with torch.cuda.device(self.device):
             if self.graph_steps > 0 and steps >= self.graph_steps:
-                if self.steps_done == 0:
-                    self.step_once()  # warm the launch path before capture
-                    steps -= 1
-                if self.parity not in self._graphs:
-                    self._capture()
+                if self.steps_done == 0 or len(self._graphs) < 2:
+                    steps -= 1 if self.steps_done == 0 else 0
+                    self.prepare()
                 graph = self._graphs[self.parity]  # an even step count returns to this parity
                 reps = steps // self.graph_steps
                 for _ in range(reps):

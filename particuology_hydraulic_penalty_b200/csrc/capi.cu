@@ -84,14 +84,16 @@ size_t psc_scan_tmp_bytes(int64_t n) { return scan_tmp_bytes(n < 0 ? 0 : n); }
 int psc_plan_tiles(psc_window* h_windows, int nwin, int tile_cells, int64_t* h_total_tiles) {
     if (!h_windows || nwin <= 0 || !h_total_tiles) return fail(PSC_E_INVALID, "psc_plan_tiles: bad arguments");
     if (tile_cells == 0) tile_cells = STEP_THREADS;
-    if (tile_cells != STEP_THREADS)
-        return fail(PSC_E_UNSUPPORTED, "psc_plan_tiles: tile_cells must be 0 or " + std::to_string(STEP_THREADS));
+    if (tile_cells != STEP_THREADS && tile_cells != 2 * STEP_THREADS && tile_cells != 4 * STEP_THREADS)
+        return fail(PSC_E_UNSUPPORTED, "psc_plan_tiles: tile_cells must be 0, 256, 512 or 1024");
     int64_t begin = 0;
     for (int w = 0; w < nwin; ++w) {
         psc_window& W = h_windows[w];
         int st = check_extent(W.nx, W.ny, W.nz, "psc_plan_tiles");
         if (st) return st;
         const int64_t n = (int64_t)W.nx * W.ny * W.nz;
+        if (n * 19 >= (1ll << 31))
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_tiles: a window must hold fewer than 2^31/19 cells");
         W.tile_cells = tile_cells;
         W.tile_begin = begin;
         W.tile_count = (n + tile_cells - 1) / tile_cells;
@@ -143,14 +145,34 @@ int psc_solid_velocity(const psc_geometry* h_geo, int us_type, void* us, void* s
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_solid_velocity");
 }
 
-int psc_step(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags, int grid_ctas,
-             void* stream) {
+int psc_step_ex(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
+                const psc_launch* cfg, void* stream) {
     if (!valid_store(store)) return fail(PSC_E_INVALID, "psc_step: unknown storage mode");
     if (!d_windows || nwin <= 0 || total_tiles < 0) return fail(PSC_E_INVALID, "psc_step: bad window list");
-    if (grid_ctas < 0) return fail(PSC_E_INVALID, "psc_step: grid_ctas must be >= 0");
-    cudaError_t e = launch_step(store, d_windows, nwin, total_tiles, flags, (flags & PSC_STEP_MOVING) != 0,
-                                grid_ctas, as_stream(stream));
+    psc_launch c = {0, 1, PSC_KERNEL_AUTO, 0};
+    if (cfg) c = *cfg;
+    if (c.grid_ctas < 0) return fail(PSC_E_INVALID, "psc_step: grid_ctas must be >= 0");
+    if (c.cells_per_thread != 1 && c.cells_per_thread != 2 && c.cells_per_thread != 4)
+        return fail(PSC_E_INVALID, "psc_step: cells_per_thread must be 1, 2 or 4");
+    const bool moving = (flags & PSC_STEP_MOVING) != 0;
+    cudaError_t e;
+    if (store == PSC_STORE_F64_EXACT) {
+        if (c.cells_per_thread != 1)
+            return fail(PSC_E_UNSUPPORTED, "psc_step: PSC_STORE_F64_EXACT runs one cell per thread");
+        e = launch_step(store, d_windows, nwin, total_tiles, flags, moving, c.grid_ctas, as_stream(stream));
+    } else if (c.kernel == PSC_KERNEL_AUTO || c.kernel == PSC_KERNEL_DIRECT) {
+        e = launch_step_fast(store, d_windows, nwin, total_tiles, flags, moving, c.cells_per_thread, c.grid_ctas,
+                             as_stream(stream));
+    } else {
+        return fail(PSC_E_UNSUPPORTED, "psc_step: unknown kernel variant");
+    }
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_step");
+}
+
+int psc_step(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags, int grid_ctas,
+             void* stream) {
+    psc_launch c = {grid_ctas, 1, PSC_KERNEL_AUTO, 0};
+    return psc_step_ex(store, d_windows, nwin, total_tiles, flags, &c, stream);
 }
 
 int psc_reduce_windows(const psc_window* d_windows, int nwin, double* out, void* stream) {

@@ -16,131 +16,9 @@
 // so each population crosses HBM exactly once per step.
 #include "collide.cuh"
 #include "internal.cuh"
+#include "step_common.cuh"
 
 namespace psc {
-
-template <int STORE>
-struct StoreTraits;
-template <>
-struct StoreTraits<PSC_STORE_F64_EXACT> {
-    using T = double;
-    using R = double;
-    using O = double;
-    static constexpr bool exact = true;
-    static constexpr bool scaled = false;
-};
-template <>
-struct StoreTraits<PSC_STORE_F64> {
-    using T = double;
-    using R = double;
-    using O = double;
-    static constexpr bool exact = false;
-    static constexpr bool scaled = false;
-};
-template <>
-struct StoreTraits<PSC_STORE_F32> {
-    using T = float;
-    using R = float;
-    using O = float;
-    static constexpr bool exact = false;
-    static constexpr bool scaled = false;
-};
-template <>
-struct StoreTraits<PSC_STORE_F16> {
-    using T = __half;
-    using R = float;
-    using O = float;
-    static constexpr bool exact = false;
-    static constexpr bool scaled = true;
-};
-template <>
-struct StoreTraits<PSC_STORE_BF16> {
-    using T = __nv_bfloat16;
-    using R = float;
-    using O = float;
-    static constexpr bool exact = false;
-    static constexpr bool scaled = true;
-};
-
-__device__ __forceinline__ double ld_pop(const double* p) { return __ldg(p); }
-__device__ __forceinline__ float ld_pop(const float* p) { return __ldg(p); }
-__device__ __forceinline__ float ld_pop(const __half* p) { return __half2float(__ldg(p)); }
-__device__ __forceinline__ float ld_pop(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
-
-__device__ __forceinline__ void st_pop(double* p, double v) { *p = v; }
-__device__ __forceinline__ void st_pop(float* p, float v) { *p = v; }
-__device__ __forceinline__ void st_pop(__half* p, float v) { *p = __float2half_rn(v); }
-__device__ __forceinline__ void st_pop(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
-
-// Offset (in cells) from x to x - c_i for direction i, given the wrapped
-// neighbour offsets of this cell.
-struct NbrOffsets {
-    int32_t xm, xp, ym, yp, zm, zp;  // to ix-1, ix+1, iy-1, iy+1, iz-1, iz+1
-};
-
-__device__ __forceinline__ NbrOffsets nbr_offsets(uint32_t ix, uint32_t iy, uint32_t iz, int nx, int ny, int nz) {
-    NbrOffsets o;
-    const int32_t nyz = ny * nz;
-    o.xm = ix == 0 ? (nx - 1) * nyz : -nyz;
-    o.xp = ix == (uint32_t)(nx - 1) ? -(nx - 1) * nyz : nyz;
-    o.ym = iy == 0 ? (ny - 1) * nz : -nz;
-    o.yp = iy == (uint32_t)(ny - 1) ? -(ny - 1) * nz : nz;
-    o.zm = iz == 0 ? nz - 1 : -1;
-    o.zp = iz == (uint32_t)(nz - 1) ? -(nz - 1) : 1;
-    return o;
-}
-
-template <int I>
-__device__ __forceinline__ int32_t pull_offset(const NbrOffsets& o) {
-    // source of direction I at x is x - c_I
-    return (cxv(I) == 1 ? o.xm : (cxv(I) == -1 ? o.xp : 0)) + (cyv(I) == 1 ? o.ym : (cyv(I) == -1 ? o.yp : 0)) +
-           (czv(I) == 1 ? o.zm : (czv(I) == -1 ? o.zp : 0));
-}
-
-template <typename T, typename R, int I>
-struct PullLoop {
-    __device__ __forceinline__ static void run(R* f, const T* src, size_t N, uint32_t cell, const NbrOffsets& o,
-                                               R inv_scale, bool scaled) {
-        PullLoop<T, R, I - 1>::run(f, src, N, cell, o, inv_scale, scaled);
-        const R v = ld_pop(src + (size_t)(I - 1) * N + (size_t)((int64_t)cell + pull_offset<I - 1>(o)));
-        f[I - 1] = scaled ? v * inv_scale : v;
-    }
-};
-template <typename T, typename R>
-struct PullLoop<T, R, 0> {
-    __device__ __forceinline__ static void run(R*, const T*, size_t, uint32_t, const NbrOffsets&, R, bool) {}
-};
-
-__device__ __forceinline__ int find_window(const psc_window* wins, const int64_t* s_begin, int nwin, int64_t t) {
-    int lo = 0, hi = nwin - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        const int64_t b = s_begin ? s_begin[mid] : wins[mid].tile_begin;
-        if (b <= t) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-template <int NV>
-__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double (*s_red)[NV], double* out) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double x = v[k];
-#pragma unroll
-        for (int s = 16; s > 0; s >>= 1) x += __shfl_xor_sync(0xffffffffu, x, s);
-        if (lane == 0) s_red[warp][k] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x < NV) {
-        double acc = 0.0;
-        const int nw = blockDim.x >> 5;
-        for (int w = 0; w < nw; ++w) acc += s_red[w][threadIdx.x];
-        out[threadIdx.x] = acc;
-    }
-    __syncthreads();
-}
 
 template <int STORE, bool MOVING>
 __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restrict__ wins, int nwin,

@@ -1,0 +1,298 @@
+// Throughput kernel for the deviation storage modes (F64 / F32 / F16 / BF16).
+//
+// Same step as k_step (pull-stream + PSC-IMB collide, src/lbm_dem/psc3d.py:
+// 208-246), organised to keep the SM's issue slots for the collision:
+//  * each persistent CTA owns a CONTIGUOUS run of tiles, so it meets a new
+//    window only a few times; per-window constants (Guo terms, 1/tau, the
+//    solid-level -> B and (1-B)/tau tables, mixed-radix tile stride) are built
+//    once in shared memory when the window changes;
+//  * a tile is CPT x 256 consecutive cells; a thread owns CPT of them,
+//    issues all 19 x CPT pulls before computing, and advances its (ix, iy, iz)
+//    between cells by a carry-add instead of integer division;
+//  * 32-bit population offsets, reciprocal instead of division.
+#include "step_common.cuh"
+
+namespace psc {
+
+template <typename T, typename R, typename O>
+struct FastWin {
+    const T* src;
+    T* dst;
+    const uint8_t* level;
+    const double* solid;
+    const O* us;
+    O* imb;
+    O* mom;
+    double* partials;
+    int64_t tile_begin;
+    int64_t tile_end;
+    uint32_t nx, ny, nz, N;
+    uint32_t step_x, step_y, step_z;  // blockDim cells as a mixed-radix (x, y, z) increment
+    int32_t tile_cells;
+    int32_t moving;
+    R scale, inv_scale;
+    WinConst<R> c;
+    R Blut[256];
+    R kblut[256];
+    R alut[256];  // clipped solid fraction per level
+    R tau;
+};
+
+template <typename T, typename R, typename O>
+__device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool moving_launch) {
+    // one warp fills the scalar part, all threads the level tables
+    if (threadIdx.x == 0) {
+        s.src = reinterpret_cast<const T*>(W.f_src);
+        s.dst = reinterpret_cast<T*>(W.f_dst);
+        s.level = W.level;
+        s.solid = W.solid;
+        s.us = reinterpret_cast<const O*>(W.us);
+        s.imb = reinterpret_cast<O*>(W.imb);
+        s.mom = reinterpret_cast<O*>(W.moments);
+        s.partials = W.partials;
+        s.tile_begin = W.tile_begin;
+        s.tile_end = W.tile_begin + W.tile_count;
+        s.nx = W.nx;
+        s.ny = W.ny;
+        s.nz = W.nz;
+        s.N = (uint32_t)W.nx * W.ny * W.nz;
+        const uint32_t q = blockDim.x / (uint32_t)W.nz;
+        s.step_z = blockDim.x % (uint32_t)W.nz;
+        s.step_y = q % (uint32_t)W.ny;
+        s.step_x = q / (uint32_t)W.ny;
+        s.tile_cells = W.tile_cells;
+        s.moving = (moving_launch && (W.flags & PSC_WIN_MOVING) && W.us != nullptr) ? 1 : 0;
+        s.scale = (R)W.store_scale;
+        s.inv_scale = (R)(1.0 / W.store_scale);
+        s.tau = (R)W.tau;
+        make_win_const(s.c, W.tau, W.force[0], W.force[1], W.force[2]);
+    }
+    const int S = W.subsamples;
+    const int S3 = S * S * S;
+    if (W.level) {
+        for (int l = threadIdx.x; l <= S3 && l < 256; l += blockDim.x) {
+            const double al = (double)l / (double)S3;
+            const double B = al / (al + W.tau * (1.0 - al) + 1.0e-14);
+            s.Blut[l] = (R)B;
+            s.kblut[l] = (R)((1.0 - B) / W.tau);
+            s.alut[l] = (R)al;
+        }
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ R fast_rcp(R x);
+template <>
+__device__ __forceinline__ float fast_rcp<float>(float x) {
+    return __frcp_rn(x);
+}
+template <>
+__device__ __forceinline__ double fast_rcp<double>(double x) {
+    return __drcp_rn(x);
+}
+
+template <int STORE, bool MOVING, int CPT>
+__global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __restrict__ wins, int nwin,
+                                                             int64_t total_tiles, unsigned flags) {
+    using TR = StoreTraits<STORE>;
+    using T = typename TR::T;
+    using R = typename TR::R;
+    using O = typename TR::O;
+    __shared__ FastWin<T, R, O> sw;
+    __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
+    const bool do_collide = flags & PSC_STEP_COLLIDE;
+    const bool do_imb = do_collide && (flags & PSC_STEP_IMB);
+    const bool do_mom = flags & PSC_STEP_MOMENTS;
+    const bool do_red = flags & PSC_STEP_REDUCE;
+    const int64_t t0 = (total_tiles * (int64_t)blockIdx.x) / gridDim.x;
+    const int64_t t1 = (total_tiles * ((int64_t)blockIdx.x + 1)) / gridDim.x;
+    int64_t win_end = -1;
+    for (int64_t t = t0; t < t1; ++t) {
+        if (t >= win_end) {  // block-uniform: entering a new window
+            __syncthreads();
+            const int wi = find_window(wins, nullptr, nwin, t);
+            load_fast_win(sw, wins[wi], MOVING);
+            __syncthreads();
+            win_end = sw.tile_end;
+        }
+        const uint32_t N = sw.N, nx = sw.nx, ny = sw.ny, nz = sw.nz;
+        const uint32_t base = (uint32_t)((t - sw.tile_begin) * sw.tile_cells);
+        uint32_t cell = base + threadIdx.x;
+        uint32_t iz = cell % nz, rr = cell / nz, iy = rr % ny, ix = rr / ny;
+        const T* src = sw.src;
+        R f[CPT][Q];
+        uint32_t cells[CPT];
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            cells[k] = cell;
+            if (cell < N) {
+                const int32_t nyz = (int32_t)(ny * nz);
+                const int32_t xm = ix == 0 ? (int32_t)(nx - 1) * nyz : -nyz;
+                const int32_t xp = ix == nx - 1 ? -(int32_t)(nx - 1) * nyz : nyz;
+                const int32_t ym = iy == 0 ? (int32_t)(ny - 1) * (int32_t)nz : -(int32_t)nz;
+                const int32_t yp = iy == ny - 1 ? -(int32_t)(ny - 1) * (int32_t)nz : (int32_t)nz;
+                const int32_t zm = iz == 0 ? (int32_t)nz - 1 : -1;
+                const int32_t zp = iz == nz - 1 ? -(int32_t)(nz - 1) : 1;
+                const T* sc = src + cell;
+                uint32_t plane = 0;
+#pragma unroll
+                for (int i = 0; i < Q; ++i) {
+                    const int32_t o = (cxv(i) == 1 ? xm : (cxv(i) == -1 ? xp : 0)) +
+                                      (cyv(i) == 1 ? ym : (cyv(i) == -1 ? yp : 0)) +
+                                      (czv(i) == 1 ? zm : (czv(i) == -1 ? zp : 0));
+                    f[k][i] = ld_pop(sc + (int64_t)(int32_t)(plane + (uint32_t)o));
+                    plane += N;
+                }
+            }
+            // advance (ix, iy, iz) by blockDim cells with carries
+            cell += blockDim.x;
+            iz += sw.step_z;
+            const uint32_t cz = iz >= nz;
+            iz -= cz ? nz : 0;
+            iy += sw.step_y + cz;
+            const uint32_t cy = iy >= ny;
+            iy -= cy ? ny : 0;
+            ix += sw.step_x + cy;
+        }
+        double red[PSC_NRED];
+#pragma unroll
+        for (int q = 0; q < PSC_NRED; ++q) red[q] = 0.0;
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const uint32_t c = cells[k];
+            if (c >= N) continue;
+            R* g = f[k];
+            if (TR::scaled) {
+#pragma unroll
+                for (int i = 0; i < Q; ++i) g[i] *= sw.inv_scale;
+            }
+            R B, kb, al;
+            if (sw.level) {
+                const uint8_t lv = sw.level[c];
+                B = sw.Blut[lv];
+                kb = sw.kblut[lv];
+                al = sw.alut[lv];
+            } else {
+                al = (R)sw.solid[c];
+                B = al * fast_rcp<R>(al + sw.tau * (R(1) - al) + R(1.0e-14));
+                kb = (R(1) - B) * sw.c.inv_tau;
+            }
+            R usx = R(0), usy = R(0), usz = R(0);
+            const bool moving = MOVING && sw.moving;
+            if (moving) {
+                usx = (R)sw.us[c];
+                usy = (R)sw.us[(size_t)N + c];
+                usz = (R)sw.us[2 * (size_t)N + c];
+            }
+            R mom[4], imb[3] = {R(0), R(0), R(0)};
+            const R drho = (((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7]))) +
+                           (((g[8] + g[9]) + (g[10] + g[11])) + ((g[12] + g[13]) + (g[14] + g[15]))) +
+                           ((g[16] + g[17]) + g[18]);
+            const R irho = fast_rcp<R>(R(1) + drho);
+            if (do_collide) {
+                if (do_imb || do_red) {
+                    if (moving) collide_fast2<R, MOVING, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+                    else collide_fast2<R, false, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+                } else {
+                    if (moving) collide_fast2<R, MOVING, false>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+                    else collide_fast2<R, false, false>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+                }
+                T* dst = sw.dst + c;
+                uint32_t plane = 0;
+#pragma unroll
+                for (int i = 0; i < Q; ++i) {
+                    st_pop(dst + plane, TR::scaled ? g[i] * sw.scale : g[i]);
+                    plane += N;
+                }
+                if (do_imb) {
+                    sw.imb[c] = (O)imb[0];
+                    sw.imb[(size_t)N + c] = (O)imb[1];
+                    sw.imb[2 * (size_t)N + c] = (O)imb[2];
+                }
+            } else {
+                const R mx = ((g[1] - g[2]) + (g[7] - g[8])) + ((g[9] - g[10]) + (g[11] - g[12])) + (g[13] - g[14]);
+                const R my = ((g[3] - g[4]) + (g[7] - g[8])) + ((g[10] - g[9]) + (g[15] - g[16])) + (g[17] - g[18]);
+                const R mz = ((g[5] - g[6]) + (g[11] - g[12])) + ((g[14] - g[13]) + (g[15] - g[16])) + (g[18] - g[17]);
+                mom[0] = drho;
+                mom[1] = (mx + R(0.5) * sw.c.fx) * irho;
+                mom[2] = (my + R(0.5) * sw.c.fy) * irho;
+                mom[3] = (mz + R(0.5) * sw.c.fz) * irho;
+            }
+            if (do_mom) {
+                sw.mom[c] = (O)(R(1) + mom[0]);
+                sw.mom[(size_t)N + c] = (O)mom[1];
+                sw.mom[2 * (size_t)N + c] = (O)mom[2];
+                sw.mom[3 * (size_t)N + c] = (O)mom[3];
+            }
+            if (do_red) {
+                const double solid = (double)al;
+                const double fl = 1.0 - solid;
+                const double rho_d = 1.0 + (double)mom[0];
+                const double ux = (double)mom[1], uy = (double)mom[2], uz = (double)mom[3];
+                red[PSC_RED_RHO] += rho_d;
+                red[PSC_RED_UX] += ux;
+                red[PSC_RED_UY] += uy;
+                red[PSC_RED_UZ] += uz;
+                red[PSC_RED_FLUID_UX] += fl * ux;
+                red[PSC_RED_FLUID_UY] += fl * uy;
+                red[PSC_RED_FLUID_UZ] += fl * uz;
+                red[PSC_RED_FLUID] += fl;
+                red[PSC_RED_IMBX] += (double)imb[0];
+                red[PSC_RED_IMBY] += (double)imb[1];
+                red[PSC_RED_IMBZ] += (double)imb[2];
+                red[PSC_RED_NONFINITE] += (isfinite(rho_d) && isfinite(ux) && isfinite(uy) && isfinite(uz)) ? 0.0 : 1.0;
+                red[PSC_RED_SOLID] += solid;
+            }
+        }
+        if (do_red) block_reduce_store<PSC_NRED>(red, s_red, sw.partials + (t - sw.tile_begin) * PSC_NRED);
+    }
+}
+
+template <int STORE, bool MOVING, int CPT>
+static cudaError_t launch_fast_t(const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
+                                 int grid_ctas, cudaStream_t stream) {
+    if (grid_ctas <= 0) {
+        static int per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int& occ = per_sm[dev & 7];
+        if (occ == 0) {
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_fast<STORE, MOVING, CPT>,
+                                                                          STEP_THREADS, 0);
+            if (e != cudaSuccess) return e;
+            if (occ <= 0) occ = 1;
+        }
+        const int64_t g = (int64_t)sm_count() * occ;
+        grid_ctas = (int)(total_tiles < g ? total_tiles : g);
+    }
+    if (grid_ctas <= 0) return cudaSuccess;
+    k_step_fast<STORE, MOVING, CPT><<<grid_ctas, STEP_THREADS, 0, stream>>>(d_windows, nwin, total_tiles, flags);
+    return cudaGetLastError();
+}
+
+template <int STORE>
+static cudaError_t launch_fast_s(const psc_window* d, int nwin, int64_t tiles, unsigned flags, bool moving, int cpt,
+                                 int grid, cudaStream_t s) {
+    switch (cpt) {
+        case 1: return moving ? launch_fast_t<STORE, true, 1>(d, nwin, tiles, flags, grid, s)
+                              : launch_fast_t<STORE, false, 1>(d, nwin, tiles, flags, grid, s);
+        case 2: return moving ? launch_fast_t<STORE, true, 2>(d, nwin, tiles, flags, grid, s)
+                              : launch_fast_t<STORE, false, 2>(d, nwin, tiles, flags, grid, s);
+        case 4: return moving ? launch_fast_t<STORE, true, 4>(d, nwin, tiles, flags, grid, s)
+                              : launch_fast_t<STORE, false, 4>(d, nwin, tiles, flags, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_step_fast(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
+                             bool moving, int cpt, int grid_ctas, cudaStream_t stream) {
+    switch (store) {
+        case PSC_STORE_F64: return launch_fast_s<PSC_STORE_F64>(d_windows, nwin, total_tiles, flags, moving, cpt, grid_ctas, stream);
+        case PSC_STORE_F32: return launch_fast_s<PSC_STORE_F32>(d_windows, nwin, total_tiles, flags, moving, cpt, grid_ctas, stream);
+        case PSC_STORE_F16: return launch_fast_s<PSC_STORE_F16>(d_windows, nwin, total_tiles, flags, moving, cpt, grid_ctas, stream);
+        case PSC_STORE_BF16: return launch_fast_s<PSC_STORE_BF16>(d_windows, nwin, total_tiles, flags, moving, cpt, grid_ctas, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace psc
