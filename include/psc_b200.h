@@ -70,7 +70,8 @@ typedef struct psc_launch {
     int32_t grid_ctas;        /* persistent grid size; 0 = SM count x occupancy */
     int32_t cells_per_thread; /* 1, 2 or 4; the windows must be planned with tile_cells = 256 x this */
     int32_t kernel;           /* PSC_KERNEL_* (PSC_STORE_F64_EXACT always runs its own kernel) */
-    int32_t stages;           /* TMA pipeline depth (0 = default) */
+    int32_t stages;           /* TMA pipeline depth: 2, 3 or 4 (0 = 3) */
+    int32_t stage_bytes;      /* TMA: shared-memory bytes per stage, from psc_plan_row_tiles */
 } psc_launch;
 
 /* ---- per-window flags --------------------------------------------------- */
@@ -193,6 +194,17 @@ size_t psc_scan_tmp_bytes(int64_t n);
  * 256, 512 or 1024 (256 x cells per thread).  A window must hold fewer than
  * 2^31 / 19 cells (32-bit population offsets). */
 int psc_plan_tiles(struct psc_window* h_windows, int nwin, int tile_cells, int64_t* h_total_tiles);
+
+/* Row tiles for PSC_KERNEL_TMA: a tile is `rows` whole z-rows of one x-plane
+ * (rows = 0: chosen per window for ~512-768 cells per tile).  elem_bytes is
+ * the storage element size; every window needs nz * elem_bytes % 16 == 0 and
+ * 16-byte aligned population buffers (bulk-copy rule).  Returns the total
+ * tile count and the shared-memory bytes one stage needs. */
+int psc_plan_row_tiles(struct psc_window* h_windows, int nwin, int rows, int elem_bytes, int64_t* h_total_tiles,
+                       int32_t* h_stage_bytes);
+/* Device-side status word: non-zero after a kernel gave up a bounded wait
+ * (0x101 producer, 0x102 drain, 0x103 consumer).  Synchronises. */
+int psc_device_status(int* h_status, int clear);
 
 /* Equilibrium at rho = 1, u = 0 in the given storage mode
  * (the reference's initial state, psc3d.py:136-140). */

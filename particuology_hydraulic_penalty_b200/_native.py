@@ -103,7 +103,8 @@ KERNEL_AUTO, KERNEL_DIRECT, KERNEL_TMA = 0, 1, 2
 
 
 class PscLaunch(ctypes.Structure):
-    _fields_ = [("grid_ctas", c_int32), ("cells_per_thread", c_int32), ("kernel", c_int32), ("stages", c_int32)]
+    _fields_ = [("grid_ctas", c_int32), ("cells_per_thread", c_int32), ("kernel", c_int32), ("stages", c_int32),
+                ("stage_bytes", c_int32)]
 
 
 # name -> (restype, argtypes); every function of include/psc_b200.h
@@ -115,6 +116,8 @@ SIGNATURES = {
     "psc_adjoint_args_size": (c_size_t, []),
     "psc_scan_tmp_bytes": (c_size_t, [c_int64]),
     "psc_plan_tiles": (c_int, [POINTER(PscWindow), c_int, c_int, POINTER(c_int64)]),
+    "psc_plan_row_tiles": (c_int, [POINTER(PscWindow), c_int, c_int, c_int, POINTER(c_int64), POINTER(c_int32)]),
+    "psc_device_status": (c_int, [POINTER(c_int), c_int]),
     "psc_init_equilibrium": (c_int, [c_int, c_double, c_void_p, c_int64, c_void_p]),
     "psc_geometry_plan": (c_int, [POINTER(PscGeometry), c_void_p]),
     "psc_geometry_build": (c_int, [POINTER(PscGeometry), c_void_p]),

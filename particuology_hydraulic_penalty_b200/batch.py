@@ -50,7 +50,7 @@ class PscBatch:
 
     def __init__(self, specs, precision: str = "fp32", store_scale: float | None = None, graph_steps: int = 20,
                  grid_ctas: int = 0, device=None, tau=None, force=None, subsamples=None, cells_per_thread: int = 1,
-                 kernel: int = nat.KERNEL_AUTO):
+                 kernel: int = nat.KERNEL_AUTO, tile_rows: int = 0, stages: int = 3):
         self.device = require_cuda(device)
         self.store = store_mode(precision)
         self.precision = precision
@@ -58,6 +58,11 @@ class PscBatch:
         if self.cells_per_thread not in (1, 2, 4):
             raise ValueError("cells_per_thread must be 1, 2 or 4")
         self.kernel = int(kernel)
+        if self.kernel == nat.KERNEL_TMA and self.store == nat.STORE_F64_EXACT:
+            raise ValueError("the TMA kernel runs the deviation storage modes")
+        self.tile_rows = int(tile_rows)
+        self.stages = int(stages)
+        self.stage_bytes = 0
         self.graph_steps = int(graph_steps)
         if self.graph_steps % 2:
             raise ValueError("graph_steps must be even (the graph must end on the buffer parity it started on)")
@@ -105,7 +110,13 @@ class PscBatch:
             for k, w in enumerate(self.windows):
                 arr[k] = w.struct(parity)
             total = ctypes.c_int64(0)
-            nat.call("psc_plan_tiles", arr, nwin, nat.STEP_THREADS * self.cells_per_thread, ctypes.byref(total))
+            if self.kernel == nat.KERNEL_TMA:
+                sb = ctypes.c_int32(0)
+                elem = self.windows[0].f[0].element_size()
+                nat.call("psc_plan_row_tiles", arr, nwin, self.tile_rows, elem, ctypes.byref(total), ctypes.byref(sb))
+                self.stage_bytes = int(sb.value)
+            else:
+                nat.call("psc_plan_tiles", arr, nwin, nat.STEP_THREADS * self.cells_per_thread, ctypes.byref(total))
             if self.partials is None:
                 self.total_tiles = int(total.value)
                 self.partials = torch.zeros(self.total_tiles * nat.NRED, dtype=torch.float64, device=self.device)
@@ -125,7 +136,7 @@ class PscBatch:
         return int(self.cells.sum())
 
     def _launch(self, flags: int) -> None:
-        cfg = nat.PscLaunch(self.grid_ctas, self.cells_per_thread, self.kernel, 0)
+        cfg = nat.PscLaunch(self.grid_ctas, self.cells_per_thread, self.kernel, self.stages, self.stage_bytes)
         nat.call("psc_step_ex", self.store, vp(self._tables[self.parity]), self.nwin, self.total_tiles,
                  flags, ctypes.byref(cfg), stream_handle(self.device))
 

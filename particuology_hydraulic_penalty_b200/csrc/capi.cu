@@ -103,6 +103,52 @@ int psc_plan_tiles(psc_window* h_windows, int nwin, int tile_cells, int64_t* h_t
     return PSC_OK;
 }
 
+int psc_plan_row_tiles(psc_window* h_windows, int nwin, int rows, int elem_bytes, int64_t* h_total_tiles,
+                       int32_t* h_stage_bytes) {
+    if (!h_windows || nwin <= 0 || !h_total_tiles || !h_stage_bytes || rows < 0)
+        return fail(PSC_E_INVALID, "psc_plan_row_tiles: bad arguments");
+    if (elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8)
+        return fail(PSC_E_INVALID, "psc_plan_row_tiles: elem_bytes must be 2, 4 or 8");
+    int64_t begin = 0;
+    int64_t stage = 0;
+    for (int w = 0; w < nwin; ++w) {
+        psc_window& W = h_windows[w];
+        int st = check_extent(W.nx, W.ny, W.nz, "psc_plan_row_tiles");
+        if (st) return st;
+        const int64_t n = (int64_t)W.nx * W.ny * W.nz;
+        if (n * 19 >= (1ll << 31))
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: a window must hold fewer than 2^31/19 cells");
+        if (((int64_t)W.nz * elem_bytes) % 16 != 0)
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: nz * elem_bytes must be a multiple of 16 (window " +
+                                               std::to_string(w) + ")");
+        if ((reinterpret_cast<uintptr_t>(W.f_src) | reinterpret_cast<uintptr_t>(W.f_dst)) % 16 != 0)
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: population buffers must be 16-byte aligned");
+        int ty = rows;
+        if (ty == 0) {
+            ty = (640 + W.nz / 2) / W.nz;
+            if (ty < 1) ty = 1;
+        }
+        if (ty > W.ny) ty = W.ny;
+        const int64_t bytes = (int64_t)19 * ty * W.nz * elem_bytes;
+        if (bytes > 96 * 1024)
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: a row tile needs more than 96 kB of shared memory");
+        W.tile_cells = ty * W.nz;
+        W.tile_begin = begin;
+        W.tile_count = (int64_t)W.nx * ((W.ny + ty - 1) / ty);
+        begin += W.tile_count;
+        if (bytes > stage) stage = bytes;
+    }
+    *h_total_tiles = begin;
+    *h_stage_bytes = (int32_t)((stage + 127) / 128 * 128);
+    return PSC_OK;
+}
+
+int psc_device_status(int* h_status, int clear) {
+    if (!h_status) return fail(PSC_E_INVALID, "psc_device_status: null output");
+    cudaError_t e = read_device_status(h_status, clear != 0);
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_device_status");
+}
+
 int psc_init_equilibrium(int store, double store_scale, void* f, int64_t ncells, void* stream) {
     if (!valid_store(store)) return fail(PSC_E_INVALID, "psc_init_equilibrium: unknown storage mode");
     if (!f || ncells <= 0) return fail(PSC_E_INVALID, "psc_init_equilibrium: null buffer or empty lattice");
@@ -149,7 +195,7 @@ int psc_step_ex(int store, const psc_window* d_windows, int nwin, int64_t total_
                 const psc_launch* cfg, void* stream) {
     if (!valid_store(store)) return fail(PSC_E_INVALID, "psc_step: unknown storage mode");
     if (!d_windows || nwin <= 0 || total_tiles < 0) return fail(PSC_E_INVALID, "psc_step: bad window list");
-    psc_launch c = {0, 1, PSC_KERNEL_AUTO, 0};
+    psc_launch c = {0, 1, PSC_KERNEL_AUTO, 0, 0};
     if (cfg) c = *cfg;
     if (c.grid_ctas < 0) return fail(PSC_E_INVALID, "psc_step: grid_ctas must be >= 0");
     if (c.cells_per_thread != 1 && c.cells_per_thread != 2 && c.cells_per_thread != 4)
@@ -163,6 +209,13 @@ int psc_step_ex(int store, const psc_window* d_windows, int nwin, int64_t total_
     } else if (c.kernel == PSC_KERNEL_AUTO || c.kernel == PSC_KERNEL_DIRECT) {
         e = launch_step_fast(store, d_windows, nwin, total_tiles, flags, moving, c.cells_per_thread, c.grid_ctas,
                              as_stream(stream));
+    } else if (c.kernel == PSC_KERNEL_TMA) {
+        const int stages = c.stages == 0 ? 3 : c.stages;
+        if (stages < 2 || stages > 4) return fail(PSC_E_INVALID, "psc_step: TMA stages must be 2, 3 or 4");
+        if (c.stage_bytes <= 0 || c.stage_bytes % 16 != 0 || (int64_t)stages * c.stage_bytes > 200 * 1024)
+            return fail(PSC_E_INVALID, "psc_step: bad TMA stage_bytes (use psc_plan_row_tiles)");
+        e = launch_step_tma(store, d_windows, nwin, total_tiles, flags, moving, c.grid_ctas, stages,
+                            (uint32_t)c.stage_bytes, as_stream(stream));
     } else {
         return fail(PSC_E_UNSUPPORTED, "psc_step: unknown kernel variant");
     }
@@ -171,7 +224,7 @@ int psc_step_ex(int store, const psc_window* d_windows, int nwin, int64_t total_
 
 int psc_step(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags, int grid_ctas,
              void* stream) {
-    psc_launch c = {grid_ctas, 1, PSC_KERNEL_AUTO, 0};
+    psc_launch c = {grid_ctas, 1, PSC_KERNEL_AUTO, 0, 0};
     return psc_step_ex(store, d_windows, nwin, total_tiles, flags, &c, stream);
 }
 

@@ -29,6 +29,9 @@ cudaError_t launch_step(int store, const psc_window* d_windows, int nwin, int64_
                         bool moving, int grid_ctas, cudaStream_t stream);
 cudaError_t launch_step_fast(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
                              bool moving, int cpt, int grid_ctas, cudaStream_t stream);
+cudaError_t launch_step_tma(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
+                            bool moving, int grid_ctas, int stages, uint32_t stage_bytes, cudaStream_t stream);
+cudaError_t read_device_status(int* out, bool clear);
 cudaError_t launch_reduce_windows(const psc_window* d_windows, int nwin, double* out, cudaStream_t stream);
 cudaError_t launch_init_equilibrium(int store, double scale, void* f, int64_t ncells, cudaStream_t stream);
 cudaError_t launch_stream_push(int store, double scale, const void* src, double* dst, int nx, int ny, int nz,

@@ -54,6 +54,23 @@ __device__ __forceinline__ float ld_pop(const float* p) { return __ldg(p); }
 __device__ __forceinline__ float ld_pop(const __half* p) { return __half2float(__ldg(p)); }
 __device__ __forceinline__ float ld_pop(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
 
+template <typename R>
+__device__ __forceinline__ R fast_rcp(R x);
+template <>
+__device__ __forceinline__ float fast_rcp<float>(float x) {
+    return __frcp_rn(x);
+}
+template <>
+__device__ __forceinline__ double fast_rcp<double>(double x) {
+    return __drcp_rn(x);
+}
+
+// plain (shared-memory) reads of a stored population
+__device__ __forceinline__ double ld_smem_pop(const double* p) { return *p; }
+__device__ __forceinline__ float ld_smem_pop(const float* p) { return *p; }
+__device__ __forceinline__ float ld_smem_pop(const __half* p) { return __half2float(*p); }
+__device__ __forceinline__ float ld_smem_pop(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+
 __device__ __forceinline__ void st_pop(double* p, double v) { *p = v; }
 __device__ __forceinline__ void st_pop(float* p, float v) { *p = v; }
 __device__ __forceinline__ void st_pop(__half* p, float v) { *p = __float2half_rn(v); }

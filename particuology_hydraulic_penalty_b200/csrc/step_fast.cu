@@ -80,17 +80,6 @@ __device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool mov
     }
 }
 
-template <typename R>
-__device__ __forceinline__ R fast_rcp(R x);
-template <>
-__device__ __forceinline__ float fast_rcp<float>(float x) {
-    return __frcp_rn(x);
-}
-template <>
-__device__ __forceinline__ double fast_rcp<double>(double x) {
-    return __drcp_rn(x);
-}
-
 template <int STORE, bool MOVING, int CPT>
 __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __restrict__ wins, int nwin,
                                                              int64_t total_tiles, unsigned flags) {

@@ -69,3 +69,72 @@ def test_batch_loads_match_dropin():
         s.collide_stream_psc()
     assert np.array_equal(F, s.hydro_forces)
     assert np.array_equal(T, s.hydro_torques)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64", "bf16"])
+def test_cells_per_thread_variants_identical(precision):
+    """The multi-cell thread variants run the same per-cell arithmetic: bit-identical fields."""
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    wins = small_windows()
+    specs = [WindowSpec(w.n, w.particles, tau=0.8, force=(1e-6, 2e-7, 0.0), subsamples=4) for w in wins]
+    ref = None
+    for cpt in (1, 2, 4):
+        b = PscBatch(specs, precision=precision, graph_steps=0, cells_per_thread=cpt)
+        b.run(7)
+        fields = [b.velocity_field(k) for k in range(len(wins))]
+        red = b.observe()
+        if ref is None:
+            ref = (fields, red)
+        else:
+            for a, c in zip(fields, ref[0]):
+                assert np.array_equal(a, c)
+            # per-tile FP64 partials group cells differently: equal to round-off
+            assert np.allclose(red, ref[1], rtol=1e-13, atol=1e-13 * np.abs(ref[1]).max())
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64", "fp16"])
+@pytest.mark.parametrize("rows", [0, 3])
+def test_tma_kernel_matches_direct(precision, rows):
+    """The TMA-staged kernel computes the same per-cell arithmetic as the direct one."""
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    wins = small_windows()
+    specs = [WindowSpec(w.n, w.particles, tau=0.8, force=(1e-6, 0.0, 3e-7), subsamples=4) for w in wins]
+    d = PscBatch(specs, precision=precision, graph_steps=0)
+    d.run(9)
+    t = PscBatch(specs, precision=precision, graph_steps=4, kernel=nat.KERNEL_TMA, tile_rows=rows, stages=3)
+    t.run(9)
+    for k in range(len(wins)):
+        assert np.array_equal(t.velocity_field(k), d.velocity_field(k))
+    rd, rt = d.observe(), t.observe()
+    assert np.allclose(rt, rd, rtol=1e-13, atol=1e-13 * np.abs(rd).max())
+    status = ctypes_status()
+    assert status == 0
+
+
+def ctypes_status():
+    import ctypes
+
+    from particuology_hydraulic_penalty_b200 import _native as nat
+
+    v = ctypes.c_int(0)
+    nat.call("psc_device_status", ctypes.byref(v), 1)
+    return v.value
+
+
+def test_tma_kernel_with_reductions_and_loads():
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    w = small_windows()[2]
+    spec = WindowSpec(w.n, w.particles, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=4)
+    d = PscBatch([spec], precision="fp32", graph_steps=0)
+    t = PscBatch([spec], precision="fp32", graph_steps=0, kernel=nat.KERNEL_TMA, stages=2)
+    d.run(4)
+    t.run(4)
+    Fd, Td = d.loads()[0]
+    Ft, Tt = t.loads()[0]
+    assert np.array_equal(Fd, Ft) and np.array_equal(Td, Tt)
+    assert ctypes_status() == 0
