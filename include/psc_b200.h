@@ -196,7 +196,8 @@ size_t psc_scan_tmp_bytes(int64_t n);
 int psc_plan_tiles(struct psc_window* h_windows, int nwin, int tile_cells, int64_t* h_total_tiles);
 
 /* Row tiles for PSC_KERNEL_TMA: a tile is `rows` whole z-rows of one x-plane
- * (rows = 0: chosen per window for ~512-768 cells per tile).  elem_bytes is
+ * (rows = 0: chosen per window for ~48 kB of populations per stage; rows =
+ * -1: each window keeps the rows preset as tile_cells = rows * nz).  elem_bytes is
  * the storage element size; every window needs nz * elem_bytes % 16 == 0 and
  * 16-byte aligned population buffers (bulk-copy rule).  Returns the total
  * tile count and the shared-memory bytes one stage needs. */
@@ -245,6 +246,21 @@ int psc_reduce_windows(const struct psc_window* d_windows, int nwin, double* out
  * [P][3], torques [P][3] and diag [PSC_NDIAG]. */
 int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb, double* chunk_partials,
                        const double* imb_sums, double* forces, double* torques, double* diag, void* stream);
+
+/* ---- particle loads without caller scratch (no counterpart in the reference)
+ * For callers that cannot allocate device memory -- a solver embedded in a
+ * program that owns the device memory budget, or a coupling loop that must
+ * not call cudaMalloc after start-up (it synchronises the device).  Same
+ * results as psc_particle_loads(), but the per-chunk partial sums live in a
+ * fixed array inside the library: PSC_LOADS_STATIC_MAX_CHUNKS x 6 doubles
+ * (768 KiB) held by every GPU that loads the library until exit.
+ * h_geo->capacity_chunks must not exceed PSC_LOADS_STATIC_MAX_CHUNKS
+ * (PSC_E_CAPACITY otherwise).  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress) -- make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race. */
+#define PSC_LOADS_STATIC_MAX_CHUNKS 16384
+int psc_particle_loads_static(const psc_geometry* h_geo, int imb_type, const void* imb, const double* imb_sums,
+                              double* forces, double* torques, double* diag, void* stream);
 
 /* ---- adjoint of the permeability (no counterpart in the reference) ------- */
 /* Seed: lambda_T = dK/dS_T for K = kappa sum (1 - solid) u.dir of the

@@ -52,6 +52,7 @@ DIAG_FORCE_SUM = (3, 4, 5)
 NDIAG = 6
 
 STEP_THREADS = 256
+LOADS_STATIC_MAX_CHUNKS = 16384
 
 
 class NativeLibraryError(RuntimeError):
@@ -127,6 +128,8 @@ SIGNATURES = {
     "psc_reduce_windows": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "psc_particle_loads": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),
+    "psc_particle_loads_static": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                          c_void_p, c_void_p]),
     "psc_adjoint_seed": (c_int, [POINTER(PscAdjointArgs), c_void_p]),
     "psc_adjoint_step": (c_int, [POINTER(PscAdjointArgs), c_void_p]),
     "psc_adjoint_geometry_grad": (c_int, [POINTER(PscGeometry), POINTER(PscAdjointArgs), c_void_p, c_void_p,
