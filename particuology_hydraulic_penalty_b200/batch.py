@@ -61,6 +61,7 @@ class PscBatch:
         if self.kernel == nat.KERNEL_TMA and self.store == nat.STORE_F64_EXACT:
             raise ValueError("the TMA kernel runs the deviation storage modes")
         self.tile_rows = int(tile_rows)
+        self.rows_per_window: list[int] | None = None  # per-window TMA rows (autotuner), else tile_rows
         self.stages = int(stages)
         self.stage_bytes = 0
         self.graph_steps = int(graph_steps)
@@ -109,11 +110,14 @@ class PscBatch:
             arr = (nat.PscWindow * nwin)()
             for k, w in enumerate(self.windows):
                 arr[k] = w.struct(parity)
+                if self.rows_per_window is not None:
+                    arr[k].tile_cells = int(self.rows_per_window[k]) * w.nz
             total = ctypes.c_int64(0)
             if self.kernel == nat.KERNEL_TMA:
                 sb = ctypes.c_int32(0)
                 elem = self.windows[0].f[0].element_size()
-                nat.call("psc_plan_row_tiles", arr, nwin, self.tile_rows, elem, ctypes.byref(total), ctypes.byref(sb))
+                rows = -1 if self.rows_per_window is not None else self.tile_rows
+                nat.call("psc_plan_row_tiles", arr, nwin, rows, elem, ctypes.byref(total), ctypes.byref(sb))
                 self.stage_bytes = int(sb.value)
             else:
                 nat.call("psc_plan_tiles", arr, nwin, nat.STEP_THREADS * self.cells_per_thread, ctypes.byref(total))
@@ -126,6 +130,25 @@ class PscBatch:
             tables.append(struct_to_device(arr, self.device))
         self._tables = tables
         self._graphs = {}
+
+    def configure(self, kernel: int, cells_per_thread: int = 1, tile_rows: int = 0, stages: int = 3,
+                  rows_per_window=None, grid_ctas: int | None = None) -> None:
+        """Switch the launch configuration (populations are kept; graphs are re-captured)."""
+        if kernel == nat.KERNEL_TMA and self.store == nat.STORE_F64_EXACT:
+            raise ValueError("the TMA kernel runs the deviation storage modes")
+        self.kernel = int(kernel)
+        self.cells_per_thread = int(cells_per_thread)
+        self.tile_rows = int(tile_rows)
+        self.stages = int(stages)
+        self.rows_per_window = None if rows_per_window is None else [int(r) for r in rows_per_window]
+        if grid_ctas is not None:
+            self.grid_ctas = int(grid_ctas)
+        self._build_tables()
+
+    def launch_config(self) -> dict:
+        return {"kernel": {nat.KERNEL_AUTO: "direct", nat.KERNEL_DIRECT: "direct", nat.KERNEL_TMA: "tma"}[self.kernel],
+                "cells_per_thread": self.cells_per_thread, "tile_rows": self.tile_rows, "stages": self.stages,
+                "rows_per_window": self.rows_per_window, "stage_bytes": self.stage_bytes}
 
     @property
     def nwin(self) -> int:

@@ -105,7 +105,7 @@ int psc_plan_tiles(psc_window* h_windows, int nwin, int tile_cells, int64_t* h_t
 
 int psc_plan_row_tiles(psc_window* h_windows, int nwin, int rows, int elem_bytes, int64_t* h_total_tiles,
                        int32_t* h_stage_bytes) {
-    if (!h_windows || nwin <= 0 || !h_total_tiles || !h_stage_bytes || rows < 0)
+    if (!h_windows || nwin <= 0 || !h_total_tiles || !h_stage_bytes || rows < -1)
         return fail(PSC_E_INVALID, "psc_plan_row_tiles: bad arguments");
     if (elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8)
         return fail(PSC_E_INVALID, "psc_plan_row_tiles: elem_bytes must be 2, 4 or 8");
@@ -121,17 +121,32 @@ int psc_plan_row_tiles(psc_window* h_windows, int nwin, int rows, int elem_bytes
         if (((int64_t)W.nz * elem_bytes) % 16 != 0)
             return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: nz * elem_bytes must be a multiple of 16 (window " +
                                                std::to_string(w) + ")");
+        const int geo_bytes = W.level ? 1 : 8;  // uint8 level or FP64 solid rides in the stage
+        if (!W.level && !W.solid) return fail(PSC_E_INVALID, "psc_plan_row_tiles: window without level or solid");
+        if (((int64_t)W.nz * geo_bytes) % 16 != 0)
+            return fail(PSC_E_UNSUPPORTED, std::string("psc_plan_row_tiles: the ") + (W.level ? "uint8 level" : "FP64 solid") +
+                                               " rows need nz * " + std::to_string(geo_bytes) +
+                                               " to be a multiple of 16 (window " + std::to_string(w) + ")");
+        if ((reinterpret_cast<uintptr_t>(W.level ? (const void*)W.level : (const void*)W.solid)) % 16 != 0)
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: level / solid buffers must be 16-byte aligned");
         if ((reinterpret_cast<uintptr_t>(W.f_src) | reinterpret_cast<uintptr_t>(W.f_dst)) % 16 != 0)
             return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: population buffers must be 16-byte aligned");
         int ty = rows;
-        if (ty == 0) {
-            ty = (640 + W.nz / 2) / W.nz;
+        if (ty == -1) {  // keep the rows preset in tile_cells (= rows * nz)
+            if (W.tile_cells <= 0 || W.tile_cells % W.nz != 0)
+                return fail(PSC_E_INVALID, "psc_plan_row_tiles: rows = -1 needs tile_cells = rows * nz preset");
+            ty = W.tile_cells / W.nz;
+        }
+        if (ty == 0) {  // ~24 kB per stage: three stages and two CTAs fit on one SM
+            ty = (int)((24 * 1024) / ((int64_t)W.nz * (19 * elem_bytes + geo_bytes)));
             if (ty < 1) ty = 1;
         }
         if (ty > W.ny) ty = W.ny;
-        const int64_t bytes = (int64_t)19 * ty * W.nz * elem_bytes;
+        const int64_t bytes = (int64_t)ty * W.nz * (19 * elem_bytes + geo_bytes);
         if (bytes > 96 * 1024)
             return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: a row tile needs more than 96 kB of shared memory");
+        if (ty * W.nz > 4096)
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: more than 4096 cells per row tile");
         W.tile_cells = ty * W.nz;
         W.tile_begin = begin;
         W.tile_count = (int64_t)W.nx * ((W.ny + ty - 1) / ty);

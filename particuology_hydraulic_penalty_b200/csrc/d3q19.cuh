@@ -32,6 +32,15 @@ PSC_HD constexpr int czv(int i) {
     return (i == 5 || i == 11 || i == 14 || i == 15 || i == 18) ? 1
            : (i == 6 || i == 12 || i == 13 || i == 16 || i == 17) ? -1 : 0;
 }
+// Runtime lookups (one lane per direction): table reads instead of branch chains.
+PSC_HD int cxv_rt(int i) {
+    const int8_t t[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    return t[i];
+}
+PSC_HD int cyv_rt(int i) {
+    const int8_t t[19] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1};
+    return t[i];
+}
 PSC_HD constexpr int cv(int axis, int i) { return axis == 0 ? cxv(i) : (axis == 1 ? cyv(i) : czv(i)); }
 PSC_HD constexpr int opp(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
 

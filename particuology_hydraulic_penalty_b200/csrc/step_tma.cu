@@ -12,6 +12,9 @@
 // flight per CTA, so the SM has tens of kB of HBM reads outstanding without
 // spending registers or issue slots on global loads.
 //
+// The tile's uint8 solid level (or FP64 smooth solid fraction) rides in the
+// same stage, so the consumers touch global memory only to store.
+//
 // Every mbarrier wait is bounded: after PSC_WAIT_LIMIT polls the kernel
 // records an error in psc_device_status (read with psc_device_status()),
 // stops issuing work, waits (bounded) for its own copies in flight and returns.
@@ -105,7 +108,7 @@ __device__ __forceinline__ void row_tile(const psc_window& W, int64_t t, uint32_
 }
 
 template <int STORE, bool MOVING, int STAGES>
-__global__ void __launch_bounds__(TMA_THREADS) k_step_tma(const psc_window* __restrict__ wins, int nwin,
+__global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* __restrict__ wins, int nwin,
                                                            int64_t total_tiles, unsigned flags, uint32_t stage_bytes) {
     using TR = StoreTraits<STORE>;
     using T = typename TR::T;
@@ -131,15 +134,24 @@ __global__ void __launch_bounds__(TMA_THREADS) k_step_tma(const psc_window* __re
     __syncthreads();
 
     if (producer) {
-        if (threadIdx.x != TMA_CONSUMERS) return;  // one elected producer lane
+        // The whole producer warp works each tile: lane 0 arms the stage's
+        // mbarrier with the byte count, then lane i < 19 issues the bulk copy
+        // (or two, across a y wrap) of population i and lane 19 the tile's
+        // solid level, so no lane does more than a few address computations.
+        const int lane = threadIdx.x - TMA_CONSUMERS;
         int64_t win_end = -1;
         int wi = 0;
         uint32_t issued = 0;
+        bool stop = false;
         for (int64_t t = t0; t < t1; ++t, ++issued) {
             const int s = (int)(issued % STAGES);
             if (issued >= (uint32_t)STAGES) {
-                if (!mbar_wait(&empty[s], ((issued / STAGES) - 1) & 1, 0x101) || s_abort) {
-                    s_abort = 1;
+                int ok = 1;
+                if (lane == 0) ok = mbar_wait(&empty[s], ((issued / STAGES) - 1) & 1, 0x101) && !s_abort;
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    if (lane == 0) s_abort = 1;
+                    stop = true;
                     break;
                 }
             }
@@ -151,19 +163,19 @@ __global__ void __launch_bounds__(TMA_THREADS) k_step_tma(const psc_window* __re
             uint32_t ix, y0, rows;
             row_tile(W, t, ix, y0, rows);
             const uint32_t nx = W.nx, ny = W.ny, nz = W.nz;
-            const size_t N = (size_t)nx * ny * nz;
             const uint32_t row_bytes = nz * (uint32_t)sizeof(T);
             const uint32_t pop_bytes = (uint32_t)(W.tile_cells) * (uint32_t)sizeof(T);  // ty * nz * sizeof(T)
             unsigned char* stage = smem + (size_t)s * stage_bytes;
-            mbar_expect_tx(&full[s], 19u * rows * row_bytes);
-            const T* src = reinterpret_cast<const T*>(W.f_src);
-#pragma unroll 1
-            for (int i = 0; i < Q; ++i) {
-                const int cx = cxv(i), cy = cyv(i);
-                const uint32_t xs = (uint32_t)(((int)ix - cx + (int)nx) % (int)nx);
+            if (lane == 0) mbar_expect_tx(&full[s], 19u * rows * row_bytes + rows * nz * (W.level ? 1u : 8u));
+            __syncwarp();
+            if (lane < Q) {
+                const int i = lane;
+                const int cx = cxv_rt(i), cy = cyv_rt(i);
+                const uint32_t xs = cx == 1 ? (ix == 0 ? nx - 1 : ix - 1) : (cx == -1 ? (ix + 1 == nx ? 0 : ix + 1) : ix);
                 int ys = (int)y0 - cy;
                 unsigned char* dst = stage + (size_t)i * pop_bytes;
-                const T* plane = src + (size_t)i * N + (size_t)xs * ny * nz;
+                const T* plane = reinterpret_cast<const T*>(W.f_src) + (size_t)i * ((size_t)nx * ny * nz) +
+                                 (size_t)xs * ny * nz;
                 uint32_t r0 = 0;
                 if (ys < 0) {  // first row wraps to ny - 1
                     bulk_g2s(dst, plane + (size_t)(ny - 1) * nz, row_bytes, &full[s]);
@@ -175,12 +187,21 @@ __global__ void __launch_bounds__(TMA_THREADS) k_step_tma(const psc_window* __re
                 if (n_in) bulk_g2s(dst + (size_t)r0 * row_bytes, plane + (size_t)ys * nz, n_in * row_bytes, &full[s]);
                 const uint32_t rest = rows - r0 - n_in;  // rows wrapping to y = 0
                 if (rest) bulk_g2s(dst + (size_t)(r0 + n_in) * row_bytes, plane, rest * row_bytes, &full[s]);
+            } else if (lane == Q) {
+                // the tile's own solid level (uint8) or smooth solid fraction (double), no shift
+                const size_t base = ((size_t)ix * ny + y0) * nz;
+                unsigned char* gdst = stage + (size_t)19 * pop_bytes;
+                if (W.level) bulk_g2s(gdst, W.level + base, rows * nz, &full[s]);
+                else bulk_g2s(gdst, W.solid + base, rows * nz * 8u, &full[s]);
             }
         }
+        (void)stop;
         // drain: wait (bounded) for every issued stage to land before the CTA may exit
-        const uint32_t n_issued = issued;
-        for (uint32_t k = (n_issued > (uint32_t)STAGES ? n_issued - STAGES : 0); k < n_issued; ++k)
-            mbar_wait(&full[k % STAGES], (k / STAGES) & 1, 0x102);
+        if (lane == 0) {
+            const uint32_t n_issued = issued;
+            for (uint32_t k = (n_issued > (uint32_t)STAGES ? n_issued - STAGES : 0); k < n_issued; ++k)
+                mbar_wait(&full[k % STAGES], (k / STAGES) & 1, 0x102);
+        }
         return;
     }
 
@@ -250,6 +271,7 @@ __global__ void __launch_bounds__(TMA_THREADS) k_step_tma(const psc_window* __re
         const uint32_t ncell = rows * nz;
         const uint32_t pop_elems = sw.ty * nz;
         const T* st = reinterpret_cast<const T*>(smem + (size_t)s * stage_bytes);
+        const unsigned char* st_geo = smem + (size_t)s * stage_bytes + (size_t)19 * pop_elems * sizeof(T);
         const uint32_t base = (ix * ny + y0) * nz;
         double red[PSC_NRED];
 #pragma unroll
@@ -276,12 +298,12 @@ __global__ void __launch_bounds__(TMA_THREADS) k_step_tma(const psc_window* __re
             const uint32_t cell = base + c;
             R B, kb, al;
             if (sw.level) {
-                const uint8_t lv = sw.level[cell];
+                const uint8_t lv = st_geo[c];
                 B = sw.Blut[lv];
                 kb = sw.kblut[lv];
                 al = sw.alut[lv];
             } else {
-                al = (R)sw.solid[cell];
+                al = (R)reinterpret_cast<const double*>(st_geo)[c];
                 B = al * fast_rcp<R>(al + sw.tau * (R(1) - al) + R(1.0e-14));
                 kb = (R(1) - B) * sw.c.inv_tau;
             }

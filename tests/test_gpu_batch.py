@@ -100,7 +100,11 @@ def test_tma_kernel_matches_direct(precision, rows):
     from particuology_hydraulic_penalty_b200 import _native as nat
     from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
 
-    wins = small_windows()
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+
+    # row tiles carry the uint8 level by bulk copy: nz must be a multiple of 16
+    wins = [wgen.make_window(16, "skeleton", 1), wgen.make_window(32, "passive", 2),
+            wgen.make_window(48, "preloaded", 3)]
     specs = [WindowSpec(w.n, w.particles, tau=0.8, force=(1e-6, 0.0, 3e-7), subsamples=4) for w in wins]
     d = PscBatch(specs, precision=precision, graph_steps=0)
     d.run(9)
@@ -128,7 +132,7 @@ def test_tma_kernel_with_reductions_and_loads():
     from particuology_hydraulic_penalty_b200 import _native as nat
     from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
 
-    w = small_windows()[2]
+    w = small_windows()[1]
     spec = WindowSpec(w.n, w.particles, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=4)
     d = PscBatch([spec], precision="fp32", graph_steps=0)
     t = PscBatch([spec], precision="fp32", graph_steps=0, kernel=nat.KERNEL_TMA, stages=2)

@@ -176,3 +176,31 @@ def test_nan_particle_rejected():
 
     with pytest.raises(ValueError):
         SparsePscD3Q19(8, [Particle3D(float("nan"), 4.0, 4.0, 2.0)])
+
+
+def test_probe_cli_matches_oracle(tmp_path):
+    """The GPU probe (fp64-exact) reproduces the CSV quantities the reference computes, on a synthetic dump."""
+    import csv
+
+    from particuology_hydraulic_penalty_b200 import probe
+
+    dump = tmp_path / "w.dump"
+    dump.write_text("ITEM: ATOMS id type x y z radius\n"
+                    "1 1 0.0045 0.0045 0.0045 0.0021\n2 1 0.0009 0.0011 0.0082 0.0016\n"
+                    "3 2 0.0071 0.0022 0.0030 0.0004\n")
+    args = ["--case", "skeleton", "--resolution", "20", "--source-dump", str(dump), "--steps", "6",
+            "--outdir", str(tmp_path), "--quiet", "--subsamples", "2"]
+    row = probe.main(args)
+    rows = probe.parse_dump(dump)
+    parts = probe.to_particle_array(rows, 20)
+    o = orc.OracleSolver(20, parts, tau=0.72, subsamples=2, body_force_z=2e-7, static_geometry=True)
+    last = None
+    for _ in range(6):
+        last = o.collide_stream_psc()
+    d = orc.darcy_permeability(o.solid, o.uz, 0.72, 2e-7)
+    assert abs(row["permeability_lu"] - d["permeability_lu"]) <= 1e-12 * abs(d["permeability_lu"])
+    assert row["porosity_psc"] == d["porosity_psc"]
+    assert row["max_uz"] == float(np.max(o.uz))
+    with (tmp_path / "skeleton_n020.csv").open() as f:
+        got = list(csv.DictReader(f))
+    assert len(got) == 1 and set(got[0]) == set(probe.FIELDS)
