@@ -50,7 +50,14 @@ struct StoreTraits<PSC_STORE_BF16> {
 };
 
 __device__ __forceinline__ double ld_pop(const double* p) { return __ldg(p); }
-__device__ __forceinline__ float ld_pop(const float* p) { return __ldg(p); }
+// FP32 pulls ask L2 to fetch the whole 256-byte line pair: consecutive tiles of
+// a CTA read consecutive rows, so the neighbouring sectors are used next
+// (measured +1.3 % on the 24-window batch).
+__device__ __forceinline__ float ld_pop(const float* p) {
+    float v;
+    asm volatile("ld.global.nc.L2::256B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
 __device__ __forceinline__ float ld_pop(const __half* p) { return __half2float(__ldg(p)); }
 __device__ __forceinline__ float ld_pop(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
 
@@ -73,8 +80,9 @@ __device__ __forceinline__ float ld_smem_pop(const __nv_bfloat16* p) { return __
 
 __device__ __forceinline__ void st_pop(double* p, double v) { *p = v; }
 __device__ __forceinline__ void st_pop(float* p, float v) { *p = v; }
-__device__ __forceinline__ void st_pop(__half* p, float v) { *p = __float2half_rn(v); }
-__device__ __forceinline__ void st_pop(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+// 16-bit stores stream (evict-first): measured +7 % for FP16 storage.
+__device__ __forceinline__ void st_pop(__half* p, float v) { __stcs(p, __float2half_rn(v)); }
+__device__ __forceinline__ void st_pop(__nv_bfloat16* p, float v) { __stcs(p, __float2bfloat16_rn(v)); }
 
 // Offset (in cells) from x to x - c_i for direction i, given the wrapped
 // neighbour offsets of this cell.
