@@ -247,6 +247,20 @@ int psc_reduce_windows(const struct psc_window* d_windows, int nwin, double* out
 int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb, double* chunk_partials,
                        const double* imb_sums, double* forces, double* torques, double* diag, void* stream);
 
+/* ---- voxel bounce-back window LBM (scripts/run_3d_window_lbm.py) -------- */
+/* solid[(ix*ny + iy)*nz + iz] = 1 where the cell centre lo + (i + 0.5) dx lies
+ * inside any sphere of the given radius (voxelize, run_3d_window_lbm.py:73-92).
+ * d_points [M][3] device; h_lo, h_dx HOST double[3].  solid is OR-ed into
+ * (clear it first). */
+int psc_voxelize_spheres(const double* d_points, int M, const double* h_lo, const double* h_dx, double radius,
+                         int nx, int ny, int nz, uint8_t* solid, void* stream);
+/* One step of run_lbm (:100-119) on post-collision FP64 populations (pull,
+ * solid-node pair overwrite as in the reference, moments with u = 0 at solid
+ * nodes, BGK + Guo with force (fx, fy, fz)); flags PSC_STEP_COLLIDE and/or
+ * PSC_STEP_MOMENTS (rho, ux, uy, uz [4][N]). */
+int psc_bounceback_step(const double* f_src, double* f_dst, const uint8_t* solid, int nx, int ny, int nz, double tau,
+                        double fx, double fy, double fz, unsigned flags, double* moments, void* stream);
+
 /* ---- particle loads without caller scratch (no counterpart in the reference)
  * For callers that cannot allocate device memory -- a solver embedded in a
  * program that owns the device memory budget, or a coupling loop that must

@@ -134,6 +134,10 @@ SIGNATURES = {
     "psc_adjoint_step": (c_int, [POINTER(PscAdjointArgs), c_void_p]),
     "psc_adjoint_geometry_grad": (c_int, [POINTER(PscGeometry), POINTER(PscAdjointArgs), c_void_p, c_void_p,
                                           c_void_p]),
+    "psc_voxelize_spheres": (c_int, [c_void_p, c_int, POINTER(c_double), POINTER(c_double), c_double, c_int, c_int,
+                                     c_int, c_void_p, c_void_p]),
+    "psc_bounceback_step": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double, c_double,
+                                    c_double, c_uint, c_void_p, c_void_p]),
     "psc_stream_push": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "psc_stream_pull_store": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
 }

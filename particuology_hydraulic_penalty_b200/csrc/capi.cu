@@ -306,6 +306,31 @@ int psc_adjoint_geometry_grad(const psc_geometry* h_geo, const psc_adjoint_args*
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_adjoint_geometry_grad");
 }
 
+int psc_voxelize_spheres(const double* d_points, int M, const double* h_lo, const double* h_dx, double radius,
+                         int nx, int ny, int nz, uint8_t* solid, void* stream) {
+    int st = check_extent(nx, ny, nz, "psc_voxelize_spheres");
+    if (st) return st;
+    if (M < 0 || (M > 0 && !d_points) || !h_lo || !h_dx || !solid)
+        return fail(PSC_E_INVALID, "psc_voxelize_spheres: bad arguments");
+    if (!(h_dx[0] > 0.0 && h_dx[1] > 0.0 && h_dx[2] > 0.0) || !(radius == radius))
+        return fail(PSC_E_INVALID, "psc_voxelize_spheres: cell sizes must be > 0");
+    cudaError_t e = launch_vox_spheres(d_points, M, h_lo, h_dx, radius, nx, ny, nz, solid, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_voxelize_spheres");
+}
+
+int psc_bounceback_step(const double* f_src, double* f_dst, const uint8_t* solid, int nx, int ny, int nz, double tau,
+                        double fx, double fy, double fz, unsigned flags, double* moments, void* stream) {
+    int st = check_extent(nx, ny, nz, "psc_bounceback_step");
+    if (st) return st;
+    if (!f_src || !solid || ((flags & PSC_STEP_COLLIDE) && (!f_dst || f_dst == f_src)) ||
+        ((flags & PSC_STEP_MOMENTS) && !moments))
+        return fail(PSC_E_INVALID, "psc_bounceback_step: bad buffers");
+    if (!(tau > 0.5)) return fail(PSC_E_INVALID, "psc_bounceback_step: tau must exceed 0.5");
+    cudaError_t e = launch_bb_step(f_src, f_dst, solid, nx, ny, nz, tau, fx, fy, fz, flags, moments,
+                                   as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_bounceback_step");
+}
+
 int psc_stream_push(int store, double store_scale, const void* src, double* dst, int nx, int ny, int nz,
                     void* stream) {
     if (!valid_store(store) || !src || !dst) return fail(PSC_E_INVALID, "psc_stream_push: bad arguments");

@@ -341,3 +341,63 @@ PSC_HD void collide_fast2(R* g, const WinConst<R>& c, R B, R kb, R usx, R usy, R
 }
 
 }  // namespace psc
+
+namespace psc {
+
+// ===========================================================================
+// voxel bounce-back D3Q19 (scripts/run_3d_window_lbm.py:95-146), exact FP64
+// ===========================================================================
+// At a solid node the reference overwrites populations in index order,
+// f[i] = f[OPP[i]] for i = 0..18 (:117-119); because f[2k+1] is overwritten
+// before f[2k+2] reads it, both members of each pair end up holding the old
+// f[2k+2].  Reproduced as written.
+PSC_HD void bounce_solid_as_reference(double* f) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[2 * k + 1] = f[2 * k + 2];
+}
+
+// BGK + Guo with the single half-force shift of run_3d_window_lbm.py:106-114:
+// u = (m + F/2)/rho, u = 0 at solid nodes, f <- f - (f - feq)/tau + guo(u).
+PSC_HD void collide_bb_exact(double* f, bool solid, double tau, double fx, double fy, double fz, double* mom) {
+    const double hfx = xmul(0.5, fx), hfy = xmul(0.5, fy), hfz = xmul(0.5, fz);
+    ExactMoments mo = moments_exact(f, hfx, hfy, hfz);
+    if (solid) {
+        mo.ux = 0.0;
+        mo.uy = 0.0;
+        mo.uz = 0.0;
+    }
+    mom[0] = mo.rho;
+    mom[1] = mo.ux;
+    mom[2] = mo.uy;
+    mom[3] = mo.uz;
+    const double rho = mo.rho, ux = mo.ux, uy = mo.uy, uz = mo.uz;
+    const double uu = xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz));
+    const double ct = xdiv(xmul(0.5, uu), CS2);
+    const double pref = xsub(1.0, xdiv(0.5, tau));
+    const double uf = xadd(xadd(xmul(ux, fx), xmul(uy, fy)), xmul(uz, fz));
+    {
+        const double feq = xmul(xmul(W0, rho), xsub(1.0, ct));
+        const double g = xmul(xmul(pref, W0), xdiv(-uf, CS2));
+        f[0] = xadd(xsub(f[0], xdiv(xsub(f[0], feq), tau)), g);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const int i = 2 * k + 1, j = i + 1;
+        const double w = wgt(i);
+        const double wr = xmul(w, rho);
+        const double cu = xadd(xadd(cm(cxv(i), ux), cm(cyv(i), uy)), cm(czv(i), uz));
+        const double q = xdiv(cu, CS2);
+        const double b = xdiv(xmul(xmul(0.5, cu), cu), CS2SQ);
+        const double feq_i = xmul(wr, xsub(xadd(xadd(1.0, q), b), ct));
+        const double feq_j = xmul(wr, xsub(xadd(xadd(1.0, -q), b), ct));
+        const double cf = xadd(xadd(cm(cxv(i), fx), cm(cyv(i), fy)), cm(czv(i), fz));
+        const double pw = xmul(pref, w);
+        const double t2 = xdiv(xmul(cu, cf), CS2SQ);
+        const double g_i = xmul(pw, xadd(xdiv(xsub(cf, uf), CS2), t2));
+        const double g_j = xmul(pw, xadd(xdiv(xsub(-cf, uf), CS2), t2));
+        f[i] = xadd(xsub(f[i], xdiv(xsub(f[i], feq_i), tau)), g_i);
+        f[j] = xadd(xsub(f[j], xdiv(xsub(f[j], feq_j), tau)), g_j);
+    }
+}
+
+}  // namespace psc

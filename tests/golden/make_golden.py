@@ -120,6 +120,45 @@ def run_case(ref, spec):
     return out
 
 
+def voxel_cases():
+    """Cases of the reference's voxel bounce-back solver (scripts/run_3d_window_lbm.py)."""
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(0.0, 0.009, size=(12, 3))
+    return {
+        "voxel_bb_n16": dict(points=pts, center=np.array([0.0045, 0.0045, 0.0045]),
+                             size=np.array([0.009, 0.009, 0.009]), radius=0.0012, n=16, tau=0.8,
+                             force_z=1e-6, steps=40),
+        "voxel_bb_n12_offset": dict(points=pts[:5] + 0.001, center=np.array([0.005, 0.004, 0.0045]),
+                                    size=np.array([0.008, 0.009, 0.007]), radius=0.0016, n=12, tau=0.72,
+                                    force_z=2e-7, steps=25),
+    }
+
+
+def run_voxel_case(reference_root, spec):
+    import types
+
+    # The script imports matplotlib at module level for its figures; voxelize and
+    # run_lbm do not use it, and it is not installed here: register a stub.
+    if "matplotlib" not in sys.modules:
+        mpl = types.ModuleType("matplotlib")
+        mpl.pyplot = types.ModuleType("matplotlib.pyplot")
+        sys.modules["matplotlib"] = mpl
+        sys.modules["matplotlib.pyplot"] = mpl.pyplot
+    sys.path.insert(0, str(Path(reference_root).resolve() / "scripts"))
+    import run_3d_window_lbm as vref  # noqa: E402
+
+    solid, dx = vref.voxelize(spec["points"], spec["center"], spec["size"], spec["radius"], spec["n"])
+    res = vref.run_lbm(solid, spec["tau"], spec["force_z"], spec["steps"], return_fields=True)
+    out = dict(points=spec["points"], center=spec["center"], size=spec["size"], solid=solid, dx=dx,
+               ux=res["ux"], uy=res["uy"], uz=res["uz"],
+               scalars=np.array([res["mean_uz_fluid"], res["superficial_uz"], res["max_uz"],
+                                 res["permeability_lu"], res["porosity_voxel"]]))
+    meta = {k: spec[k] for k in ("radius", "n", "tau", "force_z", "steps")}
+    meta["kind"] = "voxel"
+    out["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--reference", required=True, help="root of the reference checkout")
@@ -132,6 +171,12 @@ def main():
         if args.only and name not in args.only:
             continue
         out = run_case(ref, spec)
+        np.savez_compressed(HERE / f"{name}.npz", **out)
+        print(f"wrote {name}.npz")
+    for name, spec in voxel_cases().items():
+        if args.only and name not in args.only:
+            continue
+        out = run_voxel_case(args.reference, spec)
         np.savez_compressed(HERE / f"{name}.npz", **out)
         print(f"wrote {name}.npz")
 

@@ -9,7 +9,13 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
 def names():
-    return sorted(p.stem for p in GOLDEN.glob("*.npz"))
+    """The PSC-IMB cases (psc3d.py)."""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("voxel_"))
+
+
+def voxel_names():
+    """The voxel bounce-back cases (run_3d_window_lbm.py)."""
+    return sorted(p.stem for p in GOLDEN.glob("voxel_*.npz"))
 
 
 def load(name):
