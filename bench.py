@@ -321,7 +321,15 @@ def run_ours(args):
         cpu["cpu_model"] = cpu_model()
 
     specs = [WindowSpec(w.n, w.particles, TAU, FORCE, SUBSAMPLES, name=w.kind) for w in wins]
-    batch = PscBatch(specs, precision=args.precision, graph_steps=args.graph_steps)
+    from particuology_hydraulic_penalty_b200 import _native as nat
+
+    kernel = {"direct": nat.KERNEL_DIRECT, "tma": nat.KERNEL_TMA}[args.kernel]
+    batch = PscBatch(specs, precision=args.precision, graph_steps=args.graph_steps, kernel=kernel)
+    tuned = None
+    if args.autotune:
+        from particuology_hydraulic_penalty_b200 import autotune
+
+        tuned = autotune.tune(batch, steps=20)
     clocks = ClockSampler(local)
     clocks.start()
     batch.prepare()  # graph capture of both buffer parities happens here, outside the timed region
@@ -349,12 +357,14 @@ def run_ours(args):
         "config": {"workload": WORKLOADS[args.workload].format(prec=args.precision.upper()),
                    "windows_per_gpu": len(wins), "cells_per_gpu": cells_rank,
                    "l2": "inputs (~5 GB/GPU) exceed the 126 MB L2; no flush", "parallelism": f"window-parallel x{world}",
-                   "graph_steps": args.graph_steps},
+                   "graph_steps": args.graph_steps, "launch": batch.launch_config(),
+                   "autotuned": bool(args.autotune)},
         "gpu_launches": args.steps * batch.launches_per_step(),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                      "traffic": traffic, "bytes_per_lup": bpl,
-                     "kernel": "psc::k_step (fused pull-stream + PSC collide), avg launch = timed region / steps"},
+                     "kernel": "psc::k_step_fast (fused pull-stream + PSC collide, deviation storage); avg launch = "
+                  "timed region / steps"},
         "clocks": clk,
         "nonfinite": nonfinite,
     }
@@ -436,6 +446,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="batch24")
     ap.add_argument("--precision", choices=["fp32", "fp64", "fp16", "bf16"], default="fp32")
     ap.add_argument("--graph-steps", type=int, default=20)
+    ap.add_argument("--kernel", choices=["direct", "tma"], default="direct")
+    ap.add_argument("--autotune", action="store_true", help="pick the launch with the project autotuner first")
     ap.add_argument("--fp64-steps", type=int, default=20)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=2)

@@ -73,6 +73,76 @@ def hasimoto_drag(n: int = 32, radius: float = 4.0, tau: float = 1.0, subsamples
             "ratio_over_hasimoto": float(tail.mean() / h), "hasimoto_factor": h}
 
 
+def adjoint_check(n: int = 96, n_fines: int = 64, steps: int = 2000, every: int = 100, n_check: int = 8,
+                  h: float = 1.0e-3, seed: int = 5, eps: float = 0.05, tau: float = 0.8,
+                  force=(1.0e-6, 0.0, 0.0), subsamples: int = 4) -> dict:
+    """Adjoint dK/d(x, y, z, r) of the fines of a preloaded window vs central differences.
+
+    The FP32 adjoint (the production setting) is timed against its forward
+    pass; its gradient is compared with the FP64 adjoint and with FP64
+    central differences of K for ``n_check`` seeded random fines.  The
+    gradient of a fine sums over its periodic images (all emitted copies).
+    """
+    import torch
+
+    from .adjoint import PermeabilityProblem
+
+    w = wgen.make_window(n, "preloaded", seed, n_fines=n_fines)
+    parts = w.particles
+    fines = np.unique(w.owner[w.is_fine])
+    rng = np.random.default_rng(seed)
+    pick = rng.choice(fines, size=min(n_check, len(fines)), replace=False)
+
+    def problem(prec):
+        return PermeabilityProblem(n, tau=tau, force=force, subsamples=subsamples, eps=eps, steps=steps,
+                                   checkpoint_every=every, precision=prec)
+
+    def per_sphere(g):
+        out = np.zeros((w.n_spheres, 4))
+        np.add.at(out, w.owner, g)
+        return out
+
+    p32 = problem("fp32")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    K32 = p32.forward(parts)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    g32 = per_sphere(p32.backward())
+    torch.cuda.synchronize()
+    t_bwd = time.perf_counter() - t0
+    p64 = problem("fp64")
+    K64 = p64.forward(parts)
+    g64 = per_sphere(p64.backward())
+    gap = p64.solid_gap()
+    rows = []
+    for s_id in pick:
+        idx = np.nonzero(w.owner == s_id)[0]
+        for k in range(4):
+            pp = parts.copy()
+            pp[idx, k] += h
+            pm = parts.copy()
+            pm[idx, k] -= h
+            fd = (problem("fp64").forward(pp) - problem("fp64").forward(pm)) / (2.0 * h)
+            rows.append({"sphere": int(s_id), "component": "xyzr"[k], "fd_fp64": fd, "adjoint_fp64": g64[s_id, k],
+                         "adjoint_fp32": g32[s_id, k]})
+    fd = np.array([r["fd_fp64"] for r in rows])
+    a64 = np.array([r["adjoint_fp64"] for r in rows])
+    a32 = np.array([r["adjoint_fp32"] for r in rows])
+    scale = np.abs(fd).max()
+    return {
+        "n": n, "steps": steps, "checkpoint_every": every, "n_fines": int(len(fines)), "K_fp32": K32,
+        "K_fp64": K64, "forward_s_fp32": t_fwd, "backward_s_fp32": t_bwd, "backward_over_forward": t_bwd / t_fwd,
+        "adjoint_plus_forward_over_forward": (t_fwd + t_bwd) / t_fwd,
+        "fd_vs_adjoint_fp64_max_rel": float(np.max(np.abs(fd - a64) / np.maximum(np.abs(fd), 1e-3 * scale))),
+        "fd_vs_adjoint_fp64_norm_rel": float(np.linalg.norm(fd - a64) / np.linalg.norm(fd)),
+        "adjoint_fp32_vs_fp64_norm_rel": float(np.linalg.norm(a32 - a64) / np.linalg.norm(a64)),
+        "fd_vs_adjoint_fp32_norm_rel": float(np.linalg.norm(fd - a32) / np.linalg.norm(fd)),
+        "solid_gap_smooth_vs_counted": gap, "checks": rows,
+    }
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -83,15 +153,25 @@ def main(argv=None):
     lad.add_argument("--check-every", type=int, default=200)
     lad.add_argument("--max-steps", type=int, default=100000)
     lad.add_argument("--precisions", nargs="+", default=["fp64", "fp32", "fp16", "bf16"])
+    lad.add_argument("--kinds", nargs="+", default=list(wgen.GEOMETRY_TYPES))
+    lad.add_argument("--sizes", nargs="+", type=int, default=None, help="window edges (default: --n)")
+    adj = sub.add_parser("adjoint")
+    adj.add_argument("--n", type=int, default=96)
+    adj.add_argument("--fines", type=int, default=64)
+    adj.add_argument("--steps", type=int, default=2000)
+    adj.add_argument("--every", type=int, default=100)
+    adj.add_argument("--check", type=int, default=8)
     has = sub.add_parser("hasimoto")
     has.add_argument("--n", type=int, default=32)
     has.add_argument("--radius", type=float, default=4.0)
     has.add_argument("--steps", type=int, default=4000)
     args = ap.parse_args(argv)
     if args.cmd == "ladder":
-        wins = [wgen.make_window(args.n, k, args.seed) for k in wgen.GEOMETRY_TYPES]
+        wins = [wgen.make_window(n, k, args.seed) for n in (args.sizes or [args.n]) for k in args.kinds]
         res = precision_ladder(wins, precisions=tuple(args.precisions), tol=args.tol, check_every=args.check_every,
                                max_steps=args.max_steps)
+    elif args.cmd == "adjoint":
+        res = adjoint_check(n=args.n, n_fines=args.fines, steps=args.steps, every=args.every, n_check=args.check)
     else:
         res = hasimoto_drag(n=args.n, radius=args.radius, steps=args.steps)
     print(json.dumps(res))
