@@ -247,6 +247,15 @@ int psc_reduce_windows(const struct psc_window* d_windows, int nwin, double* out
 int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb, double* chunk_partials,
                        const double* imb_sums, double* forces, double* torques, double* diag, void* stream);
 
+/* ---- element-wise helpers of the reference module ----------------------- */
+/* out[i][c] = equilibrium of (rho, u) at n cells, exact FP64 in the
+ * reference's operation order (equilibrium, psc3d.py:97-103). */
+int psc_equilibrium(const double* rho, const double* ux, const double* uy, const double* uz, double* out, int64_t n,
+                    void* stream);
+/* out[i][c] = Guo forcing term for force (fx, fy, fz) (guo_force, psc3d.py:106-114). */
+int psc_guo_force(double fx, double fy, double fz, const double* ux, const double* uy, const double* uz, double tau,
+                  double* out, int64_t n, void* stream);
+
 /* ---- voxel bounce-back window LBM (scripts/run_3d_window_lbm.py) -------- */
 /* solid[(ix*ny + iy)*nz + iz] = 1 where the cell centre lo + (i + 0.5) dx lies
  * inside any sphere of the given radius (voxelize, run_3d_window_lbm.py:73-92).

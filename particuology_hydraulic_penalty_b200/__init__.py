@@ -5,6 +5,6 @@ Drop-in for the hot path of wangjianfttt/particuology_Hydraulic-penalty-
 the lattice constants keep the reference's names and call surface.
 """
 
-from .psc3d import C, CS2, OPP, W, Particle3D, PscD3Q19, SparsePscD3Q19
+from .psc3d import C, CS2, OPP, W, Particle3D, PscD3Q19, SparsePscD3Q19, equilibrium, guo_force
 
-__all__ = ["C", "CS2", "OPP", "W", "Particle3D", "PscD3Q19", "SparsePscD3Q19"]
+__all__ = ["C", "CS2", "OPP", "W", "Particle3D", "PscD3Q19", "SparsePscD3Q19", "equilibrium", "guo_force"]

@@ -134,6 +134,9 @@ SIGNATURES = {
     "psc_adjoint_step": (c_int, [POINTER(PscAdjointArgs), c_void_p]),
     "psc_adjoint_geometry_grad": (c_int, [POINTER(PscGeometry), POINTER(PscAdjointArgs), c_void_p, c_void_p,
                                           c_void_p]),
+    "psc_equilibrium": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p]),
+    "psc_guo_force": (c_int, [c_double, c_double, c_double, c_void_p, c_void_p, c_void_p, c_double, c_void_p, c_int64,
+                              c_void_p]),
     "psc_voxelize_spheres": (c_int, [c_void_p, c_int, POINTER(c_double), POINTER(c_double), c_double, c_int, c_int,
                                      c_int, c_void_p, c_void_p]),
     "psc_bounceback_step": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double, c_double,

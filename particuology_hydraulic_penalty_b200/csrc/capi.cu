@@ -306,6 +306,23 @@ int psc_adjoint_geometry_grad(const psc_geometry* h_geo, const psc_adjoint_args*
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_adjoint_geometry_grad");
 }
 
+int psc_equilibrium(const double* rho, const double* ux, const double* uy, const double* uz, double* out, int64_t n,
+                    void* stream) {
+    if (n < 0 || (n > 0 && (!rho || !ux || !uy || !uz || !out)))
+        return fail(PSC_E_INVALID, "psc_equilibrium: bad arguments");
+    if (n == 0) return PSC_OK;
+    cudaError_t e = launch_equilibrium(rho, ux, uy, uz, out, n, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_equilibrium");
+}
+
+int psc_guo_force(double fx, double fy, double fz, const double* ux, const double* uy, const double* uz, double tau,
+                  double* out, int64_t n, void* stream) {
+    if (n < 0 || (n > 0 && (!ux || !uy || !uz || !out))) return fail(PSC_E_INVALID, "psc_guo_force: bad arguments");
+    if (n == 0) return PSC_OK;
+    cudaError_t e = launch_guo(fx, fy, fz, ux, uy, uz, tau, out, n, as_stream(stream));
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_guo_force");
+}
+
 int psc_voxelize_spheres(const double* d_points, int M, const double* h_lo, const double* h_dx, double radius,
                          int nx, int ny, int nz, uint8_t* solid, void* stream) {
     int st = check_extent(nx, ny, nz, "psc_voxelize_spheres");

@@ -56,6 +56,11 @@ cudaError_t launch_vox_spheres(const double* pts, int M, const double* lo, const
 cudaError_t launch_bb_step(const double* src, double* dst, const uint8_t* solid, int nx, int ny, int nz, double tau,
                            double fx, double fy, double fz, unsigned flags, double* mom, cudaStream_t s);
 
+cudaError_t launch_equilibrium(const double* rho, const double* ux, const double* uy, const double* uz, double* out,
+                               int64_t n, cudaStream_t s);
+cudaError_t launch_guo(double fx, double fy, double fz, const double* ux, const double* uy, const double* uz,
+                       double tau, double* out, int64_t n, cudaStream_t s);
+
 // exclusive scan of int32 counts -> int32 offsets, out has n + 1 entries
 size_t scan_tmp_bytes(int64_t n);
 cudaError_t scan_exclusive_i32(const int32_t* in, int32_t* out, int64_t n, void* tmp, cudaStream_t stream);

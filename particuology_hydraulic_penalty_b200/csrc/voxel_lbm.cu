@@ -102,3 +102,61 @@ cudaError_t launch_bb_step(const double* src, double* dst, const uint8_t* solid,
 }
 
 }  // namespace psc
+
+namespace psc {
+
+// Element-wise equilibrium (src/lbm_dem/psc3d.py:97-103) and Guo forcing
+// (:106-114) in the reference's operation order, for the module-level helpers.
+__global__ void k_equilibrium(const double* rho, const double* ux, const double* uy, const double* uz, double* out,
+                              int64_t n) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const double r = rho[c], x = ux[c], y = uy[c], z = uz[c];
+        const double uu = xadd(xadd(xmul(x, x), xmul(y, y)), xmul(z, z));
+        const double ct = xdiv(xmul(0.5, uu), CS2);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const double cu = xadd(xadd(cm(cxv(i), x), cm(cyv(i), y)), cm(czv(i), z));
+            const double a = xadd(1.0, xdiv(cu, CS2));
+            const double b = xdiv(xmul(xmul(0.5, cu), cu), CS2SQ);
+            out[(size_t)i * n + c] = xmul(xmul(wgt(i), r), xsub(xadd(a, b), ct));
+        }
+    }
+}
+
+__global__ void k_guo(double fx, double fy, double fz, const double* ux, const double* uy, const double* uz,
+                      double tau, double* out, int64_t n) {
+    const double pref = xsub(1.0, xdiv(0.5, tau));
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const double x = ux[c], y = uy[c], z = uz[c];
+        const double uf = xadd(xadd(xmul(x, fx), xmul(y, fy)), xmul(z, fz));
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const double cu = xadd(xadd(cm(cxv(i), x), cm(cyv(i), y)), cm(czv(i), z));
+            const double cf = xadd(xadd(cm(cxv(i), fx), cm(cyv(i), fy)), cm(czv(i), fz));
+            out[(size_t)i * n + c] =
+                xmul(xmul(pref, wgt(i)), xadd(xdiv(xsub(cf, uf), CS2), xdiv(xmul(cu, cf), CS2SQ)));
+        }
+    }
+}
+
+cudaError_t launch_equilibrium(const double* rho, const double* ux, const double* uy, const double* uz, double* out,
+                               int64_t n, cudaStream_t s) {
+    int64_t g = (n + 255) / 256;
+    const int64_t cap = (int64_t)sm_count() * 8;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    k_equilibrium<<<(unsigned)g, 256, 0, s>>>(rho, ux, uy, uz, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_guo(double fx, double fy, double fz, const double* ux, const double* uy, const double* uz,
+                       double tau, double* out, int64_t n, cudaStream_t s) {
+    int64_t g = (n + 255) / 256;
+    const int64_t cap = (int64_t)sm_count() * 8;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    k_guo<<<(unsigned)g, 256, 0, s>>>(fx, fy, fz, ux, uy, uz, tau, out, n);
+    return cudaGetLastError();
+}
+
+}  // namespace psc

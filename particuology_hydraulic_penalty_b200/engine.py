@@ -150,6 +150,8 @@ class DeviceGeometry:
         self.totals = torch.zeros(4, dtype=i64, device=device)
         self.P = -1
         self.particles = torch.zeros((0, 10), dtype=f64, device=device)
+        self._pinned = None
+        self._upload_done = None
         self.bbox = self.ent_off = self.chunk_off = None
         self.cap_entries = 0
         self.cap_chunks = 0
@@ -164,8 +166,13 @@ class DeviceGeometry:
         self.built = False
         self.host_particles = np.zeros((0, 10))
 
-    def set_particles(self, arr: np.ndarray) -> None:
-        """Upload the (P, 10) particle state (positions, radii, velocities, spins)."""
+    def set_particles(self, arr: np.ndarray) -> bool:
+        """Upload the (P, 10) particle state (positions, radii, velocities, spins).
+
+        Staged through a pinned host buffer and copied asynchronously on the
+        current stream (every call: callers may mutate particles in place).
+        Returns True when the state differs from the previous upload.
+        """
         P = arr.shape[0]
         if P != self.P:
             dev = self.device
@@ -173,9 +180,21 @@ class DeviceGeometry:
             self.bbox = torch.zeros(max(P, 1) * 6, dtype=torch.int32, device=dev)
             self.ent_off = torch.zeros(P + 1, dtype=torch.int64, device=dev)
             self.chunk_off = torch.zeros(P + 1, dtype=torch.int64, device=dev)
+            self.particles = torch.zeros((P, 10), dtype=torch.float64, device=dev)
+            self._pinned = torch.zeros((max(P, 1), 10), dtype=torch.float64).pin_memory()
+            self._upload_done = None
             self.built = False
-        self.host_particles = arr
-        self.particles = torch.from_numpy(arr).to(self.device, non_blocking=False).reshape(P, 10)
+            self.host_particles = np.zeros((0, 10))
+        changed = not (self.host_particles.shape == arr.shape and np.array_equal(self.host_particles, arr))
+        self.host_particles = arr.copy()
+        if P:
+            if self._upload_done is not None:
+                self._upload_done.synchronize()  # the pinned buffer is free again
+            self._pinned[:P].numpy()[...] = arr
+            self.particles.copy_(self._pinned[:P], non_blocking=True)
+            self._upload_done = torch.cuda.Event()
+            self._upload_done.record()
+        return changed
 
     def struct(self) -> nat.PscGeometry:
         g = nat.PscGeometry()

@@ -37,6 +37,39 @@ OPP = np.array([0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17
 CS2 = 1.0 / 3.0
 
 
+def _to_dev(a, dev):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+
+
+def equilibrium(rho, ux, uy, uz) -> np.ndarray:
+    """Second-order D3Q19 equilibrium, (19, *shape) (psc3d.py:97-103), computed on the GPU in FP64."""
+    dev = require_cuda()
+    shape = np.shape(rho)
+    n = int(np.prod(shape)) if shape else 1
+    with torch.cuda.device(dev):
+        args = [_to_dev(np.broadcast_to(a, shape), dev) for a in (rho, ux, uy, uz)]
+        out = torch.empty(19 * n, dtype=torch.float64, device=dev)
+        from .engine import stream_handle, vp
+
+        nat.call("psc_equilibrium", *(vp(a) for a in args), vp(out), n, stream_handle(dev))
+        return out.view(19, *shape).cpu().numpy()
+
+
+def guo_force(fx: float, fy: float, fz: float, ux, uy, uz, tau: float) -> np.ndarray:
+    """Guo forcing term, (19, *shape) (psc3d.py:106-114), computed on the GPU in FP64."""
+    dev = require_cuda()
+    shape = np.shape(ux)
+    n = int(np.prod(shape)) if shape else 1
+    with torch.cuda.device(dev):
+        args = [_to_dev(np.broadcast_to(a, shape), dev) for a in (ux, uy, uz)]
+        out = torch.empty(19 * n, dtype=torch.float64, device=dev)
+        from .engine import stream_handle, vp
+
+        nat.call("psc_guo_force", float(fx), float(fy), float(fz), *(vp(a) for a in args), float(tau), vp(out), n,
+                 stream_handle(dev))
+        return out.view(19, *shape).cpu().numpy()
+
+
 @dataclass
 class Particle3D:
     """Sphere state in lattice units (psc3d.py:46-57)."""
@@ -87,12 +120,16 @@ class PscD3Q19:
             self._forces_dev = torch.zeros((self._P, 3), dtype=torch.float64, device=self._device)
             self._torques_dev = torch.zeros((self._P, 3), dtype=torch.float64, device=self._device)
             self._diag_dev = torch.zeros(nat.NDIAG, dtype=torch.float64, device=self._device)
+            self._out_dev = torch.zeros(nat.NRED + nat.NDIAG, dtype=torch.float64, device=self._device)
+            self._out_host = torch.zeros(nat.NRED + nat.NDIAG, dtype=torch.float64).pin_memory()
         self._geometry_built = False
         self._stepped = False
+        self._moments_ready = False
+        self._loads_host = None
         self._cache: dict = {}
-        self.hydro_forces = np.zeros((self._P, 3), dtype=float)
-        self.hydro_torques = np.zeros((self._P, 3), dtype=float)
-        self.momentum_residual = 0.0
+        self._hf = np.zeros((self._P, 3), dtype=float)
+        self._ht = np.zeros((self._P, 3), dtype=float)
+        self._momentum_residual = 0.0
 
     # ------------------------------------------------------------------
     # geometry
@@ -151,32 +188,76 @@ class PscD3Q19:
             win.step(nat.STEP_IMB | nat.STEP_REDUCE)
             win.reduce(win.red)
             self._geo.loads(win.imb, win.red[nat.RED_IMBX:], self._forces_dev, self._torques_dev, self._diag_dev)
-            win.moments_pass(win.red_post, write_fields=True)
-            host = torch.cat([win.red_post, self._diag_dev, self._forces_dev.view(-1),
-                              self._torques_dev.view(-1)]).cpu().numpy()
+            # reductions of the post-stream state only; the fields are made on access
+            win.moments_pass(win.red_post, write_fields=False)
+            self._out_dev[: nat.NRED].copy_(win.red_post)
+            self._out_dev[nat.NRED:].copy_(self._diag_dev)
+            self._out_host.copy_(self._out_dev, non_blocking=True)
+            torch.cuda.current_stream(self._device).synchronize()
         self._stepped = True
+        self._moments_ready = False
+        self._loads_host = None
         self._cache.clear()
+        host = self._out_host.numpy()
         red_post = host[: nat.NRED]
-        diag = host[nat.NRED: nat.NRED + nat.NDIAG]
+        diag = host[nat.NRED:]
         P = self._P
-        forces = host[nat.NRED + nat.NDIAG: nat.NRED + nat.NDIAG + 3 * P].reshape(P, 3)
-        torques = host[nat.NRED + nat.NDIAG + 3 * P:].reshape(P, 3)
-        self._store_loads(forces, torques)
-        self.momentum_residual = float(diag[nat.DIAG_MOMENTUM_RESIDUAL])
+        self._momentum_residual = float(diag[nat.DIAG_MOMENTUM_RESIDUAL])
         if red_post[nat.RED_NONFINITE] > 0:
             self._nonfinite = True
         return {
             "solid_volume_lu": float(red_post[nat.RED_SOLID]),
             "mean_uz": float(red_post[nat.RED_UZ] / self._geo.N),
-            "momentum_residual": float(self.momentum_residual),
+            "momentum_residual": float(self._momentum_residual),
             "max_force": float(diag[nat.DIAG_MAX_FORCE]) if P else 0.0,
             "max_torque": float(diag[nat.DIAG_MAX_TORQUE]) if P else 0.0,
         }
 
+    # loads are copied to the host when read ------------------------------
+    def _fetch_loads(self) -> None:
+        if self._loads_host is None:
+            with torch.cuda.device(self._device):
+                f = self._forces_dev.cpu().numpy()
+                t = self._torques_dev.cpu().numpy()
+            self._store_loads(f, t)
+            self._loads_host = True
+
+    @property
+    def hydro_forces(self) -> np.ndarray:
+        if self._stepped:
+            self._fetch_loads()
+        return self._hf
+
+    @hydro_forces.setter
+    def hydro_forces(self, value) -> None:
+        if self._stepped:
+            self._fetch_loads()  # results of the last step go into the old array first
+        self._hf = value
+
+    @property
+    def hydro_torques(self) -> np.ndarray:
+        if self._stepped:
+            self._fetch_loads()
+        return self._ht
+
+    @hydro_torques.setter
+    def hydro_torques(self, value) -> None:
+        if self._stepped:
+            self._fetch_loads()
+        self._ht = value
+
+    @property
+    def momentum_residual(self) -> float:
+        return self._momentum_residual
+
+    @momentum_residual.setter
+    def momentum_residual(self, value) -> None:
+        self._momentum_residual = float(value)
+
     def _store_loads(self, forces: np.ndarray, torques: np.ndarray) -> None:
         # the coupled driver reallocates hydro_forces / hydro_torques itself
         # (couple_psc_liggghts.py:592-594); write into its arrays when they fit
-        for name, val in (("hydro_forces", forces), ("hydro_torques", torques)):
+        for name, val in (("_hf", forces), ("_ht", torques)):
             cur = getattr(self, name, None)
             if isinstance(cur, np.ndarray) and cur.shape == val.shape and cur.dtype == np.float64:
                 cur[...] = val
@@ -193,6 +274,7 @@ class PscD3Q19:
             host = torch.cat([self._diag_dev, self._forces_dev.view(-1), self._torques_dev.view(-1)]).cpu().numpy()
         P = self._P
         self._store_loads(host[nat.NDIAG: nat.NDIAG + 3 * P].reshape(P, 3), host[nat.NDIAG + 3 * P:].reshape(P, 3))
+        self._loads_host = True
         self.momentum_residual = float(host[nat.DIAG_MOMENTUM_RESIDUAL])
 
     # ------------------------------------------------------------------
@@ -204,6 +286,10 @@ class PscD3Q19:
     def _moment(self, k: int) -> np.ndarray:
         if not self._stepped:
             return np.ones(self._shape3()) if k == 0 else np.zeros(self._shape3())
+        if not self._moments_ready:
+            with torch.cuda.device(self._device):
+                self._win.moments_pass(None, write_fields=True)
+            self._moments_ready = True
         key = ("mom", k)
         if key not in self._cache:
             N = self._geo.N
@@ -269,6 +355,7 @@ class PscD3Q19:
         with torch.cuda.device(self._device):
             self._win.load_post_stream_f(t)
         self._cache.clear()
+        self._moments_ready = False
 
     @property
     def alpha_p(self) -> np.ndarray:

@@ -204,3 +204,15 @@ def test_probe_cli_matches_oracle(tmp_path):
     with (tmp_path / "skeleton_n020.csv").open() as f:
         got = list(csv.DictReader(f))
     assert len(got) == 1 and set(got[0]) == set(probe.FIELDS)
+
+
+def test_module_helpers_bitwise():
+    """equilibrium / guo_force of the package equal the reference formulas bit for bit."""
+    from particuology_hydraulic_penalty_b200 import equilibrium, guo_force
+
+    rng = np.random.default_rng(4)
+    shp = (5, 6, 7)
+    rho = 1 + rng.normal(0, 1e-3, shp)
+    u = rng.normal(0, 1e-3, (3,) + shp)
+    assert np.array_equal(equilibrium(rho, *u), orc.equilibrium(rho, *u))
+    assert np.array_equal(guo_force(1e-6, -2e-7, 3e-7, *u, 0.8), orc.guo_force(1e-6, -2e-7, 3e-7, *u, 0.8))
