@@ -260,6 +260,29 @@ def run_fp64_plain(windows, steps: int, warm: int):
     return per_window
 
 
+def run_fp64_exact_dropin(windows, steps: int, warm: int = 2):
+    """Per-window ms/step of the plain FP64 drop-in (reference arithmetic, per-call diagnostics)."""
+    import torch
+
+    from particuology_hydraulic_penalty_b200 import SparsePscD3Q19
+
+    per_window = []
+    for w in windows:
+        s = SparsePscD3Q19(w.n, w.particles, tau=TAU, subsamples=SUBSAMPLES, static_geometry=True,
+                           precision="fp64-exact", force=FORCE)
+        for _ in range(warm):
+            s.collide_stream_psc()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            s.collide_stream_psc()
+        torch.cuda.synchronize()
+        per_window.append((time.perf_counter() - t0) / steps * 1e3)
+        del s
+        torch.cuda.empty_cache()
+    return per_window
+
+
 def run_e2e(windows, steps: int):
     """MLUPS through the drop-in class (host particle upload + diagnostics read back per call)."""
     import torch
@@ -381,6 +404,15 @@ def run_ours(args):
         per_ms = run_fp64_plain(wins, steps=args.fp64_steps, warm=3)
         t_plain_h = sum(STEPS_PER_WINDOW * m * 1e-3 for m in per_ms) / 3600.0
         t_batch_h = STEPS_PER_WINDOW * (ms / args.steps) * 1e-3 / 3600.0  # all windows advance together
+        exact_ms = run_fp64_exact_dropin(wins, steps=args.fp64_steps)
+        t_exact_h = sum(STEPS_PER_WINDOW * m * 1e-3 for m in exact_ms) / 3600.0
+        out["fp64_exact_dropin"] = {
+            "what": "plain FP64 form: SparsePscD3Q19(precision='fp64-exact').collide_stream_psc() per window, "
+                    "reference arithmetic and per-call diagnostics, one window at a time",
+            "mlups": round(sum(w.n ** 3 for w in wins) / (sum(exact_ms) * 1e-3) / 1e6, 1),
+            "windows_per_hour": round(len(wins) / t_exact_h, 1),
+            "fp32_batched_over_this_windows_per_hour": round(t_exact_h / t_batch_h, 2),
+        }
         out["fp64_plain"] = {
             "mlups": round(sum(w.n ** 3 for w in wins) / (sum(per_ms) * 1e-3) / 1e6, 1),
             "windows_per_hour": round(len(wins) / t_plain_h, 1),

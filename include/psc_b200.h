@@ -75,7 +75,8 @@ typedef struct psc_launch {
 } psc_launch;
 
 /* ---- per-window flags --------------------------------------------------- */
-#define PSC_WIN_MOVING 1 /* read the solid velocity field us (else u_s = 0) */
+#define PSC_WIN_MOVING 1   /* read the solid velocity field us (else u_s = 0) */
+#define PSC_WIN_INACTIVE 2 /* skip the window's tiles: state frozen (e.g. converged); no partials written */
 
 /* Reduction slots written per tile with PSC_STEP_REDUCE and summed per window
  * by psc_reduce_windows().  Velocities are the stored-moment velocities

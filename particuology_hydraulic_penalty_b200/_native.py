@@ -38,6 +38,7 @@ STEP_REDUCE = 8
 STEP_MOVING = 16
 
 WIN_MOVING = 1
+WIN_INACTIVE = 2
 
 # reduction slots
 RED_RHO, RED_UX, RED_UY, RED_UZ = 0, 1, 2, 3

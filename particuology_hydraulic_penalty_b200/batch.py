@@ -96,6 +96,8 @@ class PscBatch:
         self.cells = np.array([w.N for w in self.windows], dtype=np.int64)
         self.parity = 0
         self.steps_done = 0
+        self.frozen: dict[int, int] = {}  # window -> buffer parity holding its frozen state
+        self._frozen_red: dict[int, np.ndarray] = {}
         self._tables = None
         self._graphs: dict = {}
         self._red = torch.zeros(len(self.windows) * nat.NRED, dtype=torch.float64, device=self.device)
@@ -110,6 +112,8 @@ class PscBatch:
             arr = (nat.PscWindow * nwin)()
             for k, w in enumerate(self.windows):
                 arr[k] = w.struct(parity)
+                if k in self.frozen:
+                    arr[k].flags |= nat.WIN_INACTIVE
                 if self.rows_per_window is not None:
                     arr[k].tile_cells = int(self.rows_per_window[k]) * w.nz
             total = ctypes.c_int64(0)
@@ -163,13 +167,35 @@ class PscBatch:
         nat.call("psc_step_ex", self.store, vp(self._tables[self.parity]), self.nwin, self.total_tiles,
                  flags, ctypes.byref(cfg), stream_handle(self.device))
 
+    def _sync_cur(self) -> None:
+        for k, w in enumerate(self.windows):
+            w.cur = self.frozen.get(k, self.parity)
+
     def step_once(self, flags: int = 0) -> None:
-        """One collide-stream step of every window (one kernel launch)."""
+        """One collide-stream step of every active window (one kernel launch)."""
         self._launch(flags | nat.STEP_COLLIDE)
         self.parity ^= 1
-        for w in self.windows:
-            w.cur = self.parity
+        self._sync_cur()
         self.steps_done += 1
+
+    def freeze(self, k: int, red_row: np.ndarray | None = None) -> None:
+        """Stop stepping window k (its tiles are skipped by the kernel); keeps its current state.
+
+        The flag is written into both device tables in place, so captured step
+        graphs stay valid.
+        """
+        if k in self.frozen:
+            return
+        self.frozen[k] = self.parity
+        if red_row is not None:
+            self._frozen_red[k] = np.array(red_row, dtype=np.float64)
+        size = ctypes.sizeof(nat.PscWindow)
+        off = nat.PscWindow.flags.offset
+        for table in self._tables:
+            cur = int(table[k * size + off: k * size + off + 4].view(torch.int32).item())
+            table[k * size + off: k * size + off + 4].copy_(
+                torch.tensor([cur | nat.WIN_INACTIVE], dtype=torch.int32).view(torch.uint8))
+        self._sync_cur()
 
     def _capture(self) -> None:
         """Capture graph_steps launches starting at the current buffer parity."""
@@ -196,8 +222,7 @@ class PscBatch:
                     if self.parity not in self._graphs:
                         self._capture()
                     self.parity ^= 1  # capture does not run anything; visit the other parity
-                for w in self.windows:
-                    w.cur = self.parity
+                self._sync_cur()
 
     def run(self, steps: int) -> None:
         """Advance every window by ``steps`` steps (graph replays plus a remainder)."""
@@ -213,8 +238,7 @@ class PscBatch:
                     graph.replay()
                 self.steps_done += reps * self.graph_steps
                 steps -= reps * self.graph_steps
-                for w in self.windows:
-                    w.cur = self.parity
+                self._sync_cur()
             for _ in range(steps):
                 self.step_once()
 
@@ -228,7 +252,10 @@ class PscBatch:
             self._launch(nat.STEP_REDUCE)
             nat.call("psc_reduce_windows", vp(self._tables[self.parity]), self.nwin, vp(self._red),
                      stream_handle(self.device))
-            return self._red.view(self.nwin, nat.NRED).cpu().numpy().copy()
+            red = self._red.view(self.nwin, nat.NRED).cpu().numpy().copy()
+        for k, row in self._frozen_red.items():  # frozen windows wrote no partials
+            red[k] = row
+        return red
 
     def permeability(self, red: np.ndarray | None = None) -> np.ndarray:
         """Darcy K per window along its body force, run_psc_permeability_resolution.py:144-150."""
@@ -245,15 +272,16 @@ class PscBatch:
         return out
 
     def run_to_convergence(self, tol: float = 1.0e-8, check_every: int = 200, max_steps: int = 200000,
-                           min_steps: int = 0) -> dict:
+                           min_steps: int = 0, freeze: bool = True) -> dict:
         """Step until every window's per-step relative change of K is below ``tol``.
 
         The criterion of the reference's coupled driver, |q_k - q_{k-1}| / |q_k| <
         tol between consecutive steps (coupling_sync/couple_psc_liggghts.py:284-296),
         applied to the Darcy flux of each window and evaluated on a pair of
         consecutive steps every ``check_every`` steps (no per-step host work in
-        between).  Windows that converge early keep stepping with the rest; their
-        convergence step is recorded.  Returns per-window steps, residuals and K.
+        between).  A window that converges is frozen (``freeze``): the kernel skips
+        its tiles from then on, so the launch spends HBM bandwidth only on the
+        windows still converging.  Returns per-window steps, residuals and K.
         """
         nwin = self.nwin
         conv_step = np.full(nwin, -1, dtype=np.int64)
@@ -275,6 +303,9 @@ class PscBatch:
             now = self.steps_done - start
             newly = (conv_step < 0) & (residual < tol) & (now >= min_steps)
             conv_step[newly] = now
+            if freeze:
+                for k in np.nonzero(newly)[0]:
+                    self.freeze(int(k), red[k])
             if np.all(conv_step >= 0):
                 break
         return {"steps": conv_step, "residual": residual, "permeability": self.permeability(),

@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restr
     for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         const int wi = find_window(wins, in_smem ? s_begin : nullptr, nwin, t);
         const psc_window& W = wins[wi];
+        if (W.flags & PSC_WIN_INACTIVE) continue;  // block-uniform
         const int nx = W.nx, ny = W.ny, nz = W.nz;
         const uint32_t N = (uint32_t)nx * (uint32_t)ny * (uint32_t)nz;
         const int64_t local_tile = t - W.tile_begin;

@@ -30,6 +30,7 @@ struct FastWin {
     uint32_t step_x, step_y, step_z;  // blockDim cells as a mixed-radix (x, y, z) increment
     int32_t tile_cells;
     int32_t moving;
+    int32_t inactive;
     R scale, inv_scale;
     WinConst<R> c;
     R Blut[256];
@@ -62,6 +63,7 @@ __device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool mov
         s.step_x = q / (uint32_t)W.ny;
         s.tile_cells = W.tile_cells;
         s.moving = (moving_launch && (W.flags & PSC_WIN_MOVING) && W.us != nullptr) ? 1 : 0;
+        s.inactive = (W.flags & PSC_WIN_INACTIVE) ? 1 : 0;
         s.scale = (R)W.store_scale;
         s.inv_scale = (R)(1.0 / W.store_scale);
         s.tau = (R)W.tau;
@@ -104,6 +106,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
             __syncthreads();
             win_end = sw.tile_end;
         }
+        if (sw.inactive) continue;  // block-uniform
         const uint32_t N = sw.N, nx = sw.nx, ny = sw.ny, nz = sw.nz;
         const uint32_t base = (uint32_t)((t - sw.tile_begin) * sw.tile_cells);
         uint32_t cell = base + threadIdx.x;

@@ -89,6 +89,7 @@ struct TmaWin {
     int64_t tile_begin, tile_end;
     uint32_t nx, ny, nz, N, ty, nyb;
     int32_t moving;
+    int32_t inactive;
     R scale, inv_scale, tau;
     WinConst<R> c;
     R Blut[256];
@@ -143,7 +144,12 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
         int wi = 0;
         uint32_t issued = 0;
         bool stop = false;
-        for (int64_t t = t0; t < t1; ++t, ++issued) {
+        for (int64_t t = t0; t < t1; ++t) {
+            if (t >= win_end) {
+                wi = find_window(wins, nullptr, nwin, t);
+                win_end = wins[wi].tile_begin + wins[wi].tile_count;
+            }
+            if (wins[wi].flags & PSC_WIN_INACTIVE) continue;  // the consumers skip the same tiles
             const int s = (int)(issued % STAGES);
             if (issued >= (uint32_t)STAGES) {
                 int ok = 1;
@@ -154,10 +160,6 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
                     stop = true;
                     break;
                 }
-            }
-            if (t >= win_end) {
-                wi = find_window(wins, nullptr, nwin, t);
-                win_end = wins[wi].tile_begin + wins[wi].tile_count;
             }
             const psc_window& W = wins[wi];
             uint32_t ix, y0, rows;
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
                 if (W.level) bulk_g2s(gdst, W.level + base, rows * nz, &full[s]);
                 else bulk_g2s(gdst, W.solid + base, rows * nz * 8u, &full[s]);
             }
+            ++issued;
         }
         (void)stop;
         // drain: wait (bounded) for every issued stage to land before the CTA may exit
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
     int64_t win_end = -1;
     uint32_t k = 0;
     bool aborted = false;  // after a stuck wait: keep joining the barriers, skip the work
-    for (int64_t t = t0; t < t1; ++t, ++k) {
+    for (int64_t t = t0; t < t1; ++t) {
         if (t >= win_end) {
             consumer_sync();
             if (threadIdx.x == 0) {
@@ -236,6 +239,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
                 sw.ty = (uint32_t)(W.tile_cells / W.nz);
                 sw.nyb = ((uint32_t)W.ny + sw.ty - 1) / sw.ty;
                 sw.moving = (MOVING && (W.flags & PSC_WIN_MOVING) && W.us != nullptr) ? 1 : 0;
+                sw.inactive = (W.flags & PSC_WIN_INACTIVE) ? 1 : 0;
                 sw.scale = (R)W.store_scale;
                 sw.inv_scale = (R)(1.0 / W.store_scale);
                 sw.tau = (R)W.tau;
@@ -258,6 +262,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
             consumer_sync();
             win_end = sw.tile_end;
         }
+        if (sw.inactive) continue;  // uniform over consumers; the producer issued nothing for it
         const int s = (int)(k % STAGES);
         if (!aborted && !mbar_wait(&full[s], (k / STAGES) & 1, 0x103)) {
             aborted = true;
@@ -388,6 +393,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
             }
             consumer_sync();
         }
+        ++k;
     }
 }
 

@@ -142,3 +142,26 @@ def test_tma_kernel_with_reductions_and_loads():
     Ft, Tt = t.loads()[0]
     assert np.array_equal(Fd, Ft) and np.array_equal(Td, Tt)
     assert ctypes_status() == 0
+
+
+@pytest.mark.parametrize("kernel", ["direct", "tma"])
+def test_converged_windows_freeze_exactly(kernel):
+    """A window frozen at convergence keeps exactly the state it had at its convergence step."""
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    k = {"direct": nat.KERNEL_DIRECT, "tma": nat.KERNEL_TMA}[kernel]
+    wins = [wgen.make_window(16, "skeleton", 4), wgen.make_window(32, "passive", 5), wgen.make_window(48, "preloaded", 6)]
+    specs = [WindowSpec(w.n, w.particles, tau=0.9, force=(1e-5, 0.0, 0.0), subsamples=2) for w in wins]
+    b = PscBatch(specs, precision="fp32", graph_steps=4, kernel=k)
+    res = b.run_to_convergence(tol=1e-5, check_every=40, max_steps=4000)
+    assert res["converged"].all()
+    assert len(set(res["steps"].tolist())) > 1  # windows converge at different steps
+    kb = b.permeability()
+    for j, spec in enumerate(specs):
+        solo = PscBatch([spec], precision="fp32", graph_steps=0, kernel=k)
+        solo.run(int(res["steps"][j]))
+        assert solo.permeability()[0] == kb[j]
+        assert np.array_equal(solo.velocity_field(0), b.velocity_field(j))
+    assert ctypes_status() == 0
