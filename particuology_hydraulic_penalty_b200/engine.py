@@ -197,6 +197,15 @@ class DeviceGeometry:
         return changed
 
     def struct(self) -> nat.PscGeometry:
+        """The psc_geometry descriptor (cached; rebuilt when a buffer or size changes)."""
+        key = (self.P, self.cap_entries, self.cap_chunks, self.particles.data_ptr() if self.particles.numel() else 0,
+               self.bbox.data_ptr() if self.bbox is not None else 0)
+        if getattr(self, "_struct_key", None) != key:
+            self._struct_cache = self._make_struct()
+            self._struct_key = key
+        return nat.PscGeometry.from_buffer_copy(self._struct_cache)  # callers may edit their copy
+
+    def _make_struct(self) -> nat.PscGeometry:
         g = nat.PscGeometry()
         g.nx, g.ny, g.nz = self.nx, self.ny, self.nz
         g.subsamples = self.subsamples

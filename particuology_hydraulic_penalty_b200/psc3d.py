@@ -119,8 +119,10 @@ class PscD3Q19:
             self._P = parr.shape[0]
             self._forces_dev = torch.zeros((self._P, 3), dtype=torch.float64, device=self._device)
             self._torques_dev = torch.zeros((self._P, 3), dtype=torch.float64, device=self._device)
-            self._diag_dev = torch.zeros(nat.NDIAG, dtype=torch.float64, device=self._device)
+            # post-stream reductions and load diagnostics land in one buffer read back per call
             self._out_dev = torch.zeros(nat.NRED + nat.NDIAG, dtype=torch.float64, device=self._device)
+            self._red_post_dev = self._out_dev[: nat.NRED]
+            self._diag_dev = self._out_dev[nat.NRED:]
             self._out_host = torch.zeros(nat.NRED + nat.NDIAG, dtype=torch.float64).pin_memory()
         self._geometry_built = False
         self._stepped = False
@@ -170,18 +172,18 @@ class PscD3Q19:
     # ------------------------------------------------------------------
     def collide_stream_psc(self) -> dict:
         """One PSC-IMB collide + stream step (psc3d.py:208-253)."""
-        if (not self.static_geometry) or (not self._geometry_built):
-            self.rebuild_geometry()
-        else:
-            # positions / velocities may have been mutated in place: they feed
-            # the solid velocity and the torque arms even for static geometry
-            self._upload_particles()
-            if not self._geometry_built:
-                self.rebuild_geometry()
-        parr = self._geo.host_particles
-        moving = bool(parr.shape[0]) and bool(np.any(parr[:, 4:10] != 0.0))
-        win = self._win
         with torch.cuda.device(self._device):
+            if (not self.static_geometry) or (not self._geometry_built):
+                self.rebuild_geometry()
+            else:
+                # positions / velocities may have been mutated in place: they feed
+                # the solid velocity and the torque arms even for static geometry
+                self._upload_particles()
+                if not self._geometry_built:
+                    self.rebuild_geometry()
+            parr = self._geo.host_particles
+            moving = bool(parr.shape[0]) and bool(np.any(parr[:, 4:10] != 0.0))
+            win = self._win
             if moving:
                 self._geo.solid_velocity(win.ensure_us())
             win.set_moving(moving)
@@ -189,9 +191,7 @@ class PscD3Q19:
             win.reduce(win.red)
             self._geo.loads(win.imb, win.red[nat.RED_IMBX:], self._forces_dev, self._torques_dev, self._diag_dev)
             # reductions of the post-stream state only; the fields are made on access
-            win.moments_pass(win.red_post, write_fields=False)
-            self._out_dev[: nat.NRED].copy_(win.red_post)
-            self._out_dev[nat.NRED:].copy_(self._diag_dev)
+            win.moments_pass(self._red_post_dev, write_fields=False)
             self._out_host.copy_(self._out_dev, non_blocking=True)
             torch.cuda.current_stream(self._device).synchronize()
         self._stepped = True
