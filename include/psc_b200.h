@@ -126,6 +126,8 @@ typedef struct psc_window {
     void* imb;             /* IMB momentum [3][N] (double in F64 modes, float otherwise) */
     void* moments;         /* rho, ux, uy, uz [4][N] (same element type as imb) */
     double* partials;      /* [tile_count][PSC_NRED] */
+    double tau_minus;      /* TRT: antisymmetric relaxation time (0 = BGK, the reference's collision);
+                              deviation storage modes only */
 } psc_window;
 
 /* Particle-derived geometry of ONE window (device arrays, caller-owned).

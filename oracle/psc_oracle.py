@@ -409,3 +409,35 @@ def darcy_permeability(solid: np.ndarray, u_along: np.ndarray, tau: float, force
         "mean_u_fluid": float(np.sum(weighted) / max(fluid_volume, 1.0e-300)),
         "permeability_lu": float(nu * superficial / max(force_mag, 1.0e-300)),
     }
+
+
+def collide_trt_deviation(g: np.ndarray, solid: np.ndarray, tau: float, tau_minus: float, force=(0.0, 0.0, 0.0)):
+    """Two-relaxation-time variant of :func:`collide` (static particles), on deviations g = f - w.
+
+    EXTENSION beyond the reference (which is BGK only, psc3d.py:221): the
+    fluid operator relaxes the symmetric part (f_i + f_opp)/2 with 1/tau and
+    the antisymmetric part (f_i - f_opp)/2 with 1/tau_minus; Guo's
+    antisymmetric term 3 w c.F takes the prefactor 1 - 1/(2 tau_minus).  The
+    PSC term and B are the reference's.  tau_minus = tau is BGK.
+    """
+    F = np.asarray(force, dtype=np.float64)
+    Cf = C.astype(np.float64)
+    Wb = W[:, None, None, None]
+    drho = g.sum(axis=0)
+    rho = 1.0 + drho
+    m = np.einsum("ia,i...->a...", Cf, g)
+    ue = (m + F[:, None, None, None]) / rho
+    uu = (ue * ue).sum(axis=0)
+    uF = np.einsum("a,a...->...", F, ue)
+    cu = np.einsum("ia,a...->i...", Cf, ue)
+    cF = (Cf @ F)[:, None, None, None]
+    geq = Wb * (drho + rho * (3.0 * cu + 4.5 * cu * cu - 1.5 * uu))
+    alpha = np.clip(solid, 0.0, 1.0)
+    B = alpha / (alpha + tau * (1.0 - alpha) + 1.0e-14)
+    os_ = g[OPP] - g + Wb * drho - geq[OPP]
+    gp, gm = 0.5 * (g + g[OPP]), 0.5 * (g - g[OPP])
+    ep, em = 0.5 * (geq + geq[OPP]), 0.5 * (geq - geq[OPP])
+    fluid = -(gp - ep) / tau - (gm - em) / tau_minus
+    pref_p, pref_m = 1.0 - 0.5 / tau, 1.0 - 0.5 / tau_minus
+    G = Wb * (pref_p * (-3.0 * uF + 9.0 * cu * cF) + pref_m * 3.0 * cF)
+    return g + (1.0 - B) * fluid + B * os_ + G

@@ -76,6 +76,7 @@ class PscWindow(ctypes.Structure):
         ("tau", c_double), ("force", c_double * 3), ("store_scale", c_double),
         ("f_src", c_void_p), ("f_dst", c_void_p), ("solid", c_void_p), ("level", c_void_p),
         ("us", c_void_p), ("imb", c_void_p), ("moments", c_void_p), ("partials", c_void_p),
+        ("tau_minus", c_double),
     ]
 
 

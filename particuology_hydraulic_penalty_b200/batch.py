@@ -22,7 +22,7 @@ import torch
 
 from . import _native as nat
 from .engine import (DeviceGeometry, LatticeWindow, particles_array, require_cuda, store_mode, stream_handle,
-                     struct_to_device, vp)
+                     struct_to_device, trt_tau_minus, vp)
 
 
 @dataclass
@@ -35,6 +35,7 @@ class WindowSpec:
     force: tuple = (1.0e-6, 0.0, 0.0)
     subsamples: int = 4
     name: str = ""
+    collision: str = "bgk"  # "bgk" (the reference) or "trt" (magic parameter 3/16)
 
 
 class PscBatch:
@@ -86,7 +87,11 @@ class PscBatch:
         with torch.cuda.device(self.device):
             for s in self.specs:
                 shape = (s.n, s.n, s.n)
-                win = LatticeWindow(shape, s.tau, s.force, s.subsamples, self.store, store_scale, self.device)
+                if s.collision not in ("bgk", "trt"):
+                    raise ValueError("collision must be 'bgk' or 'trt'")
+                tm = trt_tau_minus(s.tau) if s.collision == "trt" else 0.0
+                win = LatticeWindow(shape, s.tau, s.force, s.subsamples, self.store, store_scale, self.device,
+                                    tau_minus=tm)
                 geo = DeviceGeometry(shape, s.subsamples, self.device, want_level=self.store != nat.STORE_F64_EXACT)
                 geo.set_particles(particles_array(s.particles))
                 geo.rebuild()

@@ -218,6 +218,7 @@ int psc_step_ex(int store, const psc_window* d_windows, int nwin, int64_t total_
     const bool moving = (flags & PSC_STEP_MOVING) != 0;
     cudaError_t e;
     if (store == PSC_STORE_F64_EXACT) {
+        // (TRT windows are rejected by the hosts that build tables; the exact kernel runs BGK)
         if (c.cells_per_thread != 1)
             return fail(PSC_E_UNSUPPORTED, "psc_step: PSC_STORE_F64_EXACT runs one cell per thread");
         e = launch_step(store, d_windows, nwin, total_tiles, flags, moving, c.grid_ctas, as_stream(stream));

@@ -247,16 +247,23 @@ namespace psc {
 template <typename R>
 struct WinConst {
     R inv_tau;
+    R trt_ratio;  // omega- / omega+ (1 for BGK)
     R fx, fy, fz;
     R pw3[3];  // 3 pref w for the rest, axis and diagonal weights
     R A[9];    // 3 pref w_k (c_k . F) for the nine direction pairs
     R K[9];    // 9 pref w_k (c_k . F)
 };
 
+// tau_minus > 0 selects two-relaxation-time collision (symmetric parts relax
+// with 1/tau, antisymmetric with 1/tau_minus; Guo's antisymmetric term takes
+// the prefactor 1 - 1/(2 tau_minus)).  tau_minus = tau is BGK.
 template <typename R>
-PSC_HD void make_win_const(WinConst<R>& c, double tau, double fx, double fy, double fz) {
+PSC_HD void make_win_const(WinConst<R>& c, double tau, double fx, double fy, double fz, double tau_minus = 0.0) {
     const double pref = 1.0 - 0.5 / tau;
+    const double tm = tau_minus > 0.0 ? tau_minus : tau;
+    const double pref_m = 1.0 - 0.5 / tm;
     c.inv_tau = (R)(1.0 / tau);
+    c.trt_ratio = (R)(tau / tm);
     c.fx = (R)fx;
     c.fy = (R)fy;
     c.fz = (R)fz;
@@ -267,7 +274,7 @@ PSC_HD void make_win_const(WinConst<R>& c, double tau, double fx, double fy, dou
         const int i = 2 * k + 1;
         const double w = wgt(i);
         const double cf = cxv(i) * fx + cyv(i) * fy + czv(i) * fz;
-        c.A[k] = (R)(3.0 * pref * w * cf);
+        c.A[k] = (R)(3.0 * pref_m * w * cf);
         c.K[k] = (R)(9.0 * pref * w * cf);
     }
 }
@@ -275,9 +282,11 @@ PSC_HD void make_win_const(WinConst<R>& c, double tau, double fx, double fy, dou
 // Collide deviations g in place.  B solid weight, kb = (1 - B) / tau.
 // mom receives rho - 1 and the moment velocity u = (m + F/2)/rho of the
 // incoming state; imb the node IMB momentum when IMB.
-template <typename R, bool MOVING, bool IMB>
+template <typename R, bool MOVING, bool IMB, bool TRT = false>
 PSC_HD void collide_fast2(R* g, const WinConst<R>& c, R B, R kb, R usx, R usy, R usz, R irho_hint, R* mom,
                           R* imb) {
+    const R kbm = kb * c.trt_ratio;
+    (void)kbm;
     const R drho = (((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7]))) +
                    (((g[8] + g[9]) + (g[10] + g[11])) + ((g[12] + g[13]) + (g[14] + g[15]))) +
                    ((g[16] + g[17]) + g[18]);
@@ -324,8 +333,17 @@ PSC_HD void collide_fast2(R* g, const WinConst<R>& c, R B, R kb, R usx, R usy, R
         const R os_i = (d + e) + h;
         const R os_j = (e - d) - h;
         const R Gb = c.K[k] * cu - c.pw3[cls] * uF;
-        g[i] = omk * gi + kb * geq_i + B * os_i + (Gb + c.A[k]);
-        g[j] = omk * gj + kb * geq_j + B * os_j + (Gb - c.A[k]);
+        if (TRT) {
+            // symmetric part relaxes with kb, antisymmetric with kb * omega-/omega+
+            const R sym_neq = R(0.5) * (gi + gj) - (wdrho + wrq);
+            const R asym_neq = R(-0.5) * d - asym;
+            const R relax_s = kb * sym_neq, relax_a = kbm * asym_neq;
+            g[i] = gi - relax_s - relax_a + B * os_i + (Gb + c.A[k]);
+            g[j] = gj - relax_s + relax_a + B * os_j + (Gb - c.A[k]);
+        } else {
+            g[i] = omk * gi + kb * geq_i + B * os_i + (Gb + c.A[k]);
+            g[j] = omk * gj + kb * geq_j + B * os_j + (Gb - c.A[k]);
+        }
         if (IMB) {
             const R dm = B * (os_i - os_j);
             ax += csel(cxv(i), dm);

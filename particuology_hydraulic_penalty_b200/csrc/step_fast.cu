@@ -31,6 +31,7 @@ struct FastWin {
     int32_t tile_cells;
     int32_t moving;
     int32_t inactive;
+    int32_t trt;
     R scale, inv_scale;
     WinConst<R> c;
     R Blut[256];
@@ -67,7 +68,8 @@ __device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool mov
         s.scale = (R)W.store_scale;
         s.inv_scale = (R)(1.0 / W.store_scale);
         s.tau = (R)W.tau;
-        make_win_const(s.c, W.tau, W.force[0], W.force[1], W.force[2]);
+        make_win_const(s.c, W.tau, W.force[0], W.force[1], W.force[2], W.tau_minus);
+        s.trt = W.tau_minus > 0.0 ? 1 : 0;
     }
     const int S = W.subsamples;
     const int S3 = S * S * S;
@@ -182,7 +184,10 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
                            ((g[16] + g[17]) + g[18]);
             const R irho = fast_rcp<R>(R(1) + drho);
             if (do_collide) {
-                if (do_imb || do_red) {
+                if (sw.trt) {
+                    if (moving) collide_fast2<R, MOVING, true, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+                    else collide_fast2<R, false, true, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+                } else if (do_imb || do_red) {
                     if (moving) collide_fast2<R, MOVING, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
                     else collide_fast2<R, false, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
                 } else {

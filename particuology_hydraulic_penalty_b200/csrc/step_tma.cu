@@ -90,6 +90,7 @@ struct TmaWin {
     uint32_t nx, ny, nz, N, ty, nyb;
     int32_t moving;
     int32_t inactive;
+    int32_t trt;
     R scale, inv_scale, tau;
     WinConst<R> c;
     R Blut[256];
@@ -243,7 +244,8 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
                 sw.scale = (R)W.store_scale;
                 sw.inv_scale = (R)(1.0 / W.store_scale);
                 sw.tau = (R)W.tau;
-                make_win_const(sw.c, W.tau, W.force[0], W.force[1], W.force[2]);
+                make_win_const(sw.c, W.tau, W.force[0], W.force[1], W.force[2], W.tau_minus);
+                sw.trt = W.tau_minus > 0.0 ? 1 : 0;
             }
             consumer_sync();
             {
@@ -321,7 +323,10 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
             }
             R mom[4], imb[3] = {R(0), R(0), R(0)};
             if (do_collide) {
-                if (do_imb || do_red) {
+                if (sw.trt) {
+                    if (moving) collide_fast2<R, MOVING, true, true>(g, sw.c, B, kb, usx, usy, usz, R(0), mom, imb);
+                    else collide_fast2<R, false, true, true>(g, sw.c, B, kb, usx, usy, usz, R(0), mom, imb);
+                } else if (do_imb || do_red) {
                     if (moving) collide_fast2<R, MOVING, true>(g, sw.c, B, kb, usx, usy, usz, R(0), mom, imb);
                     else collide_fast2<R, false, true>(g, sw.c, B, kb, usx, usy, usz, R(0), mom, imb);
                 } else {

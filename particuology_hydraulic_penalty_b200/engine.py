@@ -50,6 +50,12 @@ Q = 19
 PARTICLE_FIELDS = ("x", "y", "z", "r", "vx", "vy", "vz", "wx", "wy", "wz")
 
 
+def trt_tau_minus(tau: float, magic: float = 3.0 / 16.0) -> float:
+    """Antisymmetric relaxation time of TRT from the magic parameter
+    Lambda = (tau - 1/2)(tau_minus - 1/2) (3/16 places bounce-back walls half-way)."""
+    return 0.5 + magic / (tau - 0.5)
+
+
 def store_mode(precision: str) -> int:
     try:
         return PRECISIONS[precision]
@@ -318,13 +324,16 @@ class LatticeWindow:
     """Populations and per-cell fields of one periodic window on the device."""
 
     def __init__(self, shape, tau: float, force, subsamples: int, store: int, store_scale: float | None,
-                 device):
+                 device, tau_minus: float = 0.0):
         self.nx, self.ny, self.nz = (int(v) for v in shape)
         self.N = self.nx * self.ny * self.nz
         self.tau = float(tau)
+        self.tau_minus = float(tau_minus)
         self.force = tuple(float(v) for v in force)
         self.subsamples = int(subsamples)
         self.store = int(store)
+        if self.tau_minus > 0.0 and self.store == nat.STORE_F64_EXACT:
+            raise ValueError("TRT collision runs in the deviation storage modes (fp64, fp32, fp16, bf16)")
         self.store_scale = float(DEFAULT_STORE_SCALE[self.store] if store_scale is None else store_scale)
         if self.store_scale <= 0.0 or not np.isfinite(self.store_scale):
             raise ValueError("store_scale must be a positive finite number")
@@ -383,6 +392,7 @@ class LatticeWindow:
         w.subsamples = self.subsamples
         w.flags = nat.WIN_MOVING if self.moving else 0
         w.tau = self.tau
+        w.tau_minus = self.tau_minus
         w.force[0], w.force[1], w.force[2] = self.force
         w.store_scale = self.store_scale
         w.f_src = vp(self.f[src])

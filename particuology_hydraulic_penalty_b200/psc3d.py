@@ -13,6 +13,8 @@ Extra keyword-only arguments (absent from the reference):
     force       body-force vector (fx, fy, fz); default (0, 0, body_force_z)
     store_scale scale of the FP16/BF16 stored deviations
     device      CUDA device
+    collision   "bgk" (default, the reference) or "trt" (two relaxation times,
+                magic parameter 3/16; deviation storage modes only)
 """
 
 from __future__ import annotations
@@ -23,7 +25,7 @@ import numpy as np
 import torch
 
 from . import _native as nat
-from .engine import (DeviceGeometry, LatticeWindow, particles_array, require_cuda, store_mode)
+from .engine import (DeviceGeometry, LatticeWindow, particles_array, require_cuda, store_mode, trt_tau_minus)
 
 # D3Q19 velocity set in the reference's index order (psc3d.py:17-43).
 C = np.array(
@@ -91,7 +93,7 @@ class PscD3Q19:
 
     def __init__(self, n: int, particles, tau: float = 0.72, subsamples: int = 4, body_force_z: float = 0.0,
                  static_geometry: bool = False, *, precision: str = "fp64-exact", force=None,
-                 store_scale: float | None = None, device=None):
+                 store_scale: float | None = None, device=None, collision: str = "bgk"):
         self._device = require_cuda(device)
         self.n = int(n)
         if self.n <= 0:
@@ -106,10 +108,14 @@ class PscD3Q19:
         self.force = (0.0, 0.0, self.body_force_z) if force is None else tuple(float(v) for v in force)
         if len(self.force) != 3:
             raise ValueError("force must have three components")
+        if collision not in ("bgk", "trt"):
+            raise ValueError("collision must be 'bgk' (the reference) or 'trt'")
+        self.collision = collision
         shape = (self.n,) * 3
         with torch.cuda.device(self._device):
             self._win = LatticeWindow(shape, self.tau, self.force, self.subsamples, self._store, store_scale,
-                                      self._device)
+                                      self._device,
+                                      tau_minus=trt_tau_minus(self.tau) if collision == "trt" else 0.0)
             self._geo = DeviceGeometry(shape, self.subsamples, self._device,
                                        want_level=self._store != nat.STORE_F64_EXACT)
             self._win.bind_geometry(self._geo)

@@ -165,3 +165,33 @@ def test_converged_windows_freeze_exactly(kernel):
         assert solo.permeability()[0] == kb[j]
         assert np.array_equal(solo.velocity_field(0), b.velocity_field(j))
     assert ctypes_status() == 0
+
+
+@pytest.mark.parametrize("kernel", ["direct", "tma"])
+def test_trt_matches_oracle(kernel):
+    """TRT (magic 3/16) on the GPU in FP64 against the oracle's TRT extension, 6 steps."""
+    from oracle import psc_oracle as orc
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+    from particuology_hydraulic_penalty_b200.engine import trt_tau_minus
+
+    w = small_windows()[1]
+    tau, F = 0.8, (1e-5, 0.0, 3e-6)
+    spec = WindowSpec(w.n, w.particles, tau=tau, force=F, subsamples=2, collision="trt")
+    k = {"direct": nat.KERNEL_DIRECT, "tma": nat.KERNEL_TMA}[kernel]
+    b = PscBatch([spec], precision="fp64", graph_steps=0, kernel=k)
+    b.run(6)
+    geo = orc.voxelize(w.particles, w.n, 2)
+    g = np.zeros((19,) + (w.n,) * 3)
+    S = g
+    for _ in range(6):
+        S = orc.collide_trt_deviation(orc.stream_push(S), geo.solid, tau, trt_tau_minus(tau), F)
+    f = orc.stream_push(S)
+    rho = 1.0 + f.sum(axis=0)
+    ux = (np.einsum("i,i...->...", orc.C[:, 0].astype(float), f) + 0.5 * F[0]) / rho
+    mom = b.velocity_field(0)
+    assert np.abs(mom[1] - ux).max() <= 1e-12 * np.abs(ux).max()
+    # TRT differs from BGK on the same window
+    bb = PscBatch([WindowSpec(w.n, w.particles, tau=tau, force=F, subsamples=2)], precision="fp64", graph_steps=0)
+    bb.run(6)
+    assert np.abs(bb.velocity_field(0)[1] - mom[1]).max() > 1e-3 * np.abs(ux).max()

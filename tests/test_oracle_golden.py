@@ -72,3 +72,16 @@ def test_reference_smoke_assertions_hold_on_oracle():
     assert np.isfinite(s.f).all()
     assert np.isfinite(s.hydro_forces).all()
     assert np.isfinite(d["momentum_residual"])
+
+
+def test_trt_extension_reduces_to_bgk():
+    """The oracle's TRT extension with tau_minus = tau equals the reference collision."""
+    rng = np.random.default_rng(2)
+    shp = (5, 5, 5)
+    f = orc.equilibrium(1 + rng.normal(0, 1e-3, shp), *rng.normal(0, 1e-3, (3,) + shp))
+    f = f + rng.normal(0, 1e-6, f.shape) * orc.W[:, None, None, None]
+    solid = rng.choice([0.0, 0.25, 1.0], size=shp)
+    F = (1e-5, 0.0, 2e-6)
+    post, _ = orc.collide(f, solid, None, 0.8, F)
+    trt = orc.collide_trt_deviation(f - orc.W[:, None, None, None], solid, 0.8, 0.8, F)
+    assert np.abs(trt + orc.W[:, None, None, None] - post).max() <= 2e-16
