@@ -40,7 +40,7 @@ CS2 = 1.0 / 3.0
 
 
 def _to_dev(a, dev):
-    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    return torch.from_numpy(np.array(a, dtype=np.float64, order="C")).to(dev)  # writable copy
 
 
 def equilibrium(rho, ux, uy, uz) -> np.ndarray:
