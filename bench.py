@@ -14,8 +14,14 @@ Also reported on the same line:
                  storage, one launch per step, no graph): MLUPS, windows/hour
                  at 5000 steps, and the FP32/FP64 permeability difference
                  after the same number of steps from rest
-  e2e         -- MLUPS through the drop-in SparsePscD3Q19.collide_stream_psc()
-                 (particle upload, step, loads, diagnostics read back per call)
+  fp64_exact_dropin -- the plain FP64 drop-in (reference arithmetic, per-call
+                 diagnostics), one window at a time, and the windows/hour ratio
+  e2e         -- MLUPS through the batched C ABI with host buffers: every step
+                 uploads each window's particle array and reads back every
+                 window's diagnostics (psc_batch_set_particles + psc_batch_step)
+  e2e_dropin  -- MLUPS through the drop-in SparsePscD3Q19.collide_stream_psc(),
+                 one window per call (particle upload, step, loads,
+                 diagnostics read back per call)
   roofline    -- achieved HBM GB/s of the step kernel vs the measured peak
   cpu_baseline-- the NumPy oracle port on this host's cores (bounded sample)
 
@@ -283,11 +289,12 @@ def run_fp64_exact_dropin(windows, steps: int, warm: int = 2):
     return per_window
 
 
-def run_e2e(windows, steps: int):
-    """MLUPS through the drop-in class (host particle upload + diagnostics read back per call)."""
+def run_e2e_dropin(windows, steps: int):
+    """MLUPS through the drop-in class, one window at a time (host particle upload + diagnostics read back per call)."""
     import torch
 
     from particuology_hydraulic_penalty_b200 import SparsePscD3Q19
+    from particuology_hydraulic_penalty_b200 import _native as nat
 
     solvers = [SparsePscD3Q19(w.n, w.particles, tau=TAU, subsamples=SUBSAMPLES, static_geometry=True,
                               precision="fp32", force=FORCE) for w in windows]
@@ -295,22 +302,54 @@ def run_e2e(windows, steps: int):
         s.collide_stream_psc()
     torch.cuda.synchronize()
     h2d = sum(int(w.particles.nbytes) for w in windows)
-    P = [w.particles.shape[0] for w in windows]
-    from particuology_hydraulic_penalty_b200 import _native as nat
-
-    d2h = sum((nat.NRED + nat.NDIAG + 6 * p) * 8 for p in P)
+    d2h = len(windows) * (2 * nat.NRED + nat.NDIAG) * 8  # reductions + diagnostics of each call
     t0 = time.perf_counter()
     for _ in range(steps):
         for s in solvers:
             s.collide_stream_psc()
-    torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     cells = sum(w.n ** 3 for w in windows)
     del solvers
     torch.cuda.empty_cache()
-    return {"value": cells * steps / wall / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "api": "SparsePscD3Q19.collide_stream_psc() per window, precision=fp32, static geometry",
-            "steps": steps}
+    return {"value": round(cells * steps / wall / 1e6, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "api": "SparsePscD3Q19(precision='fp32').collide_stream_psc() per window (one psc_step call each), "
+                   "static geometry", "steps": steps}
+
+
+def run_e2e_batch(windows, steps: int, graph_steps: int):
+    """MLUPS through the batched C ABI with host buffers: every step uploads each window's particle
+    array (psc_batch_set_particles) and reads back every window's diagnostics (psc_batch_step with
+    PSC_RUN_DIAG: particle loads, post-stream reductions, Darcy K)."""
+    import torch
+
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.handle import BatchHandle, make_config
+
+    cfgs = [make_config((w.n,) * 3, tau=TAU, force=FORCE, subsamples=SUBSAMPLES, store=nat.STORE_F32)
+            for w in windows]
+    b = BatchHandle(cfgs, graph_steps=graph_steps)
+    for k, w in enumerate(windows):
+        b.set_particles(k, w.particles)
+    b.step(3, nat.RUN_DIAG)  # voxelisation and first launches outside the timed region
+    h2d = sum(int(w.particles.nbytes) for w in windows)
+    d2h = len(windows) * (2 * nat.NRED + nat.NDIAG) * 8
+    k_sum = 0.0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for k, w in enumerate(windows):
+            b.set_particles(k, w.particles)
+        st = b.step(1, nat.RUN_DIAG)
+        k_sum += st[0].diag.permeability
+    wall = time.perf_counter() - t0
+    cells = sum(w.n ** 3 for w in windows)
+    b.close()
+    torch.cuda.empty_cache()
+    return {"value": round(cells * steps / wall / 1e6, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "finite": bool(np.isfinite(k_sum)),
+            "api": "C ABI psc_batch_set_particles (every window) + psc_batch_step(1, PSC_RUN_DIAG) per step: "
+                   "host particle arrays in, per-window diagnostics and Darcy K out, one persistent launch for "
+                   "all windows", "steps": steps}
 
 
 WORKLOADS = {
@@ -423,7 +462,8 @@ def run_ours(args):
             "steps_per_window_assumed": STEPS_PER_WINDOW,
         }
     if rank == 0 and world == 1 and not args.no_e2e:
-        out["e2e"] = run_e2e(wins, steps=args.e2e_steps)
+        out["e2e"] = run_e2e_batch(wins, steps=args.e2e_steps, graph_steps=args.graph_steps)
+        out["e2e_dropin"] = run_e2e_dropin(wins, steps=max(3, args.e2e_steps // 4))
     elif rank == 0:
         out["e2e"] = None
     if cpu is not None:
@@ -481,7 +521,7 @@ def main():
     ap.add_argument("--kernel", choices=["direct", "tma"], default="direct")
     ap.add_argument("--autotune", action="store_true", help="pick the launch with the project autotuner first")
     ap.add_argument("--fp64-steps", type=int, default=20)
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")

@@ -13,8 +13,13 @@
  *  - Every function returns PSC_OK (0) or a negative PSC_E* code; the message
  *    of the last failure on the calling thread is psc_last_error().
  *  - All array pointers are DEVICE pointers unless the parameter name starts
- *    with "h_".  The caller allocates every buffer; no entry point here
- *    allocates device memory.  Sizes come from the *_bytes / plan queries.
+ *    with "h_".  Two layers:
+ *      descriptor layer (psc_window / psc_geometry / psc_adjoint_args): the
+ *        caller allocates every buffer and no entry point allocates device
+ *        memory; sizes come from the *_bytes / plan queries;
+ *      handle layer (psc_solver / psc_batch, at the end of this file): the
+ *        reference's solver object -- the handle owns its device memory,
+ *        stream and CUDA graphs and takes and returns HOST arrays.
  *  - "stream" is a cudaStream_t passed as void* (NULL = legacy default stream).
  *    Work is enqueued asynchronously; nothing synchronises unless stated.
  *  - Lattice layout: structure of arrays, population plane i of a window is
@@ -37,7 +42,7 @@
 extern "C" {
 #endif
 
-#define PSC_ABI_VERSION 1
+#define PSC_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------- */
 #define PSC_OK 0
@@ -65,7 +70,7 @@ extern "C" {
 #define PSC_KERNEL_DIRECT 1 /* per-thread coalesced pulls (any window) */
 #define PSC_KERNEL_TMA 2    /* bulk-copy (TMA) row staging in shared memory */
 
-/* Launch configuration of psc_step_ex(). */
+/* Launch configuration of psc_step_windows_ex(). */
 typedef struct psc_launch {
     int32_t grid_ctas;        /* persistent grid size; 0 = SM count x occupancy */
     int32_t cells_per_thread; /* 1, 2 or 4; the windows must be planned with tile_cells = 256 x this */
@@ -106,7 +111,7 @@ typedef struct psc_launch {
 #define PSC_NDIAG 6
 
 /* One lattice window of a (batched) launch.  Lives in device memory; the
- * array of windows handed to psc_step() is a device pointer.  All windows of
+ * array of windows handed to psc_step_windows() is a device pointer.  All windows of
  * one launch share the storage mode. */
 typedef struct psc_window {
     int32_t nx, ny, nz;    /* lattice extent (the reference's n, n, n) */
@@ -231,11 +236,11 @@ int psc_solid_velocity(const psc_geometry* h_geo, int us_type, void* us, void* s
 /* One pull-stream + collide pass over every tile of every window.
  * d_windows: device array of nwin windows; total_tiles from psc_plan_tiles;
  * grid_ctas = 0 picks a persistent grid (a multiple of the SM count). */
-int psc_step(int store, const struct psc_window* d_windows, int nwin, int64_t total_tiles,
+int psc_step_windows(int store, const struct psc_window* d_windows, int nwin, int64_t total_tiles,
              unsigned flags, int grid_ctas, void* stream);
-/* psc_step with an explicit launch configuration (kernel variant, cells per
+/* psc_step_windows with an explicit launch configuration (kernel variant, cells per
  * thread, grid); cfg may be NULL for the defaults. */
-int psc_step_ex(int store, const struct psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
+int psc_step_windows_ex(int store, const struct psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
                 const psc_launch* cfg, void* stream);
 /* Sum the per-tile partials of each window in a fixed order (deterministic)
  * into out[nwin][PSC_NRED] (device). */
@@ -309,6 +314,147 @@ int psc_stream_push(int store, double store_scale, const void* src, double* dst,
 /* Inverse: absolute FP64 post-stream f -> stored representation. */
 int psc_stream_pull_store(int store, double store_scale, const double* src, void* dst, int nx, int ny, int nz,
                           void* stream);
+
+/* ======================================================================== *
+ * Handle layer: the reference's solver object (PscD3Q19 / SparsePscD3Q19,  *
+ * psc3d.py:117-407) and batches of windows.  A handle owns its device      *
+ * memory (allocated at creation and when a geometry grows), its stream and *
+ * its CUDA graphs; every array argument is a HOST array.  Functions that   *
+ * return data synchronise the handle's stream.  Handles are not            *
+ * thread-safe; distinct handles are independent.                           *
+ * ======================================================================== */
+
+/* Configuration of one lattice window (PscD3Q19.__init__, psc3d.py:120-147). */
+typedef struct psc_config {
+    int32_t nx, ny, nz;       /* lattice extent (the reference's n, n, n) */
+    int32_t subsamples;       /* S (the reference's default: 4 dense, 3 sparse) */
+    int32_t store;            /* PSC_STORE_* */
+    int32_t static_geometry;  /* 0: voxelise again whenever the particles changed (psc3d.py:209-210) */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t conv_min_steps;   /* PSC_RUN_CONVERGE: never stop before this step of the call (>= 1) */
+    double tau;               /* BGK relaxation time (default 0.72 in the reference) */
+    double tau_minus;         /* TRT antisymmetric relaxation time; 0 = BGK, the reference's collision */
+    double force[3];          /* body force; the reference: (0, 0, body_force_z) */
+    double store_scale;       /* PSC_STORE_F16 / BF16 stored-deviation scale; 0 = the mode's default */
+    double conv_tol;          /* PSC_RUN_CONVERGE tolerance; 0 = 1e-8 (couple_psc_liggghts.py:168) */
+    void* stream;             /* cudaStream_t for all work of the handle; NULL = a stream of its own */
+} psc_config;
+
+/* Diagnostics of one step.  The first five are the reference's dictionary
+ * (psc3d.py:247-253); the rest are the Darcy quantities its callers derive
+ * (run_psc_permeability_resolution.py:144-160).  Moments are those of the
+ * post-stream state. */
+typedef struct psc_diag {
+    double solid_volume_lu;   /* sum of the clipped solid fraction */
+    double mean_uz;           /* mean post-stream u_z */
+    double momentum_residual; /* |sum_p F_p + sum_x imb| */
+    double max_force;         /* max_p |F_p| (0 without particles) */
+    double max_torque;        /* max_p |T_p| */
+    double mean_u[3];         /* mean post-stream velocity */
+    double superficial_u[3];  /* sum (1 - solid) u / N */
+    double fluid_volume_lu;   /* sum (1 - solid) */
+    double imb_sum[3];        /* sum of the node IMB momentum of the step */
+    double force_sum[3];      /* sum_p F_p */
+    double permeability;      /* nu (superficial_u . F) / |F|^2, nu = (tau - 1/2) / 3; 0 when F = 0 */
+    double nonfinite_cells;   /* cells with a non-finite moment (0 for a healthy run) */
+} psc_diag;
+
+typedef struct psc_status {
+    int32_t steps_done;       /* steps taken by this call */
+    int32_t converged;        /* PSC_RUN_CONVERGE / psc_batch_converge: criterion met */
+    double residual;          /* last relative change of the convergence quantity (inf if none) */
+    psc_diag diag;            /* diagnostics of the last step (PSC_RUN_DIAG / PSC_RUN_CONVERGE) */
+} psc_status;
+
+/* psc_step() flags */
+#define PSC_RUN_DIAG 1u     /* diagnostics and particle loads of the final step */
+#define PSC_RUN_CONVERGE 2u /* diagnostics every step; stop at the first step k >= conv_min_steps with
+                               |mean_uz_k - mean_uz_{k-1}| / |mean_uz_k| < conv_tol (lbm_converge,
+                               couple_psc_liggghts.py:284-296); implies PSC_RUN_DIAG */
+#define PSC_RUN_FIELDS 4u   /* also write the rho / u fields of the final state (else made on demand) */
+
+/* psc_get_fields() selectors; every field is returned as float64 */
+#define PSC_FIELD_RHO 0       /* [N] post-stream density (1 before the first step, psc3d.py:136) */
+#define PSC_FIELD_UX 1        /* [N] */
+#define PSC_FIELD_UY 2        /* [N] */
+#define PSC_FIELD_UZ 3        /* [N] (m_z + F_z/2) / rho, psc3d.py:243-246 */
+#define PSC_FIELD_SOLID 4     /* [N] clipped solid fraction */
+#define PSC_FIELD_IMB_X 5     /* [N] IMB momentum of the last step */
+#define PSC_FIELD_IMB_Y 6
+#define PSC_FIELD_IMB_Z 7
+#define PSC_FIELD_ALPHA_SUM 8 /* [N] unclipped alpha sum (alpha_sum_flat) */
+#define PSC_FIELD_US_X 9      /* [N] solid velocity (solid_velocity(), psc3d.py:181-206) */
+#define PSC_FIELD_US_Y 10
+#define PSC_FIELD_US_Z 11
+#define PSC_FIELD_F 12        /* [19][N] post-stream populations, absolute (PscD3Q19.f) */
+
+typedef struct psc_solver psc_solver;
+
+/* PscD3Q19(n, particles, tau, subsamples, body_force_z, static_geometry):
+ * populations at the rest equilibrium, no particles yet. */
+int psc_create(const psc_config* h_cfg, psc_solver** out);
+int psc_destroy(psc_solver* h);
+/* h_particles [P][10] (x, y, z, r, vx, vy, vz, wx, wy, wz: Particle3D).  Copied;
+ * read by the next step.  A changed array triggers a new voxelisation unless
+ * static_geometry is set (the reference re-reads positions and velocities
+ * every step for the solid velocity and torque arms in either case). */
+int psc_set_particles(psc_solver* h, const double* h_particles, int nparticles);
+/* rebuild_geometry() (psc3d.py:151-179 / 328-345), now. */
+int psc_rebuild_geometry(psc_solver* h);
+/* nsteps calls of collide_stream_psc() (psc3d.py:208-253).  h_status may be
+ * NULL.  Without PSC_RUN_DIAG the intermediate steps skip the reductions
+ * (they change no state); the IMB field of the final step is always written. */
+int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status);
+/* Field `which` (PSC_FIELD_*) as float64 into h_dst ([N], or [19][N] for PSC_FIELD_F). */
+int psc_get_fields(psc_solver* h, int which, double* h_dst);
+/* Set the post-stream populations (PscD3Q19.f = ...), absolute float64 [19][N]. */
+int psc_set_populations(psc_solver* h, const double* h_f);
+/* hydro_forces / hydro_torques [P][3] of the last step (accumulate_particle_loads,
+ * psc3d.py:255-281, computed here if the last step did not). */
+int psc_get_loads(psc_solver* h, double* h_forces, double* h_torques);
+/* accumulate_particle_loads() (psc3d.py:255-281): loads and diagnostics again
+ * from the last step's IMB field with the current geometry and particle
+ * state (torque arms use the current positions). */
+int psc_accumulate_particle_loads(psc_solver* h);
+/* Diagnostics of the last step (computed here if the last step did not). */
+int psc_get_diag(psc_solver* h, psc_diag* h_diag);
+/* Sparse solid fractions per particle (SparsePscD3Q19.node_ids / alpha_vals,
+ * psc3d.py:328-345): h_offsets [P+1] is always written; the ascending node
+ * ids and alphas of particle p go to h_ids / h_vals [h_offsets[p] ..
+ * h_offsets[p+1]) when capacity >= h_offsets[P] (else only the offsets,
+ * PSC_E_CAPACITY). */
+int psc_get_sparse_alpha(psc_solver* h, int64_t* h_offsets, int64_t* h_ids, double* h_vals, int64_t capacity);
+/* Particle count and lattice cells of the handle. */
+int psc_solver_info(psc_solver* h, int* h_nparticles, int64_t* h_cells);
+/* sizeof of the handle-layer structs as compiled into the library. */
+size_t psc_config_size(void);
+size_t psc_diag_size(void);
+size_t psc_status_size(void);
+
+/* ---- batches: many windows of uneven size, one persistent launch per step */
+typedef struct psc_batch psc_batch;
+
+/* nwin windows (all with the same store, device and stream).  launch may be
+ * NULL (direct kernel, one cell per thread, automatic grid); graph_steps
+ * (even, >= 2; 0 = none) steps are captured per CUDA graph and replayed. */
+int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_launch, int graph_steps,
+                     psc_batch** out);
+int psc_batch_destroy(psc_batch* b);
+/* Particles of window `win`; a changed array re-voxelises that window before the next step. */
+int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, int nparticles);
+/* nsteps steps of every active window.  PSC_RUN_DIAG: diagnostics and loads
+ * of every window at the final step into h_status[nwin] (may be NULL). */
+int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_status);
+/* Step until every window's Darcy permeability changes by less than tol per
+ * step, checked on a pair of consecutive steps every check_every steps; a
+ * converged window is frozen (its tiles skipped) when `freeze` is set.
+ * h_status[nwin]: steps to convergence (steps_done), converged flag, residual
+ * and the diagnostics of the reductions-only pass at the end. */
+int psc_batch_converge(psc_batch* b, double tol, int check_every, int max_steps, int min_steps, int freeze,
+                       psc_status* h_status);
+int psc_batch_get_diag(psc_batch* b, int win, psc_diag* h_diag);
+int psc_batch_get_loads(psc_batch* b, int win, double* h_forces, double* h_torques);
+int psc_batch_get_fields(psc_batch* b, int win, int which, double* h_dst);
 
 #ifdef __cplusplus
 }

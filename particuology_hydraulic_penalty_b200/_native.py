@@ -14,7 +14,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libpscb200.so"
 HEADER_PATH = Path(__file__).resolve().parents[1] / "include" / "psc_b200.h"
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # status codes
 PSC_OK = 0
@@ -110,6 +110,34 @@ class PscLaunch(ctypes.Structure):
                 ("stage_bytes", c_int32)]
 
 
+class PscConfig(ctypes.Structure):
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32), ("subsamples", c_int32), ("store", c_int32),
+        ("static_geometry", c_int32), ("device", c_int32), ("conv_min_steps", c_int32),
+        ("tau", c_double), ("tau_minus", c_double), ("force", c_double * 3), ("store_scale", c_double),
+        ("conv_tol", c_double), ("stream", c_void_p),
+    ]
+
+
+class PscDiag(ctypes.Structure):
+    _fields_ = [
+        ("solid_volume_lu", c_double), ("mean_uz", c_double), ("momentum_residual", c_double),
+        ("max_force", c_double), ("max_torque", c_double), ("mean_u", c_double * 3),
+        ("superficial_u", c_double * 3), ("fluid_volume_lu", c_double), ("imb_sum", c_double * 3),
+        ("force_sum", c_double * 3), ("permeability", c_double), ("nonfinite_cells", c_double),
+    ]
+
+
+class PscStatus(ctypes.Structure):
+    _fields_ = [("steps_done", c_int32), ("converged", c_int32), ("residual", c_double), ("diag", PscDiag)]
+
+
+# psc_step() flags and psc_get_fields() selectors
+RUN_DIAG, RUN_CONVERGE, RUN_FIELDS = 1, 2, 4
+FIELD_RHO, FIELD_UX, FIELD_UY, FIELD_UZ, FIELD_SOLID = 0, 1, 2, 3, 4
+FIELD_IMB_X, FIELD_IMB_Y, FIELD_IMB_Z, FIELD_ALPHA_SUM = 5, 6, 7, 8
+FIELD_US_X, FIELD_US_Y, FIELD_US_Z, FIELD_F = 9, 10, 11, 12
+
 # name -> (restype, argtypes); every function of include/psc_b200.h
 SIGNATURES = {
     "psc_abi_version": (c_int, []),
@@ -125,8 +153,8 @@ SIGNATURES = {
     "psc_geometry_plan": (c_int, [POINTER(PscGeometry), c_void_p]),
     "psc_geometry_build": (c_int, [POINTER(PscGeometry), c_void_p]),
     "psc_solid_velocity": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p]),
-    "psc_step": (c_int, [c_int, c_void_p, c_int, c_int64, c_uint, c_int, c_void_p]),
-    "psc_step_ex": (c_int, [c_int, c_void_p, c_int, c_int64, c_uint, POINTER(PscLaunch), c_void_p]),
+    "psc_step_windows": (c_int, [c_int, c_void_p, c_int, c_int64, c_uint, c_int, c_void_p]),
+    "psc_step_windows_ex": (c_int, [c_int, c_void_p, c_int, c_int64, c_uint, POINTER(PscLaunch), c_void_p]),
     "psc_reduce_windows": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "psc_particle_loads": (c_int, [POINTER(PscGeometry), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),
@@ -145,6 +173,30 @@ SIGNATURES = {
                                     c_double, c_uint, c_void_p, c_void_p]),
     "psc_stream_push": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "psc_stream_pull_store": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
+    # handle layer
+    "psc_create": (c_int, [POINTER(PscConfig), POINTER(c_void_p)]),
+    "psc_destroy": (c_int, [c_void_p]),
+    "psc_set_particles": (c_int, [c_void_p, c_void_p, c_int]),
+    "psc_rebuild_geometry": (c_int, [c_void_p]),
+    "psc_step": (c_int, [c_void_p, c_int, c_uint, POINTER(PscStatus)]),
+    "psc_get_fields": (c_int, [c_void_p, c_int, c_void_p]),
+    "psc_set_populations": (c_int, [c_void_p, c_void_p]),
+    "psc_get_loads": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "psc_get_diag": (c_int, [c_void_p, POINTER(PscDiag)]),
+    "psc_accumulate_particle_loads": (c_int, [c_void_p]),
+    "psc_get_sparse_alpha": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64]),
+    "psc_solver_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int64)]),
+    "psc_config_size": (c_size_t, []),
+    "psc_diag_size": (c_size_t, []),
+    "psc_status_size": (c_size_t, []),
+    "psc_batch_create": (c_int, [POINTER(PscConfig), c_int, POINTER(PscLaunch), c_int, POINTER(c_void_p)]),
+    "psc_batch_destroy": (c_int, [c_void_p]),
+    "psc_batch_set_particles": (c_int, [c_void_p, c_int, c_void_p, c_int]),
+    "psc_batch_step": (c_int, [c_void_p, c_int, c_uint, POINTER(PscStatus)]),
+    "psc_batch_converge": (c_int, [c_void_p, c_double, c_int, c_int, c_int, c_int, POINTER(PscStatus)]),
+    "psc_batch_get_diag": (c_int, [c_void_p, c_int, POINTER(PscDiag)]),
+    "psc_batch_get_loads": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "psc_batch_get_fields": (c_int, [c_void_p, c_int, c_int, c_void_p]),
 }
 
 _lib = None
@@ -170,7 +222,9 @@ def load(path: Path | None = None) -> ctypes.CDLL:
     if lib.psc_abi_version() != ABI_VERSION:
         raise NativeLibraryError("libpscb200.so ABI version mismatch: rebuild the library")
     if (lib.psc_window_size() != ctypes.sizeof(PscWindow) or lib.psc_geometry_size() != ctypes.sizeof(PscGeometry)
-            or lib.psc_adjoint_args_size() != ctypes.sizeof(PscAdjointArgs)):
+            or lib.psc_adjoint_args_size() != ctypes.sizeof(PscAdjointArgs)
+            or lib.psc_config_size() != ctypes.sizeof(PscConfig) or lib.psc_diag_size() != ctypes.sizeof(PscDiag)
+            or lib.psc_status_size() != ctypes.sizeof(PscStatus)):
         raise NativeLibraryError("libpscb200.so struct layout mismatch: rebuild the library")
     if path is None:
         _lib = lib

@@ -115,7 +115,7 @@ class PermeabilityProblem:
             table = struct_to_device(arr, self.device)
             size = ctypes.sizeof(nat.PscWindow)
             for k in range(L - 1):
-                nat.call("psc_step", self.store, ctypes.c_void_p(table.data_ptr() + k * size), 1, per,
+                nat.call("psc_step_windows", self.store, ctypes.c_void_p(table.data_ptr() + k * size), 1, per,
                          nat.STEP_COLLIDE, 0, stream_handle(self.device))
         return buf
 

@@ -1,6 +1,6 @@
 """Many pore windows of uneven size stepped by one persistent launch.
 
-Every step is ONE ``psc_step`` launch whose persistent grid walks the tiles
+Every step is ONE ``psc_step_windows_ex`` launch whose persistent grid walks the tiles
 of all windows; the windows' descriptors sit in two device tables (even and
 odd step parity).  Step sequences are captured once in a CUDA graph and
 replayed, so a run issues no per-step host work.  Reductions (Darcy flux,
@@ -169,7 +169,7 @@ class PscBatch:
 
     def _launch(self, flags: int) -> None:
         cfg = nat.PscLaunch(self.grid_ctas, self.cells_per_thread, self.kernel, self.stages, self.stage_bytes)
-        nat.call("psc_step_ex", self.store, vp(self._tables[self.parity]), self.nwin, self.total_tiles,
+        nat.call("psc_step_windows_ex", self.store, vp(self._tables[self.parity]), self.nwin, self.total_tiles,
                  flags, ctypes.byref(cfg), stream_handle(self.device))
 
     def _sync_cur(self) -> None:

@@ -206,42 +206,42 @@ int psc_solid_velocity(const psc_geometry* h_geo, int us_type, void* us, void* s
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_solid_velocity");
 }
 
-int psc_step_ex(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
+int psc_step_windows_ex(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
                 const psc_launch* cfg, void* stream) {
-    if (!valid_store(store)) return fail(PSC_E_INVALID, "psc_step: unknown storage mode");
-    if (!d_windows || nwin <= 0 || total_tiles < 0) return fail(PSC_E_INVALID, "psc_step: bad window list");
+    if (!valid_store(store)) return fail(PSC_E_INVALID, "psc_step_windows: unknown storage mode");
+    if (!d_windows || nwin <= 0 || total_tiles < 0) return fail(PSC_E_INVALID, "psc_step_windows: bad window list");
     psc_launch c = {0, 1, PSC_KERNEL_AUTO, 0, 0};
     if (cfg) c = *cfg;
-    if (c.grid_ctas < 0) return fail(PSC_E_INVALID, "psc_step: grid_ctas must be >= 0");
+    if (c.grid_ctas < 0) return fail(PSC_E_INVALID, "psc_step_windows: grid_ctas must be >= 0");
     if (c.cells_per_thread != 1 && c.cells_per_thread != 2 && c.cells_per_thread != 4)
-        return fail(PSC_E_INVALID, "psc_step: cells_per_thread must be 1, 2 or 4");
+        return fail(PSC_E_INVALID, "psc_step_windows: cells_per_thread must be 1, 2 or 4");
     const bool moving = (flags & PSC_STEP_MOVING) != 0;
     cudaError_t e;
     if (store == PSC_STORE_F64_EXACT) {
         // (TRT windows are rejected by the hosts that build tables; the exact kernel runs BGK)
         if (c.cells_per_thread != 1)
-            return fail(PSC_E_UNSUPPORTED, "psc_step: PSC_STORE_F64_EXACT runs one cell per thread");
+            return fail(PSC_E_UNSUPPORTED, "psc_step_windows: PSC_STORE_F64_EXACT runs one cell per thread");
         e = launch_step(store, d_windows, nwin, total_tiles, flags, moving, c.grid_ctas, as_stream(stream));
     } else if (c.kernel == PSC_KERNEL_AUTO || c.kernel == PSC_KERNEL_DIRECT) {
         e = launch_step_fast(store, d_windows, nwin, total_tiles, flags, moving, c.cells_per_thread, c.grid_ctas,
                              as_stream(stream));
     } else if (c.kernel == PSC_KERNEL_TMA) {
         const int stages = c.stages == 0 ? 3 : c.stages;
-        if (stages < 2 || stages > 4) return fail(PSC_E_INVALID, "psc_step: TMA stages must be 2, 3 or 4");
+        if (stages < 2 || stages > 4) return fail(PSC_E_INVALID, "psc_step_windows: TMA stages must be 2, 3 or 4");
         if (c.stage_bytes <= 0 || c.stage_bytes % 16 != 0 || (int64_t)stages * c.stage_bytes > 200 * 1024)
-            return fail(PSC_E_INVALID, "psc_step: bad TMA stage_bytes (use psc_plan_row_tiles)");
+            return fail(PSC_E_INVALID, "psc_step_windows: bad TMA stage_bytes (use psc_plan_row_tiles)");
         e = launch_step_tma(store, d_windows, nwin, total_tiles, flags, moving, c.grid_ctas, stages,
                             (uint32_t)c.stage_bytes, as_stream(stream));
     } else {
-        return fail(PSC_E_UNSUPPORTED, "psc_step: unknown kernel variant");
+        return fail(PSC_E_UNSUPPORTED, "psc_step_windows: unknown kernel variant");
     }
-    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_step");
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_step_windows");
 }
 
-int psc_step(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags, int grid_ctas,
+int psc_step_windows(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags, int grid_ctas,
              void* stream) {
     psc_launch c = {grid_ctas, 1, PSC_KERNEL_AUTO, 0, 0};
-    return psc_step_ex(store, d_windows, nwin, total_tiles, flags, &c, stream);
+    return psc_step_windows_ex(store, d_windows, nwin, total_tiles, flags, &c, stream);
 }
 
 int psc_reduce_windows(const psc_window* d_windows, int nwin, double* out, void* stream) {

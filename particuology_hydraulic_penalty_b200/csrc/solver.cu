@@ -1,0 +1,1297 @@
+// Handle layer of libpscb200.so: the reference's solver object
+// (PscD3Q19 / SparsePscD3Q19, src/lbm_dem/psc3d.py:117-407) and batches of
+// windows stepped by one persistent launch, written as a native runtime.
+//
+// A handle owns its device buffers, its stream and its CUDA graphs, and
+// drives the descriptor-layer kernels (geometry, step, reductions, loads) in
+// the order of collide_stream_psc (psc3d.py:208-253):
+//   voxelise (if the particles changed and the geometry is not static)
+//   -> solid velocity (if a particle moves)
+//   -> fused pull-stream + collide (+ IMB momentum, + per-tile reductions)
+//   -> particle loads -> reductions of the post-stream state -> diagnostics.
+// One call runs any number of steps with no host work between them except
+// where the caller asks for per-step diagnostics (the lbm_converge loop).
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace psc {
+namespace {
+
+#define PSC_TRY(expr)                  \
+    do {                               \
+        int psc_try_st_ = (expr);      \
+        if (psc_try_st_ != PSC_OK) return psc_try_st_; \
+    } while (0)
+#define PSC_CUDA(expr, what)                             \
+    do {                                                 \
+        cudaError_t psc_cuda_e_ = (expr);                \
+        if (psc_cuda_e_ != cudaSuccess) return cuda_fail(psc_cuda_e_, what); \
+    } while (0)
+
+constexpr int kQ = 19;
+constexpr int kChunkEntries = 4096;  // bbox entries per load-reduction chunk
+constexpr int kOutLen = 2 * PSC_NRED + PSC_NDIAG;  // [red_pre][red_post][diag]
+
+// Owned device array (contents are not kept when it grows).
+template <class T>
+struct DArray {
+    T* p = nullptr;
+    int64_t n = 0;
+    DArray() = default;
+    DArray(const DArray&) = delete;
+    DArray& operator=(const DArray&) = delete;
+    ~DArray() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t ensure(int64_t m, bool zero, cudaStream_t s) {
+        if (m < 1) m = 1;
+        if (p && m <= n) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), (size_t)m * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        n = m;
+        return zero ? cudaMemsetAsync(p, 0, (size_t)m * sizeof(T), s) : cudaSuccess;
+    }
+};
+
+// Owned page-locked host array.
+template <class T>
+struct HArray {
+    T* p = nullptr;
+    int64_t n = 0;
+    HArray() = default;
+    HArray(const HArray&) = delete;
+    HArray& operator=(const HArray&) = delete;
+    ~HArray() {
+        if (p) cudaFreeHost(p);
+    }
+    cudaError_t ensure(int64_t m) {
+        if (m < 1) m = 1;
+        if (p && m <= n) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), (size_t)m * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        n = m;
+        return cudaSuccess;
+    }
+};
+
+// Makes the handle's device current for the duration of a call.
+struct DeviceScope {
+    int prev = -1;
+    bool changed = false;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) {
+            err = cudaSetDevice(dev);
+            changed = err == cudaSuccess;
+        }
+    }
+    ~DeviceScope() {
+        if (changed && prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+int store_elem_bytes(int store) {
+    switch (store) {
+        case PSC_STORE_F64_EXACT:
+        case PSC_STORE_F64: return 8;
+        case PSC_STORE_F32: return 4;
+        default: return 2;
+    }
+}
+
+double default_store_scale(int store) { return store == PSC_STORE_F16 ? 1048576.0 : 1.0; }  // FP16: 2^20
+
+bool finite3(const double* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+int check_config(const psc_config& c, const char* who) {
+    const std::string w(who);
+    if (c.nx <= 0 || c.ny <= 0 || c.nz <= 0) return fail(PSC_E_INVALID, w + ": lattice extents must be > 0");
+    const long long n = (long long)c.nx * c.ny * c.nz;
+    if (n * kQ >= (1ll << 31)) return fail(PSC_E_UNSUPPORTED, w + ": a window must hold fewer than 2^31 / 19 cells");
+    if (c.store < PSC_STORE_F64_EXACT || c.store > PSC_STORE_BF16) return fail(PSC_E_INVALID, w + ": unknown store");
+    if (c.subsamples < 1 || c.subsamples > 16) return fail(PSC_E_INVALID, w + ": subsamples must be in [1, 16]");
+    if (c.store != PSC_STORE_F64_EXACT && c.subsamples > 6)
+        return fail(PSC_E_UNSUPPORTED, w + ": the deviation storage modes keep the solid level as uint8 (subsamples <= 6)");
+    if (!(std::isfinite(c.tau) && c.tau > 0.0)) return fail(PSC_E_INVALID, w + ": tau must be a positive number");
+    if (!(std::isfinite(c.tau_minus) && c.tau_minus >= 0.0)) return fail(PSC_E_INVALID, w + ": tau_minus must be >= 0");
+    if (c.tau_minus > 0.0 && c.store == PSC_STORE_F64_EXACT)
+        return fail(PSC_E_UNSUPPORTED, w + ": TRT runs in the deviation storage modes only");
+    if (!finite3(c.force)) return fail(PSC_E_INVALID, w + ": the body force must be finite");
+    if (!(std::isfinite(c.store_scale) && c.store_scale >= 0.0))
+        return fail(PSC_E_INVALID, w + ": store_scale must be >= 0 (0 = default)");
+    if (!(std::isfinite(c.conv_tol) && c.conv_tol >= 0.0)) return fail(PSC_E_INVALID, w + ": conv_tol must be >= 0");
+    if (c.device < 0) return fail(PSC_E_INVALID, w + ": negative device ordinal");
+    return PSC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// one window: populations, per-cell fields and particle geometry
+// ---------------------------------------------------------------------------
+struct Window {
+    psc_config cfg{};
+    int64_t N = 0;
+    int elem = 8;          // bytes per stored population
+    bool fdouble = true;   // imb / moments / us element type: double (FP64 modes) or float
+    double scale = 1.0;
+    bool want_level = false;
+    DArray<unsigned char> f[2];
+    int cur = 0;           // buffer holding the current post-collision populations
+    DArray<unsigned char> imb, moments, us;
+    DArray<double> partials;
+    int64_t partials_cap = 0;  // tiles the partial buffer holds
+    int64_t solo_tiles = 0;
+    DArray<psc_window> solo[2];  // single-window descriptor table per parity
+    bool solo_dirty = true;
+    uint64_t desc_version = 1;   // bumped whenever a descriptor field changes
+    // particles and geometry
+    int P = 0;
+    std::vector<double> hp;
+    HArray<double> pinned;
+    cudaEvent_t upload_done = nullptr;
+    DArray<double> particles;
+    DArray<int32_t> bbox;
+    DArray<int64_t> ent_off, chunk_off, totals;
+    DArray<uint16_t> ent_cnt, cl_cnt;
+    DArray<int32_t> cell_n, cell_off, cl_pid;
+    DArray<double> alpha_sum, solid;
+    DArray<uint8_t> level;
+    DArray<unsigned char> scan_tmp;
+    DArray<double> chunk_partials;
+    int64_t cap_entries = 0, cap_chunks = 0, n_entries = 0, n_chunks = 0;
+    DArray<double> forces, torques;
+    uint64_t pversion = 1, built_version = 0, us_version = 0;
+    bool built = false;
+    bool moving = false;
+    // state of the last step's results
+    bool stepped = false, moments_ready = false, loads_ready = false, diag_ready = false;
+    DArray<double> out;  // [red_pre][red_post][diag]
+    psc_diag last{};
+
+    ~Window() {
+        if (upload_done) cudaEventDestroy(upload_done);
+    }
+
+    void touch() {
+        solo_dirty = true;
+        ++desc_version;
+    }
+    size_t field_bytes() const { return fdouble ? 8 : 4; }
+    int field_type() const { return fdouble ? 0 : 1; }  // imb_type / us_type of the descriptor layer
+
+    psc_geometry geometry() const {
+        psc_geometry g{};
+        g.nx = cfg.nx;
+        g.ny = cfg.ny;
+        g.nz = cfg.nz;
+        g.subsamples = cfg.subsamples;
+        g.nparticles = P;
+        g.chunk_entries = kChunkEntries;
+        g.capacity_entries = cap_entries;
+        g.capacity_chunks = cap_chunks;
+        g.particles = P ? particles.p : nullptr;
+        g.bbox = bbox.p;
+        g.ent_off = ent_off.p;
+        g.chunk_off = chunk_off.p;
+        g.totals = totals.p;
+        g.ent_cnt = cap_entries ? ent_cnt.p : nullptr;
+        g.cell_n = cell_n.p;
+        g.cell_off = cell_off.p;
+        g.cl_pid = cap_entries ? cl_pid.p : nullptr;
+        g.cl_cnt = cap_entries ? cl_cnt.p : nullptr;
+        g.alpha_sum = alpha_sum.p;
+        g.solid = solid.p;
+        g.level = want_level ? level.p : nullptr;
+        g.scan_tmp = scan_tmp.p;
+        g.smooth_eps = 0.0;
+        g.ent_alpha = nullptr;
+        g.cl_ent = nullptr;
+        return g;
+    }
+
+    // Descriptor reading buffer `src` (tile fields unset).
+    psc_window descriptor(int src) const {
+        psc_window d{};
+        d.nx = cfg.nx;
+        d.ny = cfg.ny;
+        d.nz = cfg.nz;
+        d.subsamples = cfg.subsamples;
+        d.flags = moving ? PSC_WIN_MOVING : 0;
+        d.tau = cfg.tau;
+        d.force[0] = cfg.force[0];
+        d.force[1] = cfg.force[1];
+        d.force[2] = cfg.force[2];
+        d.store_scale = scale;
+        d.f_src = f[src].p;
+        d.f_dst = f[1 - src].p;
+        d.solid = solid.p;
+        d.level = want_level ? level.p : nullptr;
+        d.us = moving ? us.p : nullptr;
+        d.imb = imb.p;
+        d.moments = moments.p;
+        d.partials = partials.p;
+        d.tau_minus = cfg.tau_minus;
+        return d;
+    }
+};
+
+int window_init(Window& w, const psc_config& c, cudaStream_t s, const char* who) {
+    PSC_TRY(check_config(c, who));
+    w.cfg = c;
+    w.N = (int64_t)c.nx * c.ny * c.nz;
+    w.elem = store_elem_bytes(c.store);
+    w.fdouble = c.store == PSC_STORE_F64_EXACT || c.store == PSC_STORE_F64;
+    w.scale = c.store_scale > 0.0 ? c.store_scale : default_store_scale(c.store);
+    w.want_level = c.store != PSC_STORE_F64_EXACT;
+    const int64_t N = w.N;
+    PSC_CUDA(w.f[0].ensure(kQ * N * w.elem, false, s), who);
+    PSC_CUDA(w.f[1].ensure(kQ * N * w.elem, false, s), who);
+    PSC_TRY(psc_init_equilibrium(c.store, w.scale, w.f[0].p, N, s));
+    PSC_CUDA(w.cell_n.ensure(N, true, s), who);
+    PSC_CUDA(w.cell_off.ensure(N + 1, true, s), who);
+    PSC_CUDA(w.alpha_sum.ensure(N, true, s), who);
+    PSC_CUDA(w.solid.ensure(N, true, s), who);
+    if (w.want_level) PSC_CUDA(w.level.ensure(N, true, s), who);
+    PSC_CUDA(w.scan_tmp.ensure((int64_t)scan_tmp_bytes(N + 1), false, s), who);
+    PSC_CUDA(w.totals.ensure(4, true, s), who);
+    PSC_CUDA(w.ent_off.ensure(1, true, s), who);
+    PSC_CUDA(w.chunk_off.ensure(1, true, s), who);
+    PSC_CUDA(w.bbox.ensure(6, true, s), who);
+    PSC_CUDA(w.out.ensure(kOutLen, true, s), who);
+    // per-tile partials, sized once for any tiling of the window: 256-cell
+    // tiles (ceil(N / 256)) or row tiles (at most nx * ny); descriptor tables
+    // keep this pointer, so it never moves
+    w.partials_cap = std::max<int64_t>((N + 255) / 256, (int64_t)c.nx * c.ny);
+    PSC_CUDA(w.partials.ensure(w.partials_cap * PSC_NRED, true, s), who);
+    PSC_CUDA(cudaEventCreateWithFlags(&w.upload_done, cudaEventDisableTiming), who);
+    return PSC_OK;
+}
+
+int window_ensure_imb(Window& w, cudaStream_t s) {
+    if (w.imb.p) return PSC_OK;
+    PSC_CUDA(w.imb.ensure(3 * w.N * (int64_t)w.field_bytes(), true, s), "imb field");
+    w.touch();
+    return PSC_OK;
+}
+
+int window_ensure_moments(Window& w, cudaStream_t s) {
+    if (w.moments.p) return PSC_OK;
+    PSC_CUDA(w.moments.ensure(4 * w.N * (int64_t)w.field_bytes(), true, s), "moment fields");
+    w.touch();
+    return PSC_OK;
+}
+
+int window_set_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who) {
+    if (P < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
+    if (P > 0 && !hp) return fail(PSC_E_INVALID, std::string(who) + ": null particle array");
+    for (int64_t i = 0; i < (int64_t)P * 10; ++i)
+        if (!std::isfinite(hp[i])) return fail(PSC_E_INVALID, std::string(who) + ": particle state contains NaN or Inf");
+    const bool changed = P != w.P || (P > 0 && std::memcmp(w.hp.data(), hp, (size_t)P * 10 * sizeof(double)) != 0);
+    if (P != w.P || !w.particles.p) {
+        PSC_CUDA(cudaEventSynchronize(w.upload_done), who);  // the old staging buffer may still be read
+        PSC_CUDA(w.particles.ensure((int64_t)P * 10, true, s), who);
+        PSC_CUDA(w.bbox.ensure((int64_t)std::max(P, 1) * 6, true, s), who);
+        PSC_CUDA(w.ent_off.ensure((int64_t)P + 1, true, s), who);
+        PSC_CUDA(w.chunk_off.ensure((int64_t)P + 1, true, s), who);
+        PSC_CUDA(w.forces.ensure((int64_t)P * 3, true, s), who);
+        PSC_CUDA(w.torques.ensure((int64_t)P * 3, true, s), who);
+        PSC_CUDA(w.pinned.ensure((int64_t)P * 10), who);
+        if (P != w.P) {
+            w.built = false;
+            w.loads_ready = false;
+            w.diag_ready = false;
+        }
+        w.P = P;
+    }
+    w.hp.assign(hp, hp + (size_t)P * 10);
+    if (P > 0) {
+        // every step reads the caller's current state (psc3d.py re-reads the
+        // Particle3D objects each call); staged through page-locked memory
+        PSC_CUDA(cudaEventSynchronize(w.upload_done), who);
+        std::memcpy(w.pinned.p, hp, (size_t)P * 10 * sizeof(double));
+        PSC_CUDA(cudaMemcpyAsync(w.particles.p, w.pinned.p, (size_t)P * 10 * sizeof(double), cudaMemcpyHostToDevice, s),
+                 who);
+        PSC_CUDA(cudaEventRecord(w.upload_done, s), who);
+    }
+    if (changed) ++w.pversion;
+    bool mv = false;
+    for (int p = 0; p < P && !mv; ++p)
+        for (int k = 4; k < 10; ++k)
+            if (hp[(size_t)p * 10 + k] != 0.0) {
+                mv = true;
+                break;
+            }
+    if (mv != w.moving) {
+        w.moving = mv;
+        w.touch();
+    }
+    return PSC_OK;
+}
+
+int window_rebuild(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* who) {
+    psc_geometry g = w.geometry();
+    PSC_TRY(psc_geometry_plan(&g, s));
+    PSC_CUDA(tot.ensure(4), who);
+    PSC_CUDA(cudaMemcpyAsync(tot.p, w.totals.p, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), who);
+    PSC_CUDA(cudaStreamSynchronize(s), who);
+    w.n_entries = tot.p[0];
+    w.n_chunks = tot.p[1];
+    if (w.n_entries >= (1ll << 31) - 1)
+        return fail(PSC_E_CAPACITY, std::string(who) + ": too many bounding-box entries (>= 2^31) for one window");
+    if (w.n_entries > w.cap_entries) {
+        const int64_t cap = std::min<int64_t>(w.n_entries + w.n_entries / 4 + 1024, (1ll << 31) - 2);
+        PSC_CUDA(w.ent_cnt.ensure(cap, false, s), who);
+        PSC_CUDA(w.cl_pid.ensure(cap, false, s), who);
+        PSC_CUDA(w.cl_cnt.ensure(cap, false, s), who);
+        w.cap_entries = cap;
+    }
+    if (w.n_chunks > w.cap_chunks) {
+        const int64_t cap = w.n_chunks + w.n_chunks / 4 + 16;
+        PSC_CUDA(w.chunk_partials.ensure(cap * 6, false, s), who);
+        w.cap_chunks = cap;
+    }
+    g = w.geometry();
+    PSC_TRY(psc_geometry_build(&g, s));
+    w.built = true;
+    w.built_version = w.pversion;
+    w.us_version = 0;
+    w.loads_ready = false;
+    w.diag_ready = false;
+    return PSC_OK;
+}
+
+int window_solid_velocity(Window& w, cudaStream_t s) {
+    if (!w.us.p) {
+        PSC_CUDA(w.us.ensure(3 * w.N * (int64_t)w.field_bytes(), true, s), "solid velocity");
+        w.touch();
+    }
+    psc_geometry g = w.geometry();
+    PSC_TRY(psc_solid_velocity(&g, w.field_type(), w.us.p, s));
+    w.us_version = w.pversion;
+    return PSC_OK;
+}
+
+// Geometry and solid velocity up to date for the next step (psc3d.py:209-210, :215).
+int window_prepare(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* who) {
+    if (!w.built || (!w.cfg.static_geometry && w.built_version != w.pversion)) PSC_TRY(window_rebuild(w, s, tot, who));
+    if (w.moving && w.us_version != w.pversion) PSC_TRY(window_solid_velocity(w, s));
+    return PSC_OK;
+}
+
+int window_upload_solo(Window& w, cudaStream_t s) {
+    if (!w.solo_dirty) return PSC_OK;
+    psc_window d[2] = {w.descriptor(0), w.descriptor(1)};
+    int64_t total = 0;
+    PSC_TRY(psc_plan_tiles(d, 1, 0, &total));
+    PSC_TRY(psc_plan_tiles(d + 1, 1, 0, &total));
+    if (total > w.partials_cap) return fail(PSC_E_CAPACITY, "window descriptor: tile partials too small");
+    d[0].partials = w.partials.p;
+    d[1].partials = w.partials.p;
+    w.solo_tiles = total;
+    for (int p = 0; p < 2; ++p) {
+        PSC_CUDA(w.solo[p].ensure(1, false, s), "window descriptor");
+        PSC_CUDA(cudaMemcpyAsync(w.solo[p].p, &d[p], sizeof(psc_window), cudaMemcpyHostToDevice, s), "window descriptor");
+    }
+    PSC_CUDA(cudaStreamSynchronize(s), "window descriptor");  // d lives on this stack frame
+    w.solo_dirty = false;
+    return PSC_OK;
+}
+
+int launch_solo(Window& w, unsigned flags, cudaStream_t s) {
+    PSC_TRY(window_upload_solo(w, s));
+    if (w.moving) flags |= PSC_STEP_MOVING;
+    psc_launch c = {0, 1, PSC_KERNEL_AUTO, 0, 0};
+    return psc_step_windows_ex(w.cfg.store, w.solo[w.cur].p, 1, w.solo_tiles, flags, &c, s);
+}
+
+double* red_pre(Window& w) { return w.out.p; }
+double* red_post(Window& w) { return w.out.p + PSC_NRED; }
+double* diag_dev(Window& w) { return w.out.p + 2 * PSC_NRED; }
+
+int window_loads(Window& w, cudaStream_t s) {
+    psc_geometry g = w.geometry();
+    PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
+                               w.forces.p, w.torques.p, diag_dev(w), s));
+    w.loads_ready = true;
+    return PSC_OK;
+}
+
+// Darcy permeability along the body force from one window's post-stream
+// reductions: K = nu * (sum (1 - solid) u . d) / N / |F| with d = F / |F| and
+// nu = (tau - 1/2) / 3 (run_psc_permeability_resolution.py:144-150, where
+// F = (0, 0, Fz) and d = e_z); 0 without a body force.
+double row_permeability(const Window& w, const double* row) {
+    const double* F = w.cfg.force;
+    const double fmag = std::sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]);
+    if (!(fmag > 0.0)) return 0.0;
+    const double d0 = F[0] / fmag, d1 = F[1] / fmag, d2 = F[2] / fmag;
+    const double flux = d0 * row[PSC_RED_FLUID_UX] + d1 * row[PSC_RED_FLUID_UY] + d2 * row[PSC_RED_FLUID_UZ];
+    const double superficial = flux / (double)w.N;
+    const double nu = (w.cfg.tau - 0.5) / 3.0;
+    return nu * superficial / fmag;
+}
+
+void fill_diag(const Window& w, const double* host_out, psc_diag& d) {
+    const double* pre = host_out;
+    const double* post = host_out + PSC_NRED;
+    const double* dg = host_out + 2 * PSC_NRED;
+    const double N = (double)w.N;
+    std::memset(&d, 0, sizeof(d));
+    d.solid_volume_lu = post[PSC_RED_SOLID];
+    d.mean_uz = post[PSC_RED_UZ] / N;
+    d.momentum_residual = dg[PSC_DIAG_MOMENTUM_RESIDUAL];
+    d.max_force = w.P ? dg[PSC_DIAG_MAX_FORCE] : 0.0;
+    d.max_torque = w.P ? dg[PSC_DIAG_MAX_TORQUE] : 0.0;
+    for (int k = 0; k < 3; ++k) {
+        d.mean_u[k] = post[PSC_RED_UX + k] / N;
+        d.superficial_u[k] = post[PSC_RED_FLUID_UX + k] / N;
+        d.imb_sum[k] = pre[PSC_RED_IMBX + k];
+        d.force_sum[k] = dg[PSC_DIAG_FORCE_SUM_X + k];
+    }
+    d.fluid_volume_lu = post[PSC_RED_FLUID];
+    d.permeability = row_permeability(w, post);
+    d.nonfinite_cells = post[PSC_RED_NONFINITE];
+}
+
+// Copy a [count] field of the window's field type to float64 host memory.
+int field_to_host(const Window& w, const void* src, int64_t count, double* dst, cudaStream_t s, const char* who) {
+    if (w.fdouble) {
+        PSC_CUDA(cudaMemcpyAsync(dst, src, (size_t)count * 8, cudaMemcpyDeviceToHost, s), who);
+        PSC_CUDA(cudaStreamSynchronize(s), who);
+        return PSC_OK;
+    }
+    std::vector<float> tmp((size_t)count);
+    PSC_CUDA(cudaMemcpyAsync(tmp.data(), src, (size_t)count * 4, cudaMemcpyDeviceToHost, s), who);
+    PSC_CUDA(cudaStreamSynchronize(s), who);
+    for (int64_t i = 0; i < count; ++i) dst[i] = (double)tmp[(size_t)i];
+    return PSC_OK;
+}
+
+int window_get_field(Window& w, int which, double* dst, cudaStream_t s, HArray<int64_t>& tot, const char* who) {
+    if (!dst) return fail(PSC_E_INVALID, std::string(who) + ": null output");
+    const int64_t N = w.N;
+    switch (which) {
+        case PSC_FIELD_RHO:
+        case PSC_FIELD_UX:
+        case PSC_FIELD_UY:
+        case PSC_FIELD_UZ: {
+            if (!w.stepped) {  // the reference starts from rho = 1, u = 0 arrays (psc3d.py:136-139)
+                std::fill(dst, dst + N, which == PSC_FIELD_RHO ? 1.0 : 0.0);
+                return PSC_OK;
+            }
+            if (!w.moments_ready) {
+                PSC_TRY(window_ensure_moments(w, s));
+                PSC_TRY(launch_solo(w, PSC_STEP_MOMENTS, s));
+                w.moments_ready = true;
+            }
+            return field_to_host(w, w.moments.p + (size_t)which * N * w.field_bytes(), N, dst, s, who);
+        }
+        case PSC_FIELD_SOLID:
+        case PSC_FIELD_ALPHA_SUM: {
+            if (!w.built) {
+                std::fill(dst, dst + N, 0.0);
+                return PSC_OK;
+            }
+            const double* src = which == PSC_FIELD_SOLID ? w.solid.p : w.alpha_sum.p;
+            PSC_CUDA(cudaMemcpyAsync(dst, src, (size_t)N * 8, cudaMemcpyDeviceToHost, s), who);
+            PSC_CUDA(cudaStreamSynchronize(s), who);
+            return PSC_OK;
+        }
+        case PSC_FIELD_IMB_X:
+        case PSC_FIELD_IMB_Y:
+        case PSC_FIELD_IMB_Z: {
+            if (!w.stepped || !w.imb.p) {
+                std::fill(dst, dst + N, 0.0);
+                return PSC_OK;
+            }
+            const int k = which - PSC_FIELD_IMB_X;
+            return field_to_host(w, w.imb.p + (size_t)k * N * w.field_bytes(), N, dst, s, who);
+        }
+        case PSC_FIELD_US_X:
+        case PSC_FIELD_US_Y:
+        case PSC_FIELD_US_Z: {
+            if (!w.built) PSC_TRY(window_rebuild(w, s, tot, who));
+            if (w.us_version != w.pversion || !w.us.p) PSC_TRY(window_solid_velocity(w, s));
+            const int k = which - PSC_FIELD_US_X;
+            return field_to_host(w, w.us.p + (size_t)k * N * w.field_bytes(), N, dst, s, who);
+        }
+        case PSC_FIELD_F: {
+            double* tmp = nullptr;
+            PSC_CUDA(cudaMalloc(reinterpret_cast<void**>(&tmp), (size_t)kQ * N * 8), who);
+            int st = psc_stream_push(w.cfg.store, w.scale, w.f[w.cur].p, tmp, w.cfg.nx, w.cfg.ny, w.cfg.nz, s);
+            cudaError_t e = cudaSuccess;
+            if (st == PSC_OK) e = cudaMemcpyAsync(dst, tmp, (size_t)kQ * N * 8, cudaMemcpyDeviceToHost, s);
+            if (st == PSC_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);
+            cudaFree(tmp);
+            if (st != PSC_OK) return st;
+            if (e != cudaSuccess) return cuda_fail(e, who);
+            return PSC_OK;
+        }
+        default: return fail(PSC_E_INVALID, std::string(who) + ": unknown field selector");
+    }
+}
+
+int window_set_populations(Window& w, const double* hf, cudaStream_t s, const char* who) {
+    if (!hf) return fail(PSC_E_INVALID, std::string(who) + ": null populations");
+    const int64_t n = kQ * w.N;
+    double* tmp = nullptr;
+    PSC_CUDA(cudaMalloc(reinterpret_cast<void**>(&tmp), (size_t)n * 8), who);
+    cudaError_t e = cudaMemcpyAsync(tmp, hf, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+    int st = PSC_OK;
+    if (e == cudaSuccess)
+        st = psc_stream_pull_store(w.cfg.store, w.scale, tmp, w.f[w.cur].p, w.cfg.nx, w.cfg.ny, w.cfg.nz, s);
+    if (e == cudaSuccess && st == PSC_OK) e = cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, who);
+    if (st != PSC_OK) return st;
+    w.moments_ready = false;
+    w.diag_ready = false;
+    return PSC_OK;
+}
+
+int window_sparse_alpha(Window& w, int64_t* offsets, int64_t* ids, double* vals, int64_t capacity, cudaStream_t s,
+                        const char* who) {
+    if (!offsets) return fail(PSC_E_INVALID, std::string(who) + ": null offsets");
+    const int P = w.P;
+    offsets[0] = 0;
+    if (!w.built || P == 0) {
+        for (int p = 0; p <= P; ++p) offsets[p] = 0;
+        return PSC_OK;
+    }
+    std::vector<uint16_t> cnt((size_t)w.n_entries);
+    std::vector<int64_t> off((size_t)P + 1);
+    std::vector<int32_t> box((size_t)P * 6);
+    if (w.n_entries)
+        PSC_CUDA(cudaMemcpyAsync(cnt.data(), w.ent_cnt.p, (size_t)w.n_entries * 2, cudaMemcpyDeviceToHost, s), who);
+    PSC_CUDA(cudaMemcpyAsync(off.data(), w.ent_off.p, (size_t)(P + 1) * 8, cudaMemcpyDeviceToHost, s), who);
+    PSC_CUDA(cudaMemcpyAsync(box.data(), w.bbox.p, (size_t)P * 6 * 4, cudaMemcpyDeviceToHost, s), who);
+    PSC_CUDA(cudaStreamSynchronize(s), who);
+    int64_t total = 0;
+    for (int p = 0; p < P; ++p) {
+        for (int64_t e = off[p]; e < off[p + 1]; ++e) total += cnt[(size_t)e] != 0;
+        offsets[p + 1] = total;
+    }
+    if (!ids || !vals || capacity < total) {
+        if (total == 0) return PSC_OK;
+        return fail(PSC_E_CAPACITY, std::string(who) + ": capacity below the entry count in offsets[P]");
+    }
+    const double s3 = (double)w.cfg.subsamples * w.cfg.subsamples * w.cfg.subsamples;
+    const int64_t ny = w.cfg.ny, nz = w.cfg.nz;
+    int64_t k = 0;
+    for (int p = 0; p < P; ++p) {
+        const int64_t x0 = box[(size_t)p * 6], y0 = box[(size_t)p * 6 + 1], z0 = box[(size_t)p * 6 + 2];
+        const int64_t ey = box[(size_t)p * 6 + 4], ez = box[(size_t)p * 6 + 5];
+        for (int64_t e = off[p]; e < off[p + 1]; ++e) {
+            const uint16_t c = cnt[(size_t)e];
+            if (!c) continue;
+            const int64_t loc = e - off[p];
+            const int64_t a = loc / (ey * ez);
+            const int64_t rem = loc - a * ey * ez;
+            const int64_t b = rem / ez;
+            const int64_t z = rem - b * ez;
+            ids[k] = ((a + x0) * ny + (b + y0)) * nz + (z + z0);
+            vals[k] = (double)c / s3;  // inside / S^3 (psc3d.py:88)
+            ++k;
+        }
+    }
+    return PSC_OK;
+}
+
+}  // namespace
+}  // namespace psc
+
+using namespace psc;
+
+// ---------------------------------------------------------------------------
+// single-window solver
+// ---------------------------------------------------------------------------
+struct psc_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Window w;
+    HArray<int64_t> tot;
+    HArray<double> host_out;
+};
+
+namespace psc {
+namespace {
+
+// The reductions of the post-stream state and the diagnostics of the step just
+// taken, copied to the host (psc3d.py:243-253).
+int solver_report(psc_solver& h, bool loads, bool fields, bool post = true) {
+    Window& w = h.w;
+    cudaStream_t s = h.stream;
+    if (loads) PSC_TRY(window_loads(w, s));
+    if (fields) PSC_TRY(window_ensure_moments(w, s));
+    if (post || fields) {
+        // the step's own partials (pre-collision state) were reduced into red_pre already
+        PSC_TRY(launch_solo(w, PSC_STEP_REDUCE | (fields ? PSC_STEP_MOMENTS : 0u), s));
+        PSC_TRY(psc_reduce_windows(w.solo[w.cur].p, 1, red_post(w), s));
+    }
+    PSC_CUDA(h.host_out.ensure(kOutLen), "psc_step");
+    PSC_CUDA(cudaMemcpyAsync(h.host_out.p, w.out.p, kOutLen * sizeof(double), cudaMemcpyDeviceToHost, s), "psc_step");
+    PSC_CUDA(cudaStreamSynchronize(s), "psc_step");
+    if (fields) w.moments_ready = true;
+    fill_diag(w, h.host_out.p, w.last);
+    w.diag_ready = loads;
+    return PSC_OK;
+}
+
+// One collide_stream_psc step; `imb` writes the IMB field and reduces the
+// step's partials into red_pre.
+int solver_collide(psc_solver& h, bool imb) {
+    Window& w = h.w;
+    cudaStream_t s = h.stream;
+    unsigned flags = PSC_STEP_COLLIDE;
+    if (imb) {
+        PSC_TRY(window_ensure_imb(w, s));
+        flags |= PSC_STEP_IMB | PSC_STEP_REDUCE;
+    }
+    PSC_TRY(launch_solo(w, flags, s));
+    w.cur ^= 1;
+    w.stepped = true;
+    w.moments_ready = false;
+    w.loads_ready = false;
+    w.diag_ready = false;
+    if (imb) PSC_TRY(psc_reduce_windows(w.solo[w.cur].p, 1, red_pre(w), s));
+    return PSC_OK;
+}
+
+}  // namespace
+}  // namespace psc
+
+extern "C" {
+
+int psc_create(const psc_config* h_cfg, psc_solver** out) {
+    if (!h_cfg || !out) return fail(PSC_E_INVALID, "psc_create: null argument");
+    *out = nullptr;
+    PSC_TRY(check_config(*h_cfg, "psc_create"));
+    DeviceScope ds(h_cfg->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_create: cudaSetDevice");
+    std::unique_ptr<psc_solver> h(new (std::nothrow) psc_solver());
+    if (!h) return fail(PSC_E_CAPACITY, "psc_create: out of host memory");
+    h->device = h_cfg->device;
+    if (h_cfg->stream) {
+        h->stream = as_stream(h_cfg->stream);
+    } else {
+        PSC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "psc_create");
+        h->own_stream = true;
+    }
+    int st = window_init(h->w, *h_cfg, h->stream, "psc_create");
+    if (st == PSC_OK) st = window_set_particles(h->w, nullptr, 0, h->stream, "psc_create");
+    if (st == PSC_OK) {
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "psc_create");
+    }
+    if (st != PSC_OK) {
+        psc_destroy(h.release());
+        return st;
+    }
+    *out = h.release();
+    return PSC_OK;
+}
+
+int psc_destroy(psc_solver* h) {
+    if (!h) return PSC_OK;
+    {
+        DeviceScope ds(h->device);
+        cudaStreamSynchronize(h->stream);
+        cudaStream_t s = h->stream;
+        bool own = h->own_stream;
+        delete h;  // frees the device buffers on the handle's device
+        if (own) cudaStreamDestroy(s);
+    }
+    return PSC_OK;
+}
+
+int psc_set_particles(psc_solver* h, const double* h_particles, int nparticles) {
+    if (!h) return fail(PSC_E_INVALID, "psc_set_particles: null handle");
+    DeviceScope ds(h->device);
+    return window_set_particles(h->w, h_particles, nparticles, h->stream, "psc_set_particles");
+}
+
+int psc_rebuild_geometry(psc_solver* h) {
+    if (!h) return fail(PSC_E_INVALID, "psc_rebuild_geometry: null handle");
+    DeviceScope ds(h->device);
+    return window_rebuild(h->w, h->stream, h->tot, "psc_rebuild_geometry");
+}
+
+int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status) {
+    if (!h) return fail(PSC_E_INVALID, "psc_step: null handle");
+    if (nsteps < 0) return fail(PSC_E_INVALID, "psc_step: negative step count");
+    if (flags & ~(PSC_RUN_DIAG | PSC_RUN_CONVERGE | PSC_RUN_FIELDS)) return fail(PSC_E_INVALID, "psc_step: unknown flags");
+    DeviceScope ds(h->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_step: cudaSetDevice");
+    Window& w = h->w;
+    const bool converge = (flags & PSC_RUN_CONVERGE) != 0;
+    const bool diag = converge || (flags & PSC_RUN_DIAG) != 0;
+    const bool fields = (flags & PSC_RUN_FIELDS) != 0;
+    const double tol = w.cfg.conv_tol > 0.0 ? w.cfg.conv_tol : 1.0e-8;
+    const int min_steps = std::max(1, w.cfg.conv_min_steps);
+    psc_status st{};
+    st.residual = INFINITY;
+    if (nsteps > 0) PSC_TRY(window_prepare(w, h->stream, h->tot, "psc_step"));
+    double previous = NAN;
+    int k = 0;
+    for (k = 1; k <= nsteps; ++k) {
+        const bool last = k == nsteps;
+        PSC_TRY(solver_collide(*h, last || converge));
+        if (converge) {
+            PSC_TRY(solver_report(*h, false, false));
+            const double current = w.last.mean_uz;
+            if (!std::isnan(previous)) st.residual = std::fabs(current - previous) / std::max(std::fabs(current), 1.0e-30);
+            previous = current;
+            if (k >= min_steps && st.residual < tol) {
+                st.converged = 1;
+                break;
+            }
+        }
+    }
+    st.steps_done = std::min(k, nsteps);
+    if (nsteps > 0 && (diag || fields)) {
+        // under PSC_RUN_CONVERGE the post-stream reductions of the last step are taken already
+        PSC_TRY(solver_report(*h, diag, fields, !converge));
+        if (diag) st.diag = w.last;
+    } else if (nsteps > 0) {
+        PSC_CUDA(cudaGetLastError(), "psc_step");
+    }
+    if (h_status) *h_status = st;
+    return PSC_OK;
+}
+
+int psc_get_fields(psc_solver* h, int which, double* h_dst) {
+    if (!h) return fail(PSC_E_INVALID, "psc_get_fields: null handle");
+    DeviceScope ds(h->device);
+    return window_get_field(h->w, which, h_dst, h->stream, h->tot, "psc_get_fields");
+}
+
+int psc_set_populations(psc_solver* h, const double* h_f) {
+    if (!h) return fail(PSC_E_INVALID, "psc_set_populations: null handle");
+    DeviceScope ds(h->device);
+    return window_set_populations(h->w, h_f, h->stream, "psc_set_populations");
+}
+
+int psc_get_loads(psc_solver* h, double* h_forces, double* h_torques) {
+    if (!h) return fail(PSC_E_INVALID, "psc_get_loads: null handle");
+    Window& w = h->w;
+    if (w.P > 0 && (!h_forces || !h_torques)) return fail(PSC_E_INVALID, "psc_get_loads: null output");
+    if (w.P == 0) return PSC_OK;
+    DeviceScope ds(h->device);
+    if (!w.stepped) {  // hydro_forces / hydro_torques start as zeros (psc3d.py:146-147)
+        std::fill(h_forces, h_forces + 3 * (size_t)w.P, 0.0);
+        std::fill(h_torques, h_torques + 3 * (size_t)w.P, 0.0);
+        return PSC_OK;
+    }
+    if (!w.loads_ready) {  // accumulate_particle_loads() with the current geometry (psc3d.py:255-281)
+        if (!w.imb.p) return fail(PSC_E_INVALID, "psc_get_loads: no IMB field (no step has run)");
+        PSC_TRY(window_loads(w, h->stream));
+    }
+    PSC_CUDA(cudaMemcpyAsync(h_forces, w.forces.p, (size_t)w.P * 24, cudaMemcpyDeviceToHost, h->stream),
+             "psc_get_loads");
+    PSC_CUDA(cudaMemcpyAsync(h_torques, w.torques.p, (size_t)w.P * 24, cudaMemcpyDeviceToHost, h->stream),
+             "psc_get_loads");
+    PSC_CUDA(cudaStreamSynchronize(h->stream), "psc_get_loads");
+    return PSC_OK;
+}
+
+int psc_accumulate_particle_loads(psc_solver* h) {
+    if (!h) return fail(PSC_E_INVALID, "psc_accumulate_particle_loads: null handle");
+    Window& w = h->w;
+    if (!w.stepped || !w.imb.p) return fail(PSC_E_INVALID, "psc_accumulate_particle_loads: no step has run");
+    DeviceScope ds(h->device);
+    if (!w.built) PSC_TRY(window_rebuild(w, h->stream, h->tot, "psc_accumulate_particle_loads"));
+    PSC_TRY(solver_report(*h, true, false));
+    w.diag_ready = true;
+    return PSC_OK;
+}
+
+int psc_get_diag(psc_solver* h, psc_diag* h_diag) {
+    if (!h || !h_diag) return fail(PSC_E_INVALID, "psc_get_diag: null argument");
+    Window& w = h->w;
+    if (!w.stepped) {
+        std::memset(h_diag, 0, sizeof(psc_diag));
+        return PSC_OK;
+    }
+    DeviceScope ds(h->device);
+    if (!w.diag_ready) {
+        if (!w.imb.p) return fail(PSC_E_INVALID, "psc_get_diag: no IMB field (no step has run)");
+        PSC_TRY(solver_report(*h, true, false));
+    }
+    *h_diag = w.last;
+    return PSC_OK;
+}
+
+int psc_get_sparse_alpha(psc_solver* h, int64_t* h_offsets, int64_t* h_ids, double* h_vals, int64_t capacity) {
+    if (!h) return fail(PSC_E_INVALID, "psc_get_sparse_alpha: null handle");
+    DeviceScope ds(h->device);
+    return window_sparse_alpha(h->w, h_offsets, h_ids, h_vals, capacity, h->stream, "psc_get_sparse_alpha");
+}
+
+size_t psc_config_size(void) { return sizeof(psc_config); }
+
+size_t psc_diag_size(void) { return sizeof(psc_diag); }
+
+size_t psc_status_size(void) { return sizeof(psc_status); }
+
+int psc_solver_info(psc_solver* h, int* h_nparticles, int64_t* h_cells) {
+    if (!h) return fail(PSC_E_INVALID, "psc_solver_info: null handle");
+    if (h_nparticles) *h_nparticles = h->w.P;
+    if (h_cells) *h_cells = h->w.N;
+    return PSC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+struct psc_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int store = PSC_STORE_F32;
+    psc_launch launch{0, 1, PSC_KERNEL_AUTO, 0, 0};
+    int graph_steps = 0;
+    std::vector<std::unique_ptr<Window>> w;
+    DArray<psc_window> table[2];
+    int64_t total_tiles = 0;
+    bool tables_dirty = true;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int parity = 0;
+    std::vector<int> frozen;  // -1 active, else the buffer parity holding the frozen state
+    std::vector<double> frozen_red;  // [nwin][NRED] post-stream reductions at freezing
+    DArray<double> red_pre, red_post, diag;
+    HArray<double> host;
+    HArray<int64_t> tot;
+    std::vector<psc_diag> last;
+    std::vector<char> have_diag;
+    std::vector<uint64_t> built_desc;  // descriptor versions the tables were built from
+    bool moving_any = false;
+
+    ~psc_batch() {
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+    }
+};
+
+namespace psc {
+namespace {
+
+void batch_drop_graphs(psc_batch& b) {
+    for (auto& g : b.graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+int batch_build_tables(psc_batch& b) {
+    const int nwin = (int)b.w.size();
+    std::vector<psc_window> tab[2];
+    b.moving_any = false;
+    for (int p = 0; p < 2; ++p) {
+        tab[p].resize((size_t)nwin);
+        for (int k = 0; k < nwin; ++k) {
+            Window& w = *b.w[(size_t)k];
+            tab[p][(size_t)k] = w.descriptor(p);
+            if (b.frozen[(size_t)k] >= 0) tab[p][(size_t)k].flags |= PSC_WIN_INACTIVE;
+            b.moving_any = b.moving_any || w.moving;
+        }
+        int64_t total = 0;
+        if (b.launch.kernel == PSC_KERNEL_TMA) {
+            int32_t sb = 0;
+            PSC_TRY(psc_plan_row_tiles(tab[p].data(), nwin, 0, store_elem_bytes(b.store), &total, &sb));
+            b.launch.stage_bytes = sb;
+        } else {
+            PSC_TRY(psc_plan_tiles(tab[p].data(), nwin, 256 * b.launch.cells_per_thread, &total));
+        }
+        b.total_tiles = total;
+        for (int k = 0; k < nwin; ++k) {
+            Window& w = *b.w[(size_t)k];
+            if (tab[p][(size_t)k].tile_count > w.partials_cap)
+                return fail(PSC_E_CAPACITY, "batch tables: tile partials too small");
+            tab[p][(size_t)k].partials = w.partials.p;
+        }
+    }
+    for (int p = 0; p < 2; ++p) {
+        PSC_CUDA(b.table[p].ensure(nwin, false, b.stream), "batch tables");
+        PSC_CUDA(cudaMemcpyAsync(b.table[p].p, tab[p].data(), (size_t)nwin * sizeof(psc_window),
+                                 cudaMemcpyHostToDevice, b.stream),
+                 "batch tables");
+    }
+    PSC_CUDA(cudaStreamSynchronize(b.stream), "batch tables");
+    for (int k = 0; k < nwin; ++k) b.built_desc[(size_t)k] = b.w[(size_t)k]->desc_version;
+    b.tables_dirty = false;
+    batch_drop_graphs(b);
+    return PSC_OK;
+}
+
+void batch_sync_cur(psc_batch& b) {
+    for (size_t k = 0; k < b.w.size(); ++k) b.w[k]->cur = b.frozen[k] >= 0 ? b.frozen[k] : b.parity;
+}
+
+int batch_launch(psc_batch& b, unsigned flags) {
+    if (b.moving_any) flags |= PSC_STEP_MOVING;
+    return psc_step_windows_ex(b.store, b.table[b.parity].p, (int)b.w.size(), b.total_tiles, flags, &b.launch,
+                               b.stream);
+}
+
+// Everything the next step reads is on the device and described by the tables.
+int batch_prepare(psc_batch& b, bool imb, bool moments) {
+    for (size_t k = 0; k < b.w.size(); ++k) {
+        Window& w = *b.w[k];
+        PSC_TRY(window_prepare(w, b.stream, b.tot, "psc_batch_step"));
+        if (imb) PSC_TRY(window_ensure_imb(w, b.stream));
+        if (moments) PSC_TRY(window_ensure_moments(w, b.stream));
+        if (w.desc_version != b.built_desc[k]) b.tables_dirty = true;
+    }
+    if (b.tables_dirty) PSC_TRY(batch_build_tables(b));
+    return PSC_OK;
+}
+
+int batch_capture(psc_batch& b, int parity) {
+    const int saved = b.parity;
+    b.parity = parity;
+    PSC_CUDA(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+    int st = PSC_OK;
+    for (int i = 0; i < b.graph_steps && st == PSC_OK; ++i) {
+        st = batch_launch(b, PSC_STEP_COLLIDE);
+        b.parity ^= 1;
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b.stream, &g);
+    b.parity = saved;
+    if (st != PSC_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "graph capture");
+    e = cudaGraphInstantiate(&b.graph[parity], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b.graph[parity] = nullptr;
+        return cuda_fail(e, "graph instantiate");
+    }
+    return PSC_OK;
+}
+
+int batch_plain_steps(psc_batch& b, int n) {
+    if (b.graph_steps > 0 && n >= b.graph_steps) {
+        if (!b.graph[b.parity]) PSC_TRY(batch_capture(b, b.parity));
+        const int reps = n / b.graph_steps;
+        for (int r = 0; r < reps; ++r) PSC_CUDA(cudaGraphLaunch(b.graph[b.parity], b.stream), "graph launch");
+        n -= reps * b.graph_steps;  // an even graph length returns to this parity
+    }
+    for (int i = 0; i < n; ++i) {
+        PSC_TRY(batch_launch(b, PSC_STEP_COLLIDE));
+        b.parity ^= 1;
+    }
+    batch_sync_cur(b);
+    for (auto& wp : b.w) {
+        wp->stepped = true;
+        wp->moments_ready = false;
+        wp->loads_ready = false;
+        wp->diag_ready = false;
+    }
+    return PSC_OK;
+}
+
+// Reductions of every window's current post-stream state into red_post
+// (host copy in b.host + nwin * NRED); frozen windows report their rows at freezing.
+int batch_observe(psc_batch& b, double* host_rows) {
+    const int nwin = (int)b.w.size();
+    PSC_TRY(batch_launch(b, PSC_STEP_REDUCE));
+    PSC_TRY(psc_reduce_windows(b.table[b.parity].p, nwin, b.red_post.p, b.stream));
+    PSC_CUDA(cudaMemcpyAsync(host_rows, b.red_post.p, (size_t)nwin * PSC_NRED * 8, cudaMemcpyDeviceToHost, b.stream),
+             "batch reductions");
+    PSC_CUDA(cudaStreamSynchronize(b.stream), "batch reductions");
+    for (int k = 0; k < nwin; ++k)
+        if (b.frozen[(size_t)k] >= 0)
+            std::memcpy(host_rows + (size_t)k * PSC_NRED, b.frozen_red.data() + (size_t)k * PSC_NRED,
+                        PSC_NRED * sizeof(double));
+    return PSC_OK;
+}
+
+int batch_freeze(psc_batch& b, int k, const double* row) {
+    b.frozen[(size_t)k] = b.parity;
+    std::memcpy(b.frozen_red.data() + (size_t)k * PSC_NRED, row, PSC_NRED * sizeof(double));
+    // set the flag in both device tables in place: captured graphs stay valid
+    const size_t off = (size_t)k * sizeof(psc_window) + offsetof(psc_window, flags);
+    int32_t flags = b.w[(size_t)k]->moving ? PSC_WIN_MOVING : 0;
+    flags |= PSC_WIN_INACTIVE;
+    for (int p = 0; p < 2; ++p)
+        PSC_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(b.table[p].p) + off, &flags, sizeof(flags),
+                                 cudaMemcpyHostToDevice, b.stream),
+                 "freeze");
+    PSC_CUDA(cudaStreamSynchronize(b.stream), "freeze");
+    b.w[(size_t)k]->cur = b.parity;
+    return PSC_OK;
+}
+
+}  // namespace
+}  // namespace psc
+
+extern "C" {
+
+int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_launch, int graph_steps, psc_batch** out) {
+    if (!h_cfgs || !out || nwin <= 0) return fail(PSC_E_INVALID, "psc_batch_create: bad arguments");
+    *out = nullptr;
+    if (graph_steps < 0 || graph_steps % 2)
+        return fail(PSC_E_INVALID, "psc_batch_create: graph_steps must be even and >= 0");
+    for (int k = 0; k < nwin; ++k) {
+        PSC_TRY(check_config(h_cfgs[k], "psc_batch_create"));
+        if (h_cfgs[k].store != h_cfgs[0].store || h_cfgs[k].device != h_cfgs[0].device ||
+            h_cfgs[k].stream != h_cfgs[0].stream)
+            return fail(PSC_E_INVALID, "psc_batch_create: all windows need the same store, device and stream");
+    }
+    psc_launch lc = {0, 1, PSC_KERNEL_AUTO, 0, 0};
+    if (h_launch) lc = *h_launch;
+    if (lc.grid_ctas < 0) return fail(PSC_E_INVALID, "psc_batch_create: grid_ctas must be >= 0");
+    if (lc.cells_per_thread != 1 && lc.cells_per_thread != 2 && lc.cells_per_thread != 4)
+        return fail(PSC_E_INVALID, "psc_batch_create: cells_per_thread must be 1, 2 or 4");
+    if (h_cfgs[0].store == PSC_STORE_F64_EXACT && (lc.cells_per_thread != 1 || lc.kernel == PSC_KERNEL_TMA))
+        return fail(PSC_E_UNSUPPORTED, "psc_batch_create: PSC_STORE_F64_EXACT runs the one-cell-per-thread kernel");
+    if (lc.kernel == PSC_KERNEL_TMA && lc.stages == 0) lc.stages = 3;
+    DeviceScope ds(h_cfgs[0].device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_batch_create: cudaSetDevice");
+    std::unique_ptr<psc_batch> b(new (std::nothrow) psc_batch());
+    if (!b) return fail(PSC_E_CAPACITY, "psc_batch_create: out of host memory");
+    b->device = h_cfgs[0].device;
+    b->store = h_cfgs[0].store;
+    b->launch = lc;
+    b->graph_steps = graph_steps;
+    if (h_cfgs[0].stream) {
+        b->stream = as_stream(h_cfgs[0].stream);
+    } else {
+        PSC_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "psc_batch_create");
+        b->own_stream = true;
+    }
+    int st = PSC_OK;
+    for (int k = 0; k < nwin && st == PSC_OK; ++k) {
+        b->w.emplace_back(new (std::nothrow) Window());
+        if (!b->w.back()) {
+            st = fail(PSC_E_CAPACITY, "psc_batch_create: out of host memory");
+            break;
+        }
+        st = window_init(*b->w.back(), h_cfgs[k], b->stream, "psc_batch_create");
+        if (st == PSC_OK) st = window_set_particles(*b->w.back(), nullptr, 0, b->stream, "psc_batch_create");
+    }
+    b->frozen.assign((size_t)nwin, -1);
+    b->frozen_red.assign((size_t)nwin * PSC_NRED, 0.0);
+    b->last.assign((size_t)nwin, psc_diag{});
+    b->have_diag.assign((size_t)nwin, 0);
+    b->built_desc.assign((size_t)nwin, 0);
+    if (st == PSC_OK) {
+        cudaError_t e = b->red_pre.ensure((int64_t)nwin * PSC_NRED, true, b->stream);
+        if (e == cudaSuccess) e = b->red_post.ensure((int64_t)nwin * PSC_NRED, true, b->stream);
+        if (e == cudaSuccess) e = b->diag.ensure((int64_t)nwin * PSC_NDIAG, true, b->stream);
+        if (e == cudaSuccess) e = b->host.ensure((int64_t)nwin * kOutLen);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "psc_batch_create");
+    }
+    if (st != PSC_OK) {
+        psc_batch_destroy(b.release());
+        return st;
+    }
+    *out = b.release();
+    return PSC_OK;
+}
+
+int psc_batch_destroy(psc_batch* b) {
+    if (!b) return PSC_OK;
+    DeviceScope ds(b->device);
+    cudaStreamSynchronize(b->stream);
+    cudaStream_t s = b->stream;
+    bool own = b->own_stream;
+    delete b;
+    if (own) cudaStreamDestroy(s);
+    return PSC_OK;
+}
+
+int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, int nparticles) {
+    if (!b || win < 0 || win >= (int)b->w.size()) return fail(PSC_E_INVALID, "psc_batch_set_particles: bad window");
+    DeviceScope ds(b->device);
+    return window_set_particles(*b->w[(size_t)win], h_particles, nparticles, b->stream, "psc_batch_set_particles");
+}
+
+int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_status) {
+    if (!b) return fail(PSC_E_INVALID, "psc_batch_step: null handle");
+    if (nsteps < 0) return fail(PSC_E_INVALID, "psc_batch_step: negative step count");
+    if (flags & ~(PSC_RUN_DIAG | PSC_RUN_FIELDS)) return fail(PSC_E_INVALID, "psc_batch_step: unknown flags");
+    DeviceScope ds(b->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_batch_step: cudaSetDevice");
+    const bool diag = (flags & PSC_RUN_DIAG) != 0;
+    const bool fields = (flags & PSC_RUN_FIELDS) != 0;
+    const int nwin = (int)b->w.size();
+    if (nsteps == 0) return PSC_OK;
+    PSC_TRY(batch_prepare(*b, diag, fields));
+    PSC_TRY(batch_plain_steps(*b, diag ? nsteps - 1 : nsteps));
+    if (diag) {
+        // final step: IMB and partials, then loads and post-stream reductions of every window
+        PSC_TRY(batch_launch(*b, PSC_STEP_COLLIDE | PSC_STEP_IMB | PSC_STEP_REDUCE));
+        b->parity ^= 1;
+        batch_sync_cur(*b);
+        PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_pre.p, b->stream));
+        for (int k = 0; k < nwin; ++k) {
+            Window& w = *b->w[(size_t)k];
+            if (b->frozen[(size_t)k] >= 0) continue;
+            psc_geometry g = w.geometry();
+            PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p,
+                                       b->red_pre.p + (size_t)k * PSC_NRED + PSC_RED_IMBX, w.forces.p, w.torques.p,
+                                       b->diag.p + (size_t)k * PSC_NDIAG, b->stream));
+            w.loads_ready = true;
+        }
+        PSC_TRY(batch_launch(*b, PSC_STEP_REDUCE | (fields ? PSC_STEP_MOMENTS : 0u)));
+        PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_post.p, b->stream));
+        double* host = b->host.p;
+        const size_t rows = (size_t)nwin * PSC_NRED;
+        PSC_CUDA(cudaMemcpyAsync(host, b->red_pre.p, rows * 8, cudaMemcpyDeviceToHost, b->stream), "psc_batch_step");
+        PSC_CUDA(cudaMemcpyAsync(host + rows, b->red_post.p, rows * 8, cudaMemcpyDeviceToHost, b->stream),
+                 "psc_batch_step");
+        PSC_CUDA(cudaMemcpyAsync(host + 2 * rows, b->diag.p, (size_t)nwin * PSC_NDIAG * 8, cudaMemcpyDeviceToHost,
+                                 b->stream),
+                 "psc_batch_step");
+        PSC_CUDA(cudaStreamSynchronize(b->stream), "psc_batch_step");
+        for (int k = 0; k < nwin; ++k) {
+            Window& w = *b->w[(size_t)k];
+            if (b->frozen[(size_t)k] >= 0) continue;
+            double row[kOutLen];
+            std::memcpy(row, host + (size_t)k * PSC_NRED, PSC_NRED * 8);
+            std::memcpy(row + PSC_NRED, host + rows + (size_t)k * PSC_NRED, PSC_NRED * 8);
+            std::memcpy(row + 2 * PSC_NRED, host + 2 * rows + (size_t)k * PSC_NDIAG, PSC_NDIAG * 8);
+            fill_diag(w, row, b->last[(size_t)k]);
+            b->have_diag[(size_t)k] = 1;
+            w.stepped = true;
+            w.moments_ready = fields;
+            w.diag_ready = true;
+        }
+    } else if (fields) {
+        PSC_TRY(batch_launch(*b, PSC_STEP_MOMENTS));
+        for (auto& wp : b->w) wp->moments_ready = true;
+        PSC_CUDA(cudaStreamSynchronize(b->stream), "psc_batch_step");
+    } else {
+        PSC_CUDA(cudaGetLastError(), "psc_batch_step");
+    }
+    if (h_status)
+        for (int k = 0; k < nwin; ++k) {
+            h_status[k] = psc_status{};
+            h_status[k].steps_done = b->frozen[(size_t)k] >= 0 ? 0 : nsteps;
+            h_status[k].residual = INFINITY;
+            h_status[k].diag = b->last[(size_t)k];
+        }
+    return PSC_OK;
+}
+
+int psc_batch_converge(psc_batch* b, double tol, int check_every, int max_steps, int min_steps, int freeze,
+                       psc_status* h_status) {
+    if (!b) return fail(PSC_E_INVALID, "psc_batch_converge: null handle");
+    if (!(tol > 0.0) || check_every < 2 || max_steps < 2 || min_steps < 0)
+        return fail(PSC_E_INVALID, "psc_batch_converge: need tol > 0, check_every >= 2, max_steps >= 2");
+    DeviceScope ds(b->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_batch_converge: cudaSetDevice");
+    const int nwin = (int)b->w.size();
+    PSC_TRY(batch_prepare(*b, false, false));
+    std::vector<double> r1((size_t)nwin * PSC_NRED), r2((size_t)nwin * PSC_NRED);
+    std::vector<int> conv((size_t)nwin, -1);
+    std::vector<double> resid((size_t)nwin, INFINITY);
+    int done = 0;
+    while (done < max_steps) {
+        const int n = std::max(0, std::min(check_every - 1, max_steps - done - 1));
+        PSC_TRY(batch_plain_steps(*b, n));
+        done += n;
+        PSC_TRY(batch_observe(*b, r1.data()));
+        PSC_TRY(batch_plain_steps(*b, 1));
+        done += 1;
+        PSC_TRY(batch_observe(*b, r2.data()));
+        bool all = true;
+        for (int k = 0; k < nwin; ++k) {
+            const Window& w = *b->w[(size_t)k];
+            const double* row2 = r2.data() + (size_t)k * PSC_NRED;
+            if (row2[PSC_RED_NONFINITE] > 0.0)
+                return fail(PSC_E_INVALID, "psc_batch_converge: non-finite moments in window " + std::to_string(k));
+            const double k1 = row_permeability(w, r1.data() + (size_t)k * PSC_NRED);
+            const double k2 = row_permeability(w, row2);
+            if (conv[(size_t)k] < 0) {
+                resid[(size_t)k] = std::fabs(k2 - k1) / std::max(std::fabs(k2), 1e-300);
+                if (resid[(size_t)k] < tol && done >= min_steps) {
+                    conv[(size_t)k] = done;
+                    if (freeze) PSC_TRY(batch_freeze(*b, k, row2));
+                }
+            }
+            all = all && conv[(size_t)k] >= 0;
+        }
+        if (all) break;
+    }
+    PSC_TRY(batch_observe(*b, r2.data()));
+    for (int k = 0; k < nwin; ++k) {
+        Window& w = *b->w[(size_t)k];
+        double row[kOutLen] = {0};
+        std::memcpy(row + PSC_NRED, r2.data() + (size_t)k * PSC_NRED, PSC_NRED * 8);
+        psc_diag d{};
+        fill_diag(w, row, d);
+        if (h_status) {
+            h_status[k] = psc_status{};
+            h_status[k].steps_done = conv[(size_t)k] >= 0 ? conv[(size_t)k] : done;
+            h_status[k].converged = conv[(size_t)k] >= 0;
+            h_status[k].residual = resid[(size_t)k];
+            h_status[k].diag = d;
+        }
+    }
+    return PSC_OK;
+}
+
+int psc_batch_get_diag(psc_batch* b, int win, psc_diag* h_diag) {
+    if (!b || !h_diag || win < 0 || win >= (int)b->w.size())
+        return fail(PSC_E_INVALID, "psc_batch_get_diag: bad arguments");
+    if (!b->have_diag[(size_t)win])
+        return fail(PSC_E_INVALID, "psc_batch_get_diag: no PSC_RUN_DIAG step has run for this window");
+    *h_diag = b->last[(size_t)win];
+    return PSC_OK;
+}
+
+int psc_batch_get_loads(psc_batch* b, int win, double* h_forces, double* h_torques) {
+    if (!b || win < 0 || win >= (int)b->w.size()) return fail(PSC_E_INVALID, "psc_batch_get_loads: bad window");
+    Window& w = *b->w[(size_t)win];
+    if (w.P == 0) return PSC_OK;
+    if (!h_forces || !h_torques) return fail(PSC_E_INVALID, "psc_batch_get_loads: null output");
+    if (!w.loads_ready) return fail(PSC_E_INVALID, "psc_batch_get_loads: no PSC_RUN_DIAG step has run since the last step");
+    DeviceScope ds(b->device);
+    PSC_CUDA(cudaMemcpyAsync(h_forces, w.forces.p, (size_t)w.P * 24, cudaMemcpyDeviceToHost, b->stream),
+             "psc_batch_get_loads");
+    PSC_CUDA(cudaMemcpyAsync(h_torques, w.torques.p, (size_t)w.P * 24, cudaMemcpyDeviceToHost, b->stream),
+             "psc_batch_get_loads");
+    PSC_CUDA(cudaStreamSynchronize(b->stream), "psc_batch_get_loads");
+    return PSC_OK;
+}
+
+int psc_batch_get_fields(psc_batch* b, int win, int which, double* h_dst) {
+    if (!b || win < 0 || win >= (int)b->w.size()) return fail(PSC_E_INVALID, "psc_batch_get_fields: bad window");
+    DeviceScope ds(b->device);
+    Window& w = *b->w[(size_t)win];
+    batch_sync_cur(*b);
+    return window_get_field(w, which, h_dst, b->stream, b->tot, "psc_batch_get_fields");
+}
+
+}  // extern "C"

@@ -427,7 +427,7 @@ class LatticeWindow:
         if self.solid_ptr is None:
             raise RuntimeError("geometry not bound")
         fl = flags | nat.STEP_COLLIDE | (nat.STEP_MOVING if self.moving else 0)
-        nat.call("psc_step", self.store, vp(self.windows(self.cur)), 1, self.tiles, fl, 0,
+        nat.call("psc_step_windows", self.store, vp(self.windows(self.cur)), 1, self.tiles, fl, 0,
                  stream_handle(self.device))
         self.cur = 1 - self.cur
 
@@ -438,7 +438,7 @@ class LatticeWindow:
         """Moments (and reductions) of the current post-stream state, no collision."""
         self.ensure_fields(imb=False, moments=write_fields)
         fl = (nat.STEP_MOMENTS if write_fields else 0) | (nat.STEP_REDUCE if reduce_out is not None else 0)
-        nat.call("psc_step", self.store, vp(self.windows(self.cur)), 1, self.tiles, fl, 0,
+        nat.call("psc_step_windows", self.store, vp(self.windows(self.cur)), 1, self.tiles, fl, 0,
                  stream_handle(self.device))
         if reduce_out is not None:
             self.reduce(reduce_out)

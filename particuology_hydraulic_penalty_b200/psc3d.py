@@ -5,7 +5,9 @@ src/lbm_dem/psc3d.py (wangjianfttt/particuology_Hydraulic-penalty-), so that
 the permeability probe (scripts/run_psc_permeability_resolution.py:127-143),
 the coupled driver (coupling_sync/couple_psc_liggghts.py:582-607) and the
 validation drivers run unchanged on one B200.  Every step runs in
-libpscb200.so; attributes are host copies made on access.
+libpscb200.so behind one native solver handle (``psc_solver``: device
+memory, stream, geometry, results); one ``collide_stream_psc()`` is one
+``psc_step`` call.  Attributes are host copies made on access.
 
 Extra keyword-only arguments (absent from the reference):
     precision   "fp64-exact" (default: bit-identical to the reference),
@@ -25,7 +27,8 @@ import numpy as np
 import torch
 
 from . import _native as nat
-from .engine import (DeviceGeometry, LatticeWindow, particles_array, require_cuda, store_mode, trt_tau_minus)
+from .engine import particles_array, require_cuda, store_mode, trt_tau_minus
+from .handle import SolverHandle, make_config
 
 # D3Q19 velocity set in the reference's index order (psc3d.py:17-43).
 C = np.array(
@@ -110,67 +113,53 @@ class PscD3Q19:
             raise ValueError("force must have three components")
         if collision not in ("bgk", "trt"):
             raise ValueError("collision must be 'bgk' (the reference) or 'trt'")
+        if collision == "trt" and self._store == nat.STORE_F64_EXACT:
+            raise ValueError("TRT collision runs in the deviation storage modes (fp64, fp32, fp16, bf16)")
+        if self._store != nat.STORE_F64_EXACT and self.subsamples ** 3 > 255:
+            raise ValueError("the FP32/FP16/BF16 and fast-FP64 modes store the solid level as uint8 "
+                             "and need subsamples <= 6")
+        if store_scale is not None and not (np.isfinite(store_scale) and store_scale > 0.0):
+            raise ValueError("store_scale must be a positive finite number")
         self.collision = collision
-        shape = (self.n,) * 3
-        with torch.cuda.device(self._device):
-            self._win = LatticeWindow(shape, self.tau, self.force, self.subsamples, self._store, store_scale,
-                                      self._device,
-                                      tau_minus=trt_tau_minus(self.tau) if collision == "trt" else 0.0)
-            self._geo = DeviceGeometry(shape, self.subsamples, self._device,
-                                       want_level=self._store != nat.STORE_F64_EXACT)
-            self._win.bind_geometry(self._geo)
-            self._win.ensure_fields(imb=True, moments=True)
-            parr = particles_array(particles)
-            self._geo.set_particles(parr)
-            self._P = parr.shape[0]
-            self._forces_dev = torch.zeros((self._P, 3), dtype=torch.float64, device=self._device)
-            self._torques_dev = torch.zeros((self._P, 3), dtype=torch.float64, device=self._device)
-            # post-stream reductions and load diagnostics land in one buffer read back per call
-            self._out_dev = torch.zeros(nat.NRED + nat.NDIAG, dtype=torch.float64, device=self._device)
-            self._red_post_dev = self._out_dev[: nat.NRED]
-            self._diag_dev = self._out_dev[nat.NRED:]
-            self._out_host = torch.zeros(nat.NRED + nat.NDIAG, dtype=torch.float64).pin_memory()
+        index = self._device.index if self._device.index is not None else torch.cuda.current_device()
+        cfg = make_config((self.n,) * 3, tau=self.tau, force=self.force, subsamples=self.subsamples,
+                          store=self._store, static_geometry=self.static_geometry, device_index=index,
+                          tau_minus=trt_tau_minus(self.tau) if collision == "trt" else 0.0, store_scale=store_scale)
+        self._h = SolverHandle(cfg)
+        parr = particles_array(particles)
+        self._h.set_particles(parr)
+        self._P = parr.shape[0]
         self._geometry_built = False
         self._stepped = False
-        self._moments_ready = False
         self._loads_host = None
         self._cache: dict = {}
         self._hf = np.zeros((self._P, 3), dtype=float)
         self._ht = np.zeros((self._P, 3), dtype=float)
         self._momentum_residual = 0.0
+        self._nonfinite = False
 
     # ------------------------------------------------------------------
     # geometry
     # ------------------------------------------------------------------
-    def _upload_particles(self) -> np.ndarray:
+    def _upload_particles(self) -> None:
         parr = particles_array(self.particles)
-        with torch.cuda.device(self._device):
-            self._geo.set_particles(parr)
-            if parr.shape[0] != self._P:
-                self._P = parr.shape[0]
-                self._forces_dev = torch.zeros((self._P, 3), dtype=torch.float64, device=self._device)
-                self._torques_dev = torch.zeros((self._P, 3), dtype=torch.float64, device=self._device)
-                self._geometry_built = False
-        return parr
+        self._h.set_particles(parr)
+        self._P = parr.shape[0]
 
     def rebuild_geometry(self) -> None:
         """Solid fraction from S^3 sub-samples per cell (psc3d.py:151-179 / 328-345)."""
         self._upload_particles()
-        with torch.cuda.device(self._device):
-            self._geo.rebuild()
+        self._h.rebuild_geometry()
         self._geometry_built = True
-        self._cache.pop("solid", None)
-        self._cache.pop("dense", None)
-        self._cache.pop("sparse", None)
+        for key in ("solid", "sparse", "dense", "alpha_sum"):
+            self._cache.pop(key, None)
 
     def solid_velocity(self):
         """alpha-weighted rigid-body velocity per node (psc3d.py:181-206 / 347-373)."""
-        if not self._geometry_built:
-            self.rebuild_geometry()
-        with torch.cuda.device(self._device):
-            us = torch.empty(3 * self._geo.N, dtype=torch.float64, device=self._device)
-            self._geo.solid_velocity(us)
-            us = us.view(3, self.n, self.n, self.n).cpu().numpy()
+        self._upload_particles()
+        shape = self._shape3()
+        us = [self._h.field(nat.FIELD_US_X + k).reshape(shape) for k in range(3)]
+        self._geometry_built = True
         return us[0], us[1], us[2]
 
     # ------------------------------------------------------------------
@@ -178,53 +167,29 @@ class PscD3Q19:
     # ------------------------------------------------------------------
     def collide_stream_psc(self) -> dict:
         """One PSC-IMB collide + stream step (psc3d.py:208-253)."""
-        with torch.cuda.device(self._device):
-            if (not self.static_geometry) or (not self._geometry_built):
-                self.rebuild_geometry()
-            else:
-                # positions / velocities may have been mutated in place: they feed
-                # the solid velocity and the torque arms even for static geometry
-                self._upload_particles()
-                if not self._geometry_built:
-                    self.rebuild_geometry()
-            parr = self._geo.host_particles
-            moving = bool(parr.shape[0]) and bool(np.any(parr[:, 4:10] != 0.0))
-            win = self._win
-            if moving:
-                self._geo.solid_velocity(win.ensure_us())
-            win.set_moving(moving)
-            win.step(nat.STEP_IMB | nat.STEP_REDUCE)
-            win.reduce(win.red)
-            self._geo.loads(win.imb, win.red[nat.RED_IMBX:], self._forces_dev, self._torques_dev, self._diag_dev)
-            # reductions of the post-stream state only; the fields are made on access
-            win.moments_pass(self._red_post_dev, write_fields=False)
-            self._out_host.copy_(self._out_dev, non_blocking=True)
-            torch.cuda.current_stream(self._device).synchronize()
+        # positions / velocities may have been mutated in place: they feed the
+        # geometry, the solid velocity and the torque arms (re-read every call)
+        self._upload_particles()
+        d = self._h.step(1, nat.RUN_DIAG).diag
+        self._geometry_built = True
         self._stepped = True
-        self._moments_ready = False
         self._loads_host = None
         self._cache.clear()
-        host = self._out_host.numpy()
-        red_post = host[: nat.NRED]
-        diag = host[nat.NRED:]
-        P = self._P
-        self._momentum_residual = float(diag[nat.DIAG_MOMENTUM_RESIDUAL])
-        if red_post[nat.RED_NONFINITE] > 0:
+        self._momentum_residual = float(d.momentum_residual)
+        if d.nonfinite_cells > 0:
             self._nonfinite = True
         return {
-            "solid_volume_lu": float(red_post[nat.RED_SOLID]),
-            "mean_uz": float(red_post[nat.RED_UZ] / self._geo.N),
-            "momentum_residual": float(self._momentum_residual),
-            "max_force": float(diag[nat.DIAG_MAX_FORCE]) if P else 0.0,
-            "max_torque": float(diag[nat.DIAG_MAX_TORQUE]) if P else 0.0,
+            "solid_volume_lu": float(d.solid_volume_lu),
+            "mean_uz": float(d.mean_uz),
+            "momentum_residual": float(d.momentum_residual),
+            "max_force": float(d.max_force),
+            "max_torque": float(d.max_torque),
         }
 
     # loads are copied to the host when read ------------------------------
     def _fetch_loads(self) -> None:
         if self._loads_host is None:
-            with torch.cuda.device(self._device):
-                f = self._forces_dev.cpu().numpy()
-                t = self._torques_dev.cpu().numpy()
+            f, t = self._h.loads()
             self._store_loads(f, t)
             self._loads_host = True
 
@@ -272,16 +237,17 @@ class PscD3Q19:
 
     def accumulate_particle_loads(self) -> None:
         """Recompute particle force / torque from the last step's IMB field (psc3d.py:255-281)."""
-        if not self._geometry_built:
-            self.rebuild_geometry()
-        with torch.cuda.device(self._device):
-            self._geo.loads(self._win.imb, self._win.red[nat.RED_IMBX:], self._forces_dev, self._torques_dev,
-                            self._diag_dev)
-            host = torch.cat([self._diag_dev, self._forces_dev.view(-1), self._torques_dev.view(-1)]).cpu().numpy()
-        P = self._P
-        self._store_loads(host[nat.NDIAG: nat.NDIAG + 3 * P].reshape(P, 3), host[nat.NDIAG + 3 * P:].reshape(P, 3))
+        if not self._stepped:
+            # no IMB momentum yet: the loads of a fluid at rest are zero
+            self._store_loads(np.zeros((self._P, 3)), np.zeros((self._P, 3)))
+            self.momentum_residual = 0.0
+            return
+        self._upload_particles()
+        self._h.accumulate_loads()
+        f, t = self._h.loads()
+        self._store_loads(f, t)
         self._loads_host = True
-        self.momentum_residual = float(host[nat.DIAG_MOMENTUM_RESIDUAL])
+        self.momentum_residual = float(self._h.diag().momentum_residual)
 
     # ------------------------------------------------------------------
     # host views
@@ -289,98 +255,84 @@ class PscD3Q19:
     def _shape3(self):
         return (self.n, self.n, self.n)
 
-    def _moment(self, k: int) -> np.ndarray:
-        if not self._stepped:
-            return np.ones(self._shape3()) if k == 0 else np.zeros(self._shape3())
-        if not self._moments_ready:
-            with torch.cuda.device(self._device):
-                self._win.moments_pass(None, write_fields=True)
-            self._moments_ready = True
-        key = ("mom", k)
+    def _field(self, which: int) -> np.ndarray:
+        key = ("field", which)
         if key not in self._cache:
-            N = self._geo.N
-            self._cache[key] = self._win.moments[k * N:(k + 1) * N].to(torch.float64).cpu().numpy().reshape(
-                self._shape3())
+            self._cache[key] = self._h.field(which).reshape(self._shape3())
         return self._cache[key]
 
     @property
     def rho(self) -> np.ndarray:
-        return self._moment(0)
+        return self._field(nat.FIELD_RHO)
 
     @property
     def ux(self) -> np.ndarray:
-        return self._moment(1)
+        return self._field(nat.FIELD_UX)
 
     @property
     def uy(self) -> np.ndarray:
-        return self._moment(2)
+        return self._field(nat.FIELD_UY)
 
     @property
     def uz(self) -> np.ndarray:
-        return self._moment(3)
-
-    def _imb(self, k: int) -> np.ndarray:
-        key = ("imb", k)
-        if key not in self._cache:
-            N = self._geo.N
-            self._cache[key] = self._win.imb[k * N:(k + 1) * N].to(torch.float64).cpu().numpy().reshape(
-                self._shape3())
-        return self._cache[key]
+        return self._field(nat.FIELD_UZ)
 
     @property
     def imb_mx(self) -> np.ndarray:
-        return self._imb(0)
+        return self._field(nat.FIELD_IMB_X)
 
     @property
     def imb_my(self) -> np.ndarray:
-        return self._imb(1)
+        return self._field(nat.FIELD_IMB_Y)
 
     @property
     def imb_mz(self) -> np.ndarray:
-        return self._imb(2)
+        return self._field(nat.FIELD_IMB_Z)
 
     @property
     def solid(self) -> np.ndarray:
-        if not self._geometry_built:
-            return np.zeros(self._shape3())
         if "solid" not in self._cache:
-            self._cache["solid"] = self._geo.solid.cpu().numpy().reshape(self._shape3())
+            self._cache["solid"] = self._h.field(nat.FIELD_SOLID).reshape(self._shape3())
         return self._cache["solid"]
 
     @property
     def f(self) -> np.ndarray:
         """Post-stream populations (19, n, n, n), absolute FP64 (psc3d.py:140, :242)."""
         if "f" not in self._cache:
-            with torch.cuda.device(self._device):
-                self._cache["f"] = self._win.post_stream_f().cpu().numpy()
+            self._cache["f"] = self._h.field(nat.FIELD_F).reshape((19, *self._shape3()))
         return self._cache["f"]
 
     @f.setter
     def f(self, value) -> None:
-        t = torch.as_tensor(np.asarray(value, dtype=np.float64))
-        with torch.cuda.device(self._device):
-            self._win.load_post_stream_f(t)
+        self._h.set_populations(np.asarray(value, dtype=np.float64))
         self._cache.clear()
-        self._moments_ready = False
+
+    def _sparse(self):
+        if "sparse" not in self._cache:
+            self._cache["sparse"] = self._h.sparse_alpha()
+        return self._cache["sparse"]
+
+    def _alpha_sum(self) -> np.ndarray:
+        if "alpha_sum" not in self._cache:
+            self._cache["alpha_sum"] = self._h.field(nat.FIELD_ALPHA_SUM)
+        return self._cache["alpha_sum"]
 
     @property
     def alpha_p(self) -> np.ndarray:
         """Dense (P, n, n, n) solid fractions per particle (psc3d.py:141, :173)."""
         if "dense" not in self._cache:
-            ids, vals = self._geo.sparse_lists() if self._geometry_built else ([], [])
-            n3 = self._geo.N
-            out = np.zeros((self._P, n3))
+            ids, vals = self._sparse()
+            out = np.zeros((self._h.P, self.n ** 3))
             for p, (i, v) in enumerate(zip(ids, vals)):
                 out[p, i] = v
-            self._cache["dense"] = out.reshape((self._P, *self._shape3()))
+            self._cache["dense"] = out.reshape((self._h.P, *self._shape3()))
         return self._cache["dense"]
 
     @property
     def owner_weights(self) -> np.ndarray:
         """alpha_p / sum alpha where the sum exceeds 1e-14 (psc3d.py:176-178)."""
         a = self.alpha_p
-        s = self._geo.alpha_sum.cpu().numpy().reshape(self._shape3()) if self._geometry_built else np.zeros(
-            self._shape3())
+        s = self._alpha_sum().reshape(self._shape3())
         out = np.zeros_like(a)
         mask = s > 1.0e-14
         out[:, mask] = a[:, mask] / s[mask]
@@ -402,11 +354,6 @@ class SparsePscD3Q19(PscD3Q19):
                          static_geometry=static_geometry, **kwargs)
         self.geometry_workers = max(1, int(geometry_workers))
 
-    def _sparse(self):
-        if "sparse" not in self._cache:
-            self._cache["sparse"] = self._geo.sparse_lists() if self._geometry_built else ([], [])
-        return self._cache["sparse"]
-
     @property
     def node_ids(self) -> list:
         return self._sparse()[0]
@@ -417,6 +364,4 @@ class SparsePscD3Q19(PscD3Q19):
 
     @property
     def alpha_sum_flat(self) -> np.ndarray:
-        if not self._geometry_built:
-            return np.zeros(self._geo.N)
-        return self._geo.alpha_sum.cpu().numpy()
+        return self._alpha_sum()

@@ -1,0 +1,182 @@
+"""The handle layer (psc_solver / psc_batch): multi-step calls, the
+lbm_converge criterion run natively, and batches of windows behind one
+handle must reproduce the oracle and the single-step / Python-side paths
+exactly."""
+
+import numpy as np
+import pytest
+
+from oracle import psc_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _window(n=24, kind="passive", seed=5):
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+
+    return wgen.make_window(n, kind, seed)
+
+
+def _solver(w, precision="fp64-exact", static=True, force=(0.0, 0.0, 2e-6), subsamples=2, tau=0.8, **kw):
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.engine import store_mode
+    from particuology_hydraulic_penalty_b200.handle import SolverHandle, make_config
+
+    cfg = make_config((w.n,) * 3, tau=tau, force=force, subsamples=subsamples, store=store_mode(precision),
+                      static_geometry=static, **kw)
+    h = SolverHandle(cfg)
+    h.set_particles(w.particles)
+    return h, nat
+
+
+def test_fields_before_first_step():
+    w = _window(16)
+    h, nat = _solver(w)
+    assert np.all(h.field(nat.FIELD_RHO) == 1.0)
+    assert np.all(h.field(nat.FIELD_UZ) == 0.0)
+    assert np.all(h.field(nat.FIELD_SOLID) == 0.0)  # nothing voxelised yet (psc3d.py:144)
+    F, T = h.loads()
+    assert not F.any() and not T.any()
+
+
+def test_multi_step_call_matches_oracle_bitwise():
+    w = _window()
+    h, nat = _solver(w)
+    st = h.step(6, nat.RUN_DIAG)
+    assert st.steps_done == 6
+    o = orc.OracleSolver(w.n, w.particles, tau=0.8, subsamples=2, body_force_z=2e-6, static_geometry=True)
+    for _ in range(6):
+        d = o.collide_stream_psc()
+    shape = (w.n,) * 3
+    assert np.array_equal(h.field(nat.FIELD_F).reshape((19, *shape)), o.f)
+    assert np.array_equal(h.field(nat.FIELD_UZ).reshape(shape), o.uz)
+    assert np.array_equal(h.field(nat.FIELD_SOLID).reshape(shape), o.solid)
+    assert abs(st.diag.mean_uz - d["mean_uz"]) <= 1e-14 * abs(d["mean_uz"])
+    F, T = h.loads()
+    assert np.linalg.norm(F - o.hydro_forces) <= 1e-12 * np.linalg.norm(o.hydro_forces)
+    # Darcy K of the diagnostics (run_psc_permeability_resolution.py:144-150)
+    k = orc.darcy_permeability(o.solid, o.uz, 0.8, 2e-6)["permeability_lu"]
+    assert abs(st.diag.permeability - k) <= 1e-12 * abs(k)
+
+
+def test_converge_flag_matches_python_loop():
+    """PSC_RUN_CONVERGE stops where lbm_converge (couple_psc_liggghts.py:284-296) stops."""
+    from particuology_hydraulic_penalty_b200 import SparsePscD3Q19
+    from particuology_hydraulic_penalty_b200.coupling import lbm_converge
+
+    w = _window(20, "skeleton", 7)
+    tol = 1e-2
+    h, nat = _solver(w, precision="fp32", subsamples=3, conv_tol=tol, conv_min_steps=3)
+    st = h.step(400, nat.RUN_CONVERGE)
+    s = SparsePscD3Q19(w.n, w.particles, tau=0.8, subsamples=3, body_force_z=2e-6, static_geometry=True,
+                       precision="fp32")
+    it, res, ok, diag = lbm_converge(s, residual_tol=tol, min_steps=3, max_steps=400)
+    assert ok and st.converged == 1
+    assert st.steps_done == it
+    assert st.residual == res
+    assert st.diag.mean_uz == diag["mean_uz"]
+    assert st.diag.momentum_residual == diag["momentum_residual"]
+    assert np.array_equal(h.field(nat.FIELD_F), s.f.reshape(-1))
+
+
+def test_moving_nonstatic_rebuilds_like_oracle():
+    """Particles moved between calls of a non-static solver: voxelised again, bit for bit."""
+    w = _window(20, "preloaded", 9)
+    parts = w.particles.copy()
+    parts[:, 4] = 1e-3
+    h, nat = _solver(w, static=False)
+    o = orc.OracleSolver(w.n, parts, tau=0.8, subsamples=2, body_force_z=2e-6, static_geometry=False)
+    for step in range(3):
+        moved = parts.copy()
+        moved[:, 0] += 0.37 * step
+        h.set_particles(moved)
+        o.particles = moved
+        h.step(1, nat.RUN_DIAG)
+        o.collide_stream_psc()
+    shape = (w.n,) * 3
+    assert np.array_equal(h.field(nat.FIELD_SOLID).reshape(shape), o.solid)
+    assert np.array_equal(h.field(nat.FIELD_F).reshape((19, *shape)), o.f)
+    us = np.stack([h.field(nat.FIELD_US_X + k).reshape(shape) for k in range(3)])
+    assert np.array_equal(us, orc.solid_velocity(o.particles, o.geo))
+
+
+def test_accumulate_and_populations_roundtrip():
+    w = _window(16, "skeleton", 3)
+    h, nat = _solver(w, subsamples=3)
+    h.step(2, 0)
+    F0, T0 = h.loads()
+    h.accumulate_loads()
+    F1, T1 = h.loads()
+    assert np.array_equal(F0, F1) and np.array_equal(T0, T1)
+    f = h.field(nat.FIELD_F)
+    h.set_populations(f)
+    assert np.array_equal(h.field(nat.FIELD_F), f)
+
+
+def _batch(wins, precision="fp32", launch=None, graph_steps=4):
+    from particuology_hydraulic_penalty_b200.engine import store_mode
+    from particuology_hydraulic_penalty_b200.handle import BatchHandle, make_config
+
+    cfgs = [make_config((w.n,) * 3, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=4, store=store_mode(precision))
+            for w in wins]
+    b = BatchHandle(cfgs, launch=launch, graph_steps=graph_steps)
+    for k, w in enumerate(wins):
+        b.set_particles(k, w.particles)
+    return b
+
+
+def _three():
+    return [_window(24, "skeleton", 1), _window(32, "passive", 2), _window(40, "preloaded", 3)]
+
+
+@pytest.mark.parametrize("precision", ["fp64-exact", "fp32", "fp16"])
+def test_batch_handle_matches_python_batch(precision):
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    wins = _three()
+    b = _batch(wins, precision)
+    st = b.step(11, nat.RUN_DIAG)  # graph replays + direct steps + the reporting step
+    py = PscBatch([WindowSpec(w.n, w.particles, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=4) for w in wins],
+                  precision=precision, graph_steps=4)
+    py.run(10)
+    loads = py.loads()  # one more step with IMB
+    red = py.observe()
+    K = py.permeability(red)
+    for k, w in enumerate(wins):
+        assert st[k].steps_done == 11
+        assert st[k].diag.permeability == K[k]
+        mom = py.velocity_field(k)
+        assert np.array_equal(b.field(k, nat.FIELD_UX), mom[1].reshape(-1).astype(np.float64))
+        F, T = b.loads(k)
+        assert np.array_equal(F, loads[k][0]) and np.array_equal(T, loads[k][1])
+
+
+def test_batch_handle_tma_matches_direct():
+    from particuology_hydraulic_penalty_b200 import _native as nat
+
+    wins = _three()
+    direct = _batch(wins)
+    tma = _batch(wins, launch=nat.PscLaunch(0, 1, nat.KERNEL_TMA, 3, 0))
+    direct.step(9, nat.RUN_DIAG)
+    tma.step(9, nat.RUN_DIAG)
+    for k in range(len(wins)):
+        assert np.array_equal(direct.field(k, nat.FIELD_F), tma.field(k, nat.FIELD_F))
+        assert direct.diag(k).permeability == tma.diag(k).permeability
+
+
+def test_batch_handle_converge_matches_python():
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    wins = _three()
+    b = _batch(wins, graph_steps=10)
+    st = b.converge(tol=1e-4, check_every=50, max_steps=3000)
+    py = PscBatch([WindowSpec(w.n, w.particles, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=4) for w in wins],
+                  precision="fp32", graph_steps=10)
+    res = py.run_to_convergence(tol=1e-4, check_every=50, max_steps=3000)
+    assert res["converged"].any()
+    for k in range(len(wins)):
+        assert bool(st[k].converged) == bool(res["converged"][k])
+        if res["converged"][k]:
+            assert st[k].steps_done == int(res["steps"][k])
+        assert st[k].diag.permeability == res["permeability"][k]

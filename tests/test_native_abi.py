@@ -25,7 +25,7 @@ def declared_functions():
 
 def test_header_declares_entry_points():
     names = declared_functions()
-    assert "psc_step" in names and "psc_geometry_build" in names
+    assert "psc_step_windows" in names and "psc_geometry_build" in names
     assert len(names) >= 14
 
 
@@ -63,8 +63,8 @@ def test_host_only_entry_points(lib):
 
 
 def test_null_arguments_rejected_without_device(lib):
-    assert lib.psc_step(0, None, 1, 1, 1, 0, None) == nat.PSC_E_INVALID
-    assert lib.psc_step(9, None, 1, 1, 1, 0, None) == nat.PSC_E_INVALID
+    assert lib.psc_step_windows(0, None, 1, 1, 1, 0, None) == nat.PSC_E_INVALID
+    assert lib.psc_step_windows(9, None, 1, 1, 1, 0, None) == nat.PSC_E_INVALID
     assert lib.psc_init_equilibrium(0, 1.0, None, 10, None) == nat.PSC_E_INVALID
     assert lib.psc_geometry_plan(None, None) == nat.PSC_E_INVALID
     assert lib.psc_stream_push(0, 1.0, None, None, 4, 4, 4, None) == nat.PSC_E_INVALID
@@ -79,3 +79,57 @@ def test_product_requires_cuda():
         pytest.skip("a GPU is visible")
     with pytest.raises(RuntimeError, match="CUDA"):
         PscD3Q19(8, [Particle3D(4.0, 4.0, 4.0, 2.0)])
+
+
+def _config(**kw):
+    c = nat.PscConfig()
+    c.nx = c.ny = c.nz = 16
+    c.subsamples = 4
+    c.store = nat.STORE_F32
+    c.tau = 0.8
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+def test_handle_layer_layout(lib):
+    assert lib.psc_config_size() == ctypes.sizeof(nat.PscConfig)
+    assert lib.psc_diag_size() == ctypes.sizeof(nat.PscDiag)
+    assert lib.psc_status_size() == ctypes.sizeof(nat.PscStatus)
+
+
+@pytest.mark.parametrize("kw, code, words", [
+    ({"nx": 0}, nat.PSC_E_INVALID, b"extents"),
+    ({"store": 9}, nat.PSC_E_INVALID, b"store"),
+    ({"subsamples": 7}, nat.PSC_E_UNSUPPORTED, b"uint8"),
+    ({"tau": -1.0}, nat.PSC_E_INVALID, b"tau"),
+    ({"store": nat.STORE_F64_EXACT, "tau_minus": 1.0}, nat.PSC_E_UNSUPPORTED, b"TRT"),
+    ({"nx": 1000, "ny": 1000, "nz": 200}, nat.PSC_E_UNSUPPORTED, b"2^31"),
+])
+def test_handle_config_rejected_before_device_use(lib, kw, code, words):
+    h = ctypes.c_void_p()
+    cfg = _config(**kw)
+    assert lib.psc_create(ctypes.byref(cfg), ctypes.byref(h)) == code
+    assert words in lib.psc_last_error()
+    assert not h.value
+
+
+def test_handle_null_arguments(lib):
+    h = ctypes.c_void_p()
+    assert lib.psc_create(None, ctypes.byref(h)) == nat.PSC_E_INVALID
+    st = nat.PscStatus()
+    assert lib.psc_step(None, 1, 0, ctypes.byref(st)) == nat.PSC_E_INVALID
+    assert lib.psc_get_fields(None, 0, None) == nat.PSC_E_INVALID
+    assert lib.psc_set_particles(None, None, 0) == nat.PSC_E_INVALID
+    assert lib.psc_destroy(None) == nat.PSC_OK
+    assert lib.psc_batch_destroy(None) == nat.PSC_OK
+
+
+def test_batch_config_mismatch_rejected(lib):
+    cfgs = (nat.PscConfig * 2)(_config(), _config(store=nat.STORE_F64))
+    b = ctypes.c_void_p()
+    assert lib.psc_batch_create(cfgs, 2, None, 20, ctypes.byref(b)) == nat.PSC_E_INVALID
+    assert b"same store" in lib.psc_last_error()
+    cfgs = (nat.PscConfig * 2)(_config(), _config())
+    assert lib.psc_batch_create(cfgs, 2, None, 3, ctypes.byref(b)) == nat.PSC_E_INVALID
+    assert b"even" in lib.psc_last_error()

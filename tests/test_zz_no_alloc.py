@@ -19,28 +19,44 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def _solver():
-    from particuology_hydraulic_penalty_b200 import SparsePscD3Q19
-
+def _particles():
     rng = np.random.default_rng(42)
     P = 30
     parts = np.zeros((P, 10))
     parts[:, 0:3] = rng.uniform(-1.0, 25.0, size=(P, 3))
     parts[:, 3] = rng.uniform(1.0, 4.0, size=P)
     parts[:, 4:7] = rng.normal(0.0, 1e-4, size=(P, 3))
-    s = SparsePscD3Q19(24, parts, tau=0.8, subsamples=3, body_force_z=2e-6, static_geometry=True,
-                       precision="fp64-exact")
-    s.collide_stream_psc()
-    s.collide_stream_psc()  # geometry, IMB field and its sums of the last step are now on the device
-    return s
+    return parts
+
+
+def _state():
+    """Geometry and lattice of a caller that owns the device buffers (descriptor layer), two steps in."""
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.engine import DeviceGeometry, LatticeWindow
+
+    dev = torch.device("cuda", 0)
+    shape = (24, 24, 24)
+    with torch.cuda.device(dev):
+        geo = DeviceGeometry(shape, 3, dev, want_level=False)
+        geo.set_particles(_particles())
+        geo.rebuild()
+        win = LatticeWindow(shape, 0.8, (0.0, 0.0, 2e-6), 3, nat.STORE_F64_EXACT, None, dev)
+        win.bind_geometry(geo)
+        geo.solid_velocity(win.ensure_us())
+        win.set_moving(True)
+        for _ in range(2):
+            win.step(nat.STEP_IMB | nat.STEP_REDUCE)
+        win.reduce(win.red)  # IMB momentum sums of the last step
+    return geo, win
 
 
 def test_static_scratch_loads_match_caller_scratch_loads():
     from particuology_hydraulic_penalty_b200 import _native as nat
     from particuology_hydraulic_penalty_b200.engine import stream_handle, vp
 
-    s = _solver()
-    geo, win = s._geo, s._win
+    from particuology_hydraulic_penalty_b200 import SparsePscD3Q19
+
+    geo, win = _state()
     dev = win.imb.device
     g = geo.struct()
     assert 0 < g.capacity_chunks <= nat.LOADS_STATIC_MAX_CHUNKS
@@ -63,7 +79,11 @@ def test_static_scratch_loads_match_caller_scratch_loads():
             a, b = a.cpu().numpy(), b.cpu().numpy()
             assert np.all(np.isfinite(a))
             assert np.linalg.norm(a - b) <= 1e-12 * max(np.linalg.norm(b), 1e-300)
-    # the forces also match what the drop-in solver reported for that step
+    # the forces also match what the drop-in solver reports for the same two steps
+    s = SparsePscD3Q19(24, _particles(), tau=0.8, subsamples=3, body_force_z=2e-6, static_geometry=True,
+                       precision="fp64-exact")
+    s.collide_stream_psc()
+    s.collide_stream_psc()
     assert np.linalg.norm(out[0].cpu().numpy() - s.hydro_forces) <= 1e-12 * np.linalg.norm(s.hydro_forces)
 
 
@@ -71,13 +91,13 @@ def test_static_scratch_rejects_oversized_geometry():
     from particuology_hydraulic_penalty_b200 import _native as nat
     from particuology_hydraulic_penalty_b200.engine import stream_handle, vp
 
-    s = _solver()
-    g = s._geo.struct()
+    geo, win = _state()
+    g = geo.struct()
     g.capacity_chunks = nat.LOADS_STATIC_MAX_CHUNKS + 1
     lib = nat.load()
-    out = torch.zeros((s._geo.P, 3), dtype=torch.float64, device=s._win.imb.device)
+    out = torch.zeros((geo.P, 3), dtype=torch.float64, device=win.imb.device)
     diag = torch.zeros(nat.NDIAG, dtype=torch.float64, device=out.device)
-    rc = lib.psc_particle_loads_static(ctypes.byref(g), 0, vp(s._win.imb), vp(s._win.red[nat.RED_IMBX:]), vp(out),
+    rc = lib.psc_particle_loads_static(ctypes.byref(g), 0, vp(win.imb), vp(win.red[nat.RED_IMBX:]), vp(out),
                                        vp(out), vp(diag), stream_handle(out.device))
     assert rc == nat.PSC_E_CAPACITY
     assert b"scratch holds" in lib.psc_last_error()
