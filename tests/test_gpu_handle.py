@@ -155,7 +155,8 @@ def test_batch_handle_matches_python_batch(precision):
 def test_batch_handle_tma_matches_direct():
     from particuology_hydraulic_penalty_b200 import _native as nat
 
-    wins = _three()
+    # bulk copies of the uint8 level rows need nz % 16 == 0
+    wins = [_window(32, "skeleton", 1), _window(48, "passive", 2), _window(32, "preloaded", 3)]
     direct = _batch(wins)
     tma = _batch(wins, launch=nat.PscLaunch(0, 1, nat.KERNEL_TMA, 3, 0))
     direct.step(9, nat.RUN_DIAG)
