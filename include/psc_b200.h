@@ -100,6 +100,10 @@ typedef struct psc_launch {
 #define PSC_RED_NONFINITE 11 /* number of cells with a non-finite moment */
 #define PSC_RED_SOLID 12     /* sum of the clipped solid fraction (solid_volume_lu) */
 #define PSC_NRED 13
+/* Rows of reduction partials per tile: one per warp of the step kernels'
+ * 256-thread (consumer) CTAs, so no tile waits on a block-wide barrier.
+ * psc_window.partials holds [tile_count][PSC_PARTIAL_ROWS][PSC_NRED]. */
+#define PSC_PARTIAL_ROWS 8
 
 /* Diagnostics written by psc_particle_loads() (psc3d.py:247-253). */
 #define PSC_DIAG_MOMENTUM_RESIDUAL 0
@@ -130,7 +134,7 @@ typedef struct psc_window {
     const void* us;        /* solid velocity [3][N] (double in F64 modes, float otherwise) */
     void* imb;             /* IMB momentum [3][N] (double in F64 modes, float otherwise) */
     void* moments;         /* rho, ux, uy, uz [4][N] (same element type as imb) */
-    double* partials;      /* [tile_count][PSC_NRED] */
+    double* partials;      /* [tile_count][PSC_PARTIAL_ROWS][PSC_NRED] */
     double tau_minus;      /* TRT: antisymmetric relaxation time (0 = BGK, the reference's collision);
                               deviation storage modes only */
 } psc_window;

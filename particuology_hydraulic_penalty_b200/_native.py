@@ -47,6 +47,7 @@ RED_IMBX, RED_IMBY, RED_IMBZ = 8, 9, 10
 RED_NONFINITE = 11
 RED_SOLID = 12
 NRED = 13
+PARTIAL_ROWS = 8  # partial rows per tile (one per warp of a step CTA)
 
 DIAG_MOMENTUM_RESIDUAL, DIAG_MAX_FORCE, DIAG_MAX_TORQUE = 0, 1, 2
 DIAG_FORCE_SUM = (3, 4, 5)

@@ -132,10 +132,11 @@ class PscBatch:
                 nat.call("psc_plan_tiles", arr, nwin, nat.STEP_THREADS * self.cells_per_thread, ctypes.byref(total))
             if self.partials is None:
                 self.total_tiles = int(total.value)
-                self.partials = torch.zeros(self.total_tiles * nat.NRED, dtype=torch.float64, device=self.device)
+                self.partials = torch.zeros(self.total_tiles * nat.PARTIAL_ROWS * nat.NRED, dtype=torch.float64,
+                                            device=self.device)
             base = self.partials.data_ptr()
             for k in range(nwin):
-                arr[k].partials = base + int(arr[k].tile_begin) * nat.NRED * 8
+                arr[k].partials = base + int(arr[k].tile_begin) * nat.PARTIAL_ROWS * nat.NRED * 8
             tables.append(struct_to_device(arr, self.device))
         self._tables = tables
         self._graphs = {}

@@ -338,48 +338,78 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*s)[NV]) {
 
 constexpr int LOAD_THREADS = 256;
 
-// One block per chunk of one particle's bbox entries.
+// Inside fraction inside / S^3 for every sample count (S <= 16): the exact
+// IEEE quotient of psc3d.py:88, computed once per block.
+constexpr int LOAD_ALPHA_LUT = 16 * 16 * 16 + 1;
+
+// One block per chunk of one particle's bbox entries.  A thread visits the
+// entries e0 + tid, e0 + tid + 256, ...; their bbox coordinates advance by a
+// fixed mixed-radix stride with carries (one 32-bit division per chunk).
 template <typename I>
 __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, const I* imb, double* part) {
     __shared__ double s[LOAD_THREADS / 32][6];
+    __shared__ double s_al[LOAD_ALPHA_LUT];
     const int64_t C = g.totals[1];
     const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
-    const double S3d = (double)(g.subsamples * g.subsamples * g.subsamples);
+    const uint32_t ny = (uint32_t)g.ny, nz = (uint32_t)g.nz;
+    const int S3 = g.subsamples * g.subsamples * g.subsamples;
+    const double S3d = (double)S3;
+    for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
+    __syncthreads();
     for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {
         const int p = owner_of(g.chunk_off, g.nparticles, chunk);
-        const int64_t e0 = g.ent_off[p] + (chunk - g.chunk_off[p]) * g.chunk_entries;
+        const int64_t eb = g.ent_off[p];
+        const int64_t e0 = eb + (chunk - g.chunk_off[p]) * g.chunk_entries;
         const int64_t e1 = min(e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
         const double* q = g.particles + (size_t)p * PF;
         const int32_t* bb = g.bbox + (size_t)p * 6;
-        const int64_t eyz = (int64_t)bb[4] * bb[5];
+        const uint32_t ey = (uint32_t)bb[4], ez = (uint32_t)bb[5];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-            const uint16_t cnt = g.ent_cnt[e];
-            if (cnt == 0) continue;
-            const int64_t local = e - g.ent_off[p];
-            const int32_t a = (int32_t)(local / eyz);
-            const int64_t rem = local - (int64_t)a * eyz;
-            const int32_t b = (int32_t)(rem / bb[5]);
-            const int32_t k = (int32_t)(rem - (int64_t)b * bb[5]);
-            const int32_t ix = bb[0] + a, iy = bb[1] + b, iz = bb[2] + k;
-            const uint32_t cell = ((uint32_t)ix * g.ny + iy) * g.nz + iz;
-            // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
-            const double al = xdiv((double)cnt, S3d);
-            const double as = g.alpha_sum[cell];
-            const double ow = xdiv(al, as > 1.0e-14 ? as : 1.0e-14);
-            const double nfx = -xmul(ow, (double)imb[cell]);
-            const double nfy = -xmul(ow, (double)imb[(size_t)N + cell]);
-            const double nfz = -xmul(ow, (double)imb[2 * (size_t)N + cell]);
-            // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
-            const double rx = xsub(xadd((double)ix, 0.5), q[0]);
-            const double ry = xsub(xadd((double)iy, 0.5), q[1]);
-            const double rz = xsub(xadd((double)iz, 0.5), q[2]);
-            acc[0] += nfx;
-            acc[1] += nfy;
-            acc[2] += nfz;
-            acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
-            acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
-            acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
+        if (e0 + threadIdx.x < e1) {
+            // bbox-local coordinates of this thread's first entry, and the stride
+            const uint32_t local = (uint32_t)(e0 - eb) + threadIdx.x;
+            const uint32_t eyz = ey * ez;
+            uint32_t a = local / eyz;
+            const uint32_t rem = local - a * eyz;
+            uint32_t b = rem / ez;
+            uint32_t k = rem - b * ez;
+            const uint32_t step_k = blockDim.x % ez;
+            const uint32_t step_q = blockDim.x / ez;
+            const uint32_t step_b = step_q % ey;
+            const uint32_t step_a = step_q / ey;
+            const double qx = q[0], qy = q[1], qz = q[2];
+            for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+                const uint16_t cnt = g.ent_cnt[e];
+                if (cnt != 0) {
+                    const uint32_t ix = (uint32_t)bb[0] + a, iy = (uint32_t)bb[1] + b, iz = (uint32_t)bb[2] + k;
+                    const uint32_t cell = (ix * ny + iy) * nz + iz;
+                    // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
+                    const double al = s_al[cnt];
+                    const double as = g.alpha_sum[cell];
+                    const double ow = xdiv(al, as > 1.0e-14 ? as : 1.0e-14);
+                    const double nfx = -xmul(ow, (double)imb[cell]);
+                    const double nfy = -xmul(ow, (double)imb[(size_t)N + cell]);
+                    const double nfz = -xmul(ow, (double)imb[2 * (size_t)N + cell]);
+                    // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
+                    const double rx = xsub(xadd((double)ix, 0.5), qx);
+                    const double ry = xsub(xadd((double)iy, 0.5), qy);
+                    const double rz = xsub(xadd((double)iz, 0.5), qz);
+                    acc[0] += nfx;
+                    acc[1] += nfy;
+                    acc[2] += nfz;
+                    acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
+                    acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
+                    acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
+                }
+                // next entry of this thread: (a, b, k) += (step_a, step_b, step_k) with carries
+                k += step_k;
+                const uint32_t ck = k >= ez;
+                k -= ck ? ez : 0u;
+                b += step_b + ck;
+                const uint32_t cb = b >= ey;
+                b -= cb ? ey : 0u;
+                a += step_a + cb;
+            }
         }
         block_sum<6>(acc, s);
         if (threadIdx.x == 0) {

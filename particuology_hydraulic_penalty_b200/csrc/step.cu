@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restr
     using R = typename TR::R;
     using O = typename TR::O;
     __shared__ int64_t s_begin[MAX_SMEM_WINDOWS];
-    __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
+    static_assert(STEP_THREADS / 32 == PSC_PARTIAL_ROWS, "one partial row per warp");
     const bool in_smem = nwin <= MAX_SMEM_WINDOWS;
     if (in_smem) {
         for (int i = threadIdx.x; i < nwin; i += blockDim.x) s_begin[i] = wins[i].tile_begin;
@@ -163,18 +163,18 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restr
                 red[PSC_RED_SOLID] = solid_d;
             }
         }
-        if (do_red) block_reduce_store<PSC_NRED>(red, s_red, W.partials + local_tile * PSC_NRED);
+        if (do_red) warp_reduce_store<PSC_NRED>(red, W.partials + local_tile * (PSC_PARTIAL_ROWS * PSC_NRED));
     }
 }
 
-// Sum each window's tile partials in a fixed order (deterministic).
+// Sum each window's tile partials (PSC_PARTIAL_ROWS rows per tile) in a fixed order (deterministic).
 __global__ void k_reduce_windows(const psc_window* __restrict__ wins, double* __restrict__ out) {
     __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
     const psc_window& W = wins[blockIdx.x];
     double acc[PSC_NRED];
 #pragma unroll
     for (int k = 0; k < PSC_NRED; ++k) acc[k] = 0.0;
-    for (int64_t j = threadIdx.x; j < W.tile_count; j += blockDim.x) {
+    for (int64_t j = threadIdx.x; j < W.tile_count * PSC_PARTIAL_ROWS; j += blockDim.x) {
         const double* p = W.partials + j * PSC_NRED;
 #pragma unroll
         for (int k = 0; k < PSC_NRED; ++k) acc[k] += p[k];

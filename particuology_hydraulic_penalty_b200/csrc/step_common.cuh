@@ -134,6 +134,21 @@ __device__ __forceinline__ int find_window(const psc_window* wins, const int64_t
     return lo;
 }
 
+// Warp sums of v, written as this warp's row of a tile's partials:
+// rows[warp][k] for k < NV (lane k stores value k).  No block barrier.
+template <int NV>
+__device__ __forceinline__ void warp_reduce_store(double (&v)[NV], double* rows) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* out = rows + (size_t)warp * NV;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) x += __shfl_xor_sync(0xffffffffu, x, s);
+        if (lane == k) out[k] = x;
+    }
+}
+
 template <int NV>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double (*s_red)[NV], double* out) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

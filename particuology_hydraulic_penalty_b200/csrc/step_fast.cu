@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
     using R = typename TR::R;
     using O = typename TR::O;
     __shared__ FastWin<T, R, O> sw;
-    __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
+    static_assert(STEP_THREADS / 32 == PSC_PARTIAL_ROWS, "one partial row per warp");
     const bool do_collide = flags & PSC_STEP_COLLIDE;
     const bool do_imb = do_collide && (flags & PSC_STEP_IMB);
     const bool do_mom = flags & PSC_STEP_MOMENTS;
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
                 red[PSC_RED_SOLID] += solid;
             }
         }
-        if (do_red) block_reduce_store<PSC_NRED>(red, s_red, sw.partials + (t - sw.tile_begin) * PSC_NRED);
+        if (do_red) warp_reduce_store<PSC_NRED>(red, sw.partials + (t - sw.tile_begin) * (PSC_PARTIAL_ROWS * PSC_NRED));
     }
 }
 

@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full[STAGES], empty[STAGES];
     __shared__ TmaWin<T, R, O> sw;
-    __shared__ double s_red[TMA_CONSUMERS / 32][PSC_NRED];
+    static_assert(TMA_CONSUMERS / 32 == PSC_PARTIAL_ROWS, "one partial row per consumer warp");
     __shared__ int s_abort;
 
     const int64_t t0 = (total_tiles * (int64_t)blockIdx.x) / gridDim.x;
@@ -381,23 +381,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
         // this warp is done reading stage s
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[s]);
-        if (do_red) {
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-            for (int q = 0; q < PSC_NRED; ++q) {
-                double x = red[q];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-                if (lane == 0) s_red[warp][q] = x;
-            }
-            consumer_sync();
-            if (threadIdx.x < PSC_NRED) {
-                double acc = 0.0;
-                for (int w = 0; w < TMA_CONSUMERS / 32; ++w) acc += s_red[w][threadIdx.x];
-                sw.partials[(t - sw.tile_begin) * PSC_NRED + threadIdx.x] = acc;
-            }
-            consumer_sync();
-        }
+        if (do_red) warp_reduce_store<PSC_NRED>(red, sw.partials + (t - sw.tile_begin) * (PSC_PARTIAL_ROWS * PSC_NRED));
         ++k;
     }
 }

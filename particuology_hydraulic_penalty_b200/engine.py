@@ -413,7 +413,8 @@ class LatticeWindow:
                 nat.call("psc_plan_tiles", ctypes.byref(w), 1, 0, ctypes.byref(total))
                 if self.partials is None or self.tiles != total.value:
                     self.tiles = total.value
-                    self.partials = torch.zeros(self.tiles * nat.NRED, dtype=torch.float64, device=self.device)
+                    self.partials = torch.zeros(self.tiles * nat.PARTIAL_ROWS * nat.NRED, dtype=torch.float64,
+                                                device=self.device)
                 w.partials = vp(self.partials)
                 structs.append(w)
             self._win_dev = [struct_to_device(structs[0], self.device), struct_to_device(structs[1], self.device)]

@@ -163,7 +163,9 @@ def test_batch_handle_tma_matches_direct():
     tma.step(9, nat.RUN_DIAG)
     for k in range(len(wins)):
         assert np.array_equal(direct.field(k, nat.FIELD_F), tma.field(k, nat.FIELD_F))
-        assert direct.diag(k).permeability == tma.diag(k).permeability
+        # row tiles group the FP64 partial sums differently from 256-cell tiles
+        kd, kt = direct.diag(k).permeability, tma.diag(k).permeability
+        assert abs(kd - kt) <= 1e-12 * abs(kd)
 
 
 def test_batch_handle_converge_matches_python():
