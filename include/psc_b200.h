@@ -247,7 +247,9 @@ int psc_step_windows(int store, const struct psc_window* d_windows, int nwin, in
 int psc_step_windows_ex(int store, const struct psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
                 const psc_launch* cfg, void* stream);
 /* Sum the per-tile partials of each window in a fixed order (deterministic)
- * into out[nwin][PSC_NRED] (device). */
+ * into out[nwin][PSC_NRED] (device).  The partials are consumed: segment sums
+ * are written over them, so reduce once per PSC_STEP_REDUCE pass.  nwin must
+ * not exceed 65535. */
 int psc_reduce_windows(const struct psc_window* d_windows, int nwin, double* out, void* stream);
 
 /* ---- particle loads (psc3d.py:255-281 / 375-407) ------------------------ */

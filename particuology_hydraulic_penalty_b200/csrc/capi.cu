@@ -246,6 +246,7 @@ int psc_step_windows(int store, const psc_window* d_windows, int nwin, int64_t t
 
 int psc_reduce_windows(const psc_window* d_windows, int nwin, double* out, void* stream) {
     if (!d_windows || nwin <= 0 || !out) return fail(PSC_E_INVALID, "psc_reduce_windows: bad arguments");
+    if (nwin > 65535) return fail(PSC_E_UNSUPPORTED, "psc_reduce_windows: at most 65535 windows per call");
     cudaError_t e = launch_reduce_windows(d_windows, nwin, out, as_stream(stream));
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_reduce_windows");
 }

@@ -167,15 +167,48 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restr
     }
 }
 
-// Sum each window's tile partials (PSC_PARTIAL_ROWS rows per tile) in a fixed order (deterministic).
-__global__ void k_reduce_windows(const psc_window* __restrict__ wins, double* __restrict__ out) {
+// Window sums of the tile partials ([tile_count][PSC_PARTIAL_ROWS][PSC_NRED]
+// rows), deterministic, in two launches:
+//  1. k_reduce_segments: blockIdx.y = window; blocks stride over segments of
+//     REDUCE_SEG consecutive rows; each segment is summed by a fixed tree and
+//     its sum written over the segment's first row (the partials are consumed);
+//  2. k_reduce_windows: one block per window sums the segment rows in order.
+constexpr int REDUCE_SEG = STEP_THREADS;
+constexpr int REDUCE_SEG_BLOCKS = 64;  // blocks per window in launch 1
+
+__global__ void __launch_bounds__(STEP_THREADS) k_reduce_segments(const psc_window* __restrict__ wins) {
+    __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
+    __shared__ double s_out[PSC_NRED];
+    const psc_window& W = wins[blockIdx.y];
+    const int64_t rows = W.tile_count * PSC_PARTIAL_ROWS;
+    const int64_t nseg = (rows + REDUCE_SEG - 1) / REDUCE_SEG;
+    for (int64_t sg = blockIdx.x; sg < nseg; sg += gridDim.x) {  // block-uniform
+        const int64_t r = sg * REDUCE_SEG + threadIdx.x;
+        double v[PSC_NRED];
+        if (r < rows) {
+            const double* p = W.partials + r * PSC_NRED;
+#pragma unroll
+            for (int k = 0; k < PSC_NRED; ++k) v[k] = p[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < PSC_NRED; ++k) v[k] = 0.0;
+        }
+        block_reduce_store<PSC_NRED>(v, s_red, s_out);  // every read of the segment precedes its barrier
+        if (threadIdx.x < PSC_NRED) W.partials[sg * REDUCE_SEG * PSC_NRED + threadIdx.x] = s_out[threadIdx.x];
+    }
+}
+
+__global__ void __launch_bounds__(STEP_THREADS) k_reduce_windows(const psc_window* __restrict__ wins,
+                                                                 double* __restrict__ out) {
     __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
     const psc_window& W = wins[blockIdx.x];
+    const int64_t rows = W.tile_count * PSC_PARTIAL_ROWS;
+    const int64_t nseg = (rows + REDUCE_SEG - 1) / REDUCE_SEG;
     double acc[PSC_NRED];
 #pragma unroll
     for (int k = 0; k < PSC_NRED; ++k) acc[k] = 0.0;
-    for (int64_t j = threadIdx.x; j < W.tile_count * PSC_PARTIAL_ROWS; j += blockDim.x) {
-        const double* p = W.partials + j * PSC_NRED;
+    for (int64_t sg = threadIdx.x; sg < nseg; sg += blockDim.x) {
+        const double* p = W.partials + sg * REDUCE_SEG * PSC_NRED;
 #pragma unroll
         for (int k = 0; k < PSC_NRED; ++k) acc[k] += p[k];
     }
@@ -310,6 +343,9 @@ cudaError_t launch_step(int store, const psc_window* d_windows, int nwin, int64_
 }
 
 cudaError_t launch_reduce_windows(const psc_window* d_windows, int nwin, double* out, cudaStream_t stream) {
+    k_reduce_segments<<<dim3(REDUCE_SEG_BLOCKS, (unsigned)nwin), STEP_THREADS, 0, stream>>>(d_windows);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     k_reduce_windows<<<nwin, STEP_THREADS, 0, stream>>>(d_windows, out);
     return cudaGetLastError();
 }
