@@ -100,9 +100,13 @@ typedef struct psc_launch {
 #define PSC_RED_NONFINITE 11 /* number of cells with a non-finite moment */
 #define PSC_RED_SOLID 12     /* sum of the clipped solid fraction (solid_volume_lu) */
 #define PSC_NRED 13
-/* Rows of reduction partials per tile: one per warp of the step kernels'
- * 256-thread (consumer) CTAs, so no tile waits on a block-wide barrier.
- * psc_window.partials holds [tile_count][PSC_PARTIAL_ROWS][PSC_NRED]. */
+/* Reduction partials of one window: a header row (element 0 = number of
+ * rows that follow, written by the step kernel) and up to
+ * tile_count * PSC_PARTIAL_ROWS rows of PSC_NRED doubles.  The persistent
+ * kernels accumulate each thread's cells over the CTA's whole run of tiles
+ * inside the window and write one row per warp and CTA (no per-tile
+ * reduction, no block barrier); the exact kernel writes one row per warp and
+ * tile.  Sums are deterministic for a given launch configuration. */
 #define PSC_PARTIAL_ROWS 8
 
 /* Diagnostics written by psc_particle_loads() (psc3d.py:247-253). */
@@ -134,7 +138,7 @@ typedef struct psc_window {
     const void* us;        /* solid velocity [3][N] (double in F64 modes, float otherwise) */
     void* imb;             /* IMB momentum [3][N] (double in F64 modes, float otherwise) */
     void* moments;         /* rho, ux, uy, uz [4][N] (same element type as imb) */
-    double* partials;      /* [tile_count][PSC_PARTIAL_ROWS][PSC_NRED] */
+    double* partials;      /* [1 + tile_count * PSC_PARTIAL_ROWS][PSC_NRED] (header row first) */
     double tau_minus;      /* TRT: antisymmetric relaxation time (0 = BGK, the reference's collision);
                               deviation storage modes only */
 } psc_window;

@@ -132,11 +132,12 @@ class PscBatch:
                 nat.call("psc_plan_tiles", arr, nwin, nat.STEP_THREADS * self.cells_per_thread, ctypes.byref(total))
             if self.partials is None:
                 self.total_tiles = int(total.value)
-                self.partials = torch.zeros(self.total_tiles * nat.PARTIAL_ROWS * nat.NRED, dtype=torch.float64,
-                                            device=self.device)
+                # per window: a header row, then up to tile_count * PARTIAL_ROWS rows
+                self.partials = torch.zeros((nwin + self.total_tiles * nat.PARTIAL_ROWS) * nat.NRED,
+                                            dtype=torch.float64, device=self.device)
             base = self.partials.data_ptr()
             for k in range(nwin):
-                arr[k].partials = base + int(arr[k].tile_begin) * nat.PARTIAL_ROWS * nat.NRED * 8
+                arr[k].partials = base + (k + int(arr[k].tile_begin) * nat.PARTIAL_ROWS) * nat.NRED * 8
             tables.append(struct_to_device(arr, self.device))
         self._tables = tables
         self._graphs = {}

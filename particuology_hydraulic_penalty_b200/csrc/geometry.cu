@@ -341,6 +341,7 @@ constexpr int LOAD_THREADS = 256;
 // Inside fraction inside / S^3 for every sample count (S <= 16): the exact
 // IEEE quotient of psc3d.py:88, computed once per block.
 constexpr int LOAD_ALPHA_LUT = 16 * 16 * 16 + 1;
+constexpr int LOAD_UNROLL = 4;
 
 // One block per chunk of one particle's bbox entries.  A thread visits the
 // entries e0 + tid, e0 + tid + 256, ...; their bbox coordinates advance by a
@@ -378,22 +379,52 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, c
             const uint32_t step_b = step_q % ey;
             const uint32_t step_a = step_q / ey;
             const double qx = q[0], qy = q[1], qz = q[2];
-            for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-                const uint16_t cnt = g.ent_cnt[e];
-                if (cnt != 0) {
-                    const uint32_t ix = (uint32_t)bb[0] + a, iy = (uint32_t)bb[1] + b, iz = (uint32_t)bb[2] + k;
-                    const uint32_t cell = (ix * ny + iy) * nz + iz;
+            // LOAD_UNROLL entries per pass: their loads are issued together, then
+            // accumulated in entry order (the order of a one-entry loop)
+            const uint32_t bx = (uint32_t)bb[0], by = (uint32_t)bb[1], bz = (uint32_t)bb[2];
+            for (int64_t e = e0 + threadIdx.x; e < e1; e += (int64_t)LOAD_UNROLL * blockDim.x) {
+                uint16_t cnt[LOAD_UNROLL];
+                uint32_t cx[LOAD_UNROLL], cy[LOAD_UNROLL], cz[LOAD_UNROLL];
+#pragma unroll
+                for (int u = 0; u < LOAD_UNROLL; ++u) {
+                    const int64_t eu = e + (int64_t)u * blockDim.x;
+                    cnt[u] = eu < e1 ? g.ent_cnt[eu] : (uint16_t)0;
+                    cx[u] = bx + a;
+                    cy[u] = by + b;
+                    cz[u] = bz + k;
+                    // next entry of this thread: (a, b, k) += (step_a, step_b, step_k) with carries
+                    k += step_k;
+                    const uint32_t ck = k >= ez;
+                    k -= ck ? ez : 0u;
+                    b += step_b + ck;
+                    const uint32_t cb = b >= ey;
+                    b -= cb ? ey : 0u;
+                    a += step_a + cb;
+                }
+                double as[LOAD_UNROLL], mx[LOAD_UNROLL], my[LOAD_UNROLL], mz[LOAD_UNROLL];
+#pragma unroll
+                for (int u = 0; u < LOAD_UNROLL; ++u) {
+                    if (cnt[u] != 0) {
+                        const uint32_t cell = (cx[u] * ny + cy[u]) * nz + cz[u];
+                        as[u] = g.alpha_sum[cell];
+                        mx[u] = (double)imb[cell];
+                        my[u] = (double)imb[(size_t)N + cell];
+                        mz[u] = (double)imb[2 * (size_t)N + cell];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < LOAD_UNROLL; ++u) {
+                    if (cnt[u] == 0) continue;
                     // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
-                    const double al = s_al[cnt];
-                    const double as = g.alpha_sum[cell];
-                    const double ow = xdiv(al, as > 1.0e-14 ? as : 1.0e-14);
-                    const double nfx = -xmul(ow, (double)imb[cell]);
-                    const double nfy = -xmul(ow, (double)imb[(size_t)N + cell]);
-                    const double nfz = -xmul(ow, (double)imb[2 * (size_t)N + cell]);
+                    const double al = s_al[cnt[u]];
+                    const double ow = xdiv(al, as[u] > 1.0e-14 ? as[u] : 1.0e-14);
+                    const double nfx = -xmul(ow, mx[u]);
+                    const double nfy = -xmul(ow, my[u]);
+                    const double nfz = -xmul(ow, mz[u]);
                     // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
-                    const double rx = xsub(xadd((double)ix, 0.5), qx);
-                    const double ry = xsub(xadd((double)iy, 0.5), qy);
-                    const double rz = xsub(xadd((double)iz, 0.5), qz);
+                    const double rx = xsub(xadd((double)cx[u], 0.5), qx);
+                    const double ry = xsub(xadd((double)cy[u], 0.5), qy);
+                    const double rz = xsub(xadd((double)cz[u], 0.5), qz);
                     acc[0] += nfx;
                     acc[1] += nfy;
                     acc[2] += nfz;
@@ -401,14 +432,6 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, c
                     acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
                     acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
                 }
-                // next entry of this thread: (a, b, k) += (step_a, step_b, step_k) with carries
-                k += step_k;
-                const uint32_t ck = k >= ez;
-                k -= ck ? ez : 0u;
-                b += step_b + ck;
-                const uint32_t cb = b >= ey;
-                b -= cb ? ey : 0u;
-                a += step_a + cb;
             }
         }
         block_sum<6>(acc, s);

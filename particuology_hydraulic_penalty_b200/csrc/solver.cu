@@ -283,7 +283,7 @@ int window_init(Window& w, const psc_config& c, cudaStream_t s, const char* who)
     // tiles (ceil(N / 256)) or row tiles (at most nx * ny); descriptor tables
     // keep this pointer, so it never moves
     w.partials_cap = std::max<int64_t>((N + 255) / 256, (int64_t)c.nx * c.ny);
-    PSC_CUDA(w.partials.ensure(w.partials_cap * PSC_PARTIAL_ROWS * PSC_NRED, true, s), who);
+    PSC_CUDA(w.partials.ensure((1 + w.partials_cap * PSC_PARTIAL_ROWS) * PSC_NRED, true, s), who);
     PSC_CUDA(cudaEventCreateWithFlags(&w.upload_done, cudaEventDisableTiming), who);
     return PSC_OK;
 }

@@ -163,30 +163,43 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restr
                 red[PSC_RED_SOLID] = solid_d;
             }
         }
-        if (do_red) warp_reduce_store<PSC_NRED>(red, W.partials + local_tile * (PSC_PARTIAL_ROWS * PSC_NRED));
+        if (do_red) {  // one row per warp and tile; the block of local tile 0 writes the header
+            warp_reduce_store<PSC_NRED>(red, W.partials + (1 + local_tile * PSC_PARTIAL_ROWS) * PSC_NRED);
+            if (local_tile == 0 && threadIdx.x == 0) W.partials[0] = (double)(W.tile_count * PSC_PARTIAL_ROWS);
+        }
     }
 }
 
-// Window sums of the tile partials ([tile_count][PSC_PARTIAL_ROWS][PSC_NRED]
-// rows), deterministic, in two launches:
+// Window sums of the partial rows (header row: element 0 = row count; the
+// rows follow it), deterministic, in two launches:
 //  1. k_reduce_segments: blockIdx.y = window; blocks stride over segments of
 //     REDUCE_SEG consecutive rows; each segment is summed by a fixed tree and
 //     its sum written over the segment's first row (the partials are consumed);
 //  2. k_reduce_windows: one block per window sums the segment rows in order.
 constexpr int REDUCE_SEG = STEP_THREADS;
+
+// Row count from the header, clamped to the window's capacity.
+__device__ __forceinline__ int64_t partial_rows(const psc_window& W) {
+    const double h = W.partials[0];
+    const int64_t cap = W.tile_count * PSC_PARTIAL_ROWS;
+    if (!(h > 0.0)) return 0;
+    const int64_t r = (int64_t)h;
+    return r < cap ? r : cap;
+}
 constexpr int REDUCE_SEG_BLOCKS = 64;  // blocks per window in launch 1
 
 __global__ void __launch_bounds__(STEP_THREADS) k_reduce_segments(const psc_window* __restrict__ wins) {
     __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
     __shared__ double s_out[PSC_NRED];
     const psc_window& W = wins[blockIdx.y];
-    const int64_t rows = W.tile_count * PSC_PARTIAL_ROWS;
+    const int64_t rows = partial_rows(W);
     const int64_t nseg = (rows + REDUCE_SEG - 1) / REDUCE_SEG;
+    double* body = W.partials + PSC_NRED;
     for (int64_t sg = blockIdx.x; sg < nseg; sg += gridDim.x) {  // block-uniform
         const int64_t r = sg * REDUCE_SEG + threadIdx.x;
         double v[PSC_NRED];
         if (r < rows) {
-            const double* p = W.partials + r * PSC_NRED;
+            const double* p = body + r * PSC_NRED;
 #pragma unroll
             for (int k = 0; k < PSC_NRED; ++k) v[k] = p[k];
         } else {
@@ -194,7 +207,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_reduce_segments(const psc_wind
             for (int k = 0; k < PSC_NRED; ++k) v[k] = 0.0;
         }
         block_reduce_store<PSC_NRED>(v, s_red, s_out);  // every read of the segment precedes its barrier
-        if (threadIdx.x < PSC_NRED) W.partials[sg * REDUCE_SEG * PSC_NRED + threadIdx.x] = s_out[threadIdx.x];
+        if (threadIdx.x < PSC_NRED) body[sg * REDUCE_SEG * PSC_NRED + threadIdx.x] = s_out[threadIdx.x];
     }
 }
 
@@ -202,13 +215,13 @@ __global__ void __launch_bounds__(STEP_THREADS) k_reduce_windows(const psc_windo
                                                                  double* __restrict__ out) {
     __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
     const psc_window& W = wins[blockIdx.x];
-    const int64_t rows = W.tile_count * PSC_PARTIAL_ROWS;
+    const int64_t rows = partial_rows(W);
     const int64_t nseg = (rows + REDUCE_SEG - 1) / REDUCE_SEG;
     double acc[PSC_NRED];
 #pragma unroll
     for (int k = 0; k < PSC_NRED; ++k) acc[k] = 0.0;
     for (int64_t sg = threadIdx.x; sg < nseg; sg += blockDim.x) {
-        const double* p = W.partials + sg * REDUCE_SEG * PSC_NRED;
+        const double* p = W.partials + PSC_NRED + sg * REDUCE_SEG * PSC_NRED;
 #pragma unroll
         for (int k = 0; k < PSC_NRED; ++k) acc[k] += p[k];
     }
@@ -319,6 +332,7 @@ static cudaError_t launch_step_t(const psc_window* d_windows, int nwin, int64_t 
         const int64_t g = (int64_t)sm_count() * occ;
         grid_ctas = (int)(total_tiles < g ? total_tiles : g);
     }
+    if ((int64_t)grid_ctas > total_tiles) grid_ctas = (int)total_tiles;
     if (grid_ctas <= 0) return cudaSuccess;
     k_step<STORE, MOVING><<<grid_ctas, STEP_THREADS, 0, stream>>>(d_windows, nwin, total_tiles, flags);
     return cudaGetLastError();

@@ -149,6 +149,28 @@ __device__ __forceinline__ void warp_reduce_store(double (&v)[NV], double* rows)
     }
 }
 
+// The CTA of a persistent grid of `grid` CTAs over `total` tiles (CTA b owns
+// [total * b / grid, total * (b + 1) / grid)) that owns tile t.
+__device__ __forceinline__ int64_t cta_of_tile(int64_t t, int64_t total, int64_t grid) {
+    return ((t + 1) * grid - 1) / total;
+}
+
+// End of this CTA's run of tiles inside one window: each warp writes the sums
+// of its threads' accumulators as row (b - b_first) * PSC_PARTIAL_ROWS + warp
+// of the window's partials (after the header row), and the window's first
+// CTA writes the row count into the header.  Resets the accumulators.
+template <int NV>
+__device__ __forceinline__ void flush_segment(double (&red)[NV], double* partials, int64_t tile_begin,
+                                              int64_t tile_count, int64_t total, int64_t grid) {
+    const int64_t bf = cta_of_tile(tile_begin, total, grid);
+    const int64_t bl = cta_of_tile(tile_begin + tile_count - 1, total, grid);
+    const int64_t row = ((int64_t)blockIdx.x - bf) * PSC_PARTIAL_ROWS;
+    warp_reduce_store<NV>(red, partials + (1 + row) * NV);
+    if ((int64_t)blockIdx.x == bf && threadIdx.x == 0) partials[0] = (double)((bl - bf + 1) * PSC_PARTIAL_ROWS);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) red[k] = 0.0;
+}
+
 template <int NV>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double (*s_red)[NV], double* out) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -100,8 +100,16 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
     const int64_t t0 = (total_tiles * (int64_t)blockIdx.x) / gridDim.x;
     const int64_t t1 = (total_tiles * ((int64_t)blockIdx.x + 1)) / gridDim.x;
     int64_t win_end = -1;
+    double red[PSC_NRED];  // this thread's sums over the CTA's cells of the current window
+#pragma unroll
+    for (int q = 0; q < PSC_NRED; ++q) red[q] = 0.0;
+    bool have = false;  // block-uniform: red holds cells of the window in sw
     for (int64_t t = t0; t < t1; ++t) {
         if (t >= win_end) {  // block-uniform: entering a new window
+            if (do_red && have)
+                flush_segment<PSC_NRED>(red, sw.partials, sw.tile_begin, sw.tile_end - sw.tile_begin, total_tiles,
+                                        gridDim.x);
+            have = false;
             __syncthreads();
             const int wi = find_window(wins, nullptr, nwin, t);
             load_fast_win(sw, wins[wi], MOVING);
@@ -109,6 +117,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
             win_end = sw.tile_end;
         }
         if (sw.inactive) continue;  // block-uniform
+        have = true;
         const uint32_t N = sw.N, nx = sw.nx, ny = sw.ny, nz = sw.nz;
         const uint32_t base = (uint32_t)((t - sw.tile_begin) * sw.tile_cells);
         uint32_t cell = base + threadIdx.x;
@@ -148,9 +157,6 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
             iy -= cy ? ny : 0;
             ix += sw.step_x + cy;
         }
-        double red[PSC_NRED];
-#pragma unroll
-        for (int q = 0; q < PSC_NRED; ++q) red[q] = 0.0;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             const uint32_t c = cells[k];
@@ -241,8 +247,9 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
                 red[PSC_RED_SOLID] += solid;
             }
         }
-        if (do_red) warp_reduce_store<PSC_NRED>(red, sw.partials + (t - sw.tile_begin) * (PSC_PARTIAL_ROWS * PSC_NRED));
     }
+    if (do_red && have)
+        flush_segment<PSC_NRED>(red, sw.partials, sw.tile_begin, sw.tile_end - sw.tile_begin, total_tiles, gridDim.x);
 }
 
 template <int STORE, bool MOVING, int CPT>
@@ -262,6 +269,7 @@ static cudaError_t launch_fast_t(const psc_window* d_windows, int nwin, int64_t 
         const int64_t g = (int64_t)sm_count() * occ;
         grid_ctas = (int)(total_tiles < g ? total_tiles : g);
     }
+    if ((int64_t)grid_ctas > total_tiles) grid_ctas = (int)total_tiles;  // every CTA owns >= 1 tile
     if (grid_ctas <= 0) return cudaSuccess;
     k_step_fast<STORE, MOVING, CPT><<<grid_ctas, STEP_THREADS, 0, stream>>>(d_windows, nwin, total_tiles, flags);
     return cudaGetLastError();

@@ -217,8 +217,16 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
     int64_t win_end = -1;
     uint32_t k = 0;
     bool aborted = false;  // after a stuck wait: keep joining the barriers, skip the work
+    double red[PSC_NRED];  // this thread's sums over the CTA's cells of the current window
+#pragma unroll
+    for (int q = 0; q < PSC_NRED; ++q) red[q] = 0.0;
+    bool have = false;
     for (int64_t t = t0; t < t1; ++t) {
         if (t >= win_end) {
+            if (do_red && have)
+                flush_segment<PSC_NRED>(red, sw.partials, sw.tile_begin, sw.tile_end - sw.tile_begin, total_tiles,
+                                        gridDim.x);
+            have = false;
             consumer_sync();
             if (threadIdx.x == 0) {
                 const int wi = find_window(wins, nullptr, nwin, t);
@@ -265,6 +273,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
             win_end = sw.tile_end;
         }
         if (sw.inactive) continue;  // uniform over consumers; the producer issued nothing for it
+        have = true;
         const int s = (int)(k % STAGES);
         if (!aborted && !mbar_wait(&full[s], (k / STAGES) & 1, 0x103)) {
             aborted = true;
@@ -280,9 +289,6 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
         const T* st = reinterpret_cast<const T*>(smem + (size_t)s * stage_bytes);
         const unsigned char* st_geo = smem + (size_t)s * stage_bytes + (size_t)19 * pop_elems * sizeof(T);
         const uint32_t base = (ix * ny + y0) * nz;
-        double red[PSC_NRED];
-#pragma unroll
-        for (int q = 0; q < PSC_NRED; ++q) red[q] = 0.0;
         const uint32_t dyy = TMA_CONSUMERS / nz, dz = TMA_CONSUMERS - dyy * nz;
         uint32_t yy = threadIdx.x / nz, iz = threadIdx.x - yy * nz;
         for (uint32_t c = threadIdx.x; c < (aborted ? 0u : ncell); c += TMA_CONSUMERS) {
@@ -381,9 +387,10 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
         // this warp is done reading stage s
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[s]);
-        if (do_red) warp_reduce_store<PSC_NRED>(red, sw.partials + (t - sw.tile_begin) * (PSC_PARTIAL_ROWS * PSC_NRED));
         ++k;
     }
+    if (do_red && have)
+        flush_segment<PSC_NRED>(red, sw.partials, sw.tile_begin, sw.tile_end - sw.tile_begin, total_tiles, gridDim.x);
 }
 
 template <int STORE, bool MOVING, int STAGES>
@@ -401,6 +408,7 @@ static cudaError_t launch_tma_t(const psc_window* d, int nwin, int64_t tiles, un
         const int64_t g = (int64_t)sm_count() * occ;
         grid = (int)(tiles < g ? tiles : g);
     }
+    if ((int64_t)grid > tiles) grid = (int)tiles;  // every CTA owns >= 1 tile
     if (grid <= 0) return cudaSuccess;
     kern<<<grid, TMA_THREADS, smem, s>>>(d, nwin, tiles, flags, stage_bytes);
     return cudaGetLastError();

@@ -413,7 +413,7 @@ class LatticeWindow:
                 nat.call("psc_plan_tiles", ctypes.byref(w), 1, 0, ctypes.byref(total))
                 if self.partials is None or self.tiles != total.value:
                     self.tiles = total.value
-                    self.partials = torch.zeros(self.tiles * nat.PARTIAL_ROWS * nat.NRED, dtype=torch.float64,
+                    self.partials = torch.zeros((1 + self.tiles * nat.PARTIAL_ROWS) * nat.NRED, dtype=torch.float64,
                                                 device=self.device)
                 w.partials = vp(self.partials)
                 structs.append(w)

@@ -1,8 +1,10 @@
 """Batched uneven windows: each window of a batch must evolve exactly as when solved alone.
 
 The per-cell arithmetic does not depend on how cells are tiled or which
-windows share a launch, so batched and solo runs agree bit for bit in every
-storage mode; CUDA-graph replays must match direct launches.
+windows share a launch, so batched and solo populations agree bit for bit in
+every storage mode; CUDA-graph replays must match direct launches.  FP64
+reduction sums are grouped by each launch's CTA runs, so they agree to
+rounding.
 """
 
 import numpy as np
@@ -33,7 +35,8 @@ def test_batched_equals_solo(precision):
     for k, spec in enumerate(specs):
         solo = PscBatch([spec], precision=precision, graph_steps=0)
         solo.run(11)
-        assert solo.permeability()[0] == kb[k]
+        # FP64 reduction rows are grouped by the launch's CTA runs: equal to rounding
+        assert abs(solo.permeability()[0] - kb[k]) <= 1e-12 * abs(kb[k])
         assert np.array_equal(solo.velocity_field(0), fields_b[k])
 
 
@@ -162,7 +165,7 @@ def test_converged_windows_freeze_exactly(kernel):
     for j, spec in enumerate(specs):
         solo = PscBatch([spec], precision="fp32", graph_steps=0, kernel=k)
         solo.run(int(res["steps"][j]))
-        assert solo.permeability()[0] == kb[j]
+        assert abs(solo.permeability()[0] - kb[j]) <= 1e-12 * abs(kb[j])
         assert np.array_equal(solo.velocity_field(0), b.velocity_field(j))
     assert ctypes_status() == 0
 
