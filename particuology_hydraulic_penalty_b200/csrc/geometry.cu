@@ -338,9 +338,8 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*s)[NV]) {
 
 constexpr int LOAD_THREADS = 256;
 
-// Inside fraction inside / S^3 for every sample count (S <= 16): the exact
-// IEEE quotient of psc3d.py:88, computed once per block.
-constexpr int LOAD_ALPHA_LUT = 16 * 16 * 16 + 1;
+// The block's table of inside / S^3 for every sample count (S <= 16) holds
+// the exact IEEE quotients of psc3d.py:88, computed once per block.
 constexpr int LOAD_UNROLL = 4;
 
 // One block per chunk of one particle's bbox entries.  A thread visits the
@@ -349,7 +348,7 @@ constexpr int LOAD_UNROLL = 4;
 template <typename I>
 __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, const I* imb, double* part) {
     __shared__ double s[LOAD_THREADS / 32][6];
-    __shared__ double s_al[LOAD_ALPHA_LUT];
+    extern __shared__ double s_al[];  // S^3 + 1 entries (dynamic)
     const int64_t C = g.totals[1];
     const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
     const uint32_t ny = (uint32_t)g.ny, nz = (uint32_t)g.nz;
@@ -614,14 +613,15 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
                                   const double* imb_sums, double* forces, double* torques, double* diag,
                                   cudaStream_t stream) {
     if (g.capacity_chunks > 0 && g.nparticles > 0) {
-        const int64_t cap = (int64_t)sm_count() * 8;
+        const int64_t cap = (int64_t)sm_count() * 16;
         const unsigned grid = (unsigned)(g.capacity_chunks < cap ? g.capacity_chunks : cap);
+        const size_t lut = (size_t)(g.subsamples * g.subsamples * g.subsamples + 1) * sizeof(double);
         if (imb_type == 0)
-            k_loads_chunks<double><<<grid, LOAD_THREADS, 0, stream>>>(g, reinterpret_cast<const double*>(imb),
-                                                                      chunk_partials);
+            k_loads_chunks<double><<<grid, LOAD_THREADS, lut, stream>>>(g, reinterpret_cast<const double*>(imb),
+                                                                        chunk_partials);
         else
-            k_loads_chunks<float><<<grid, LOAD_THREADS, 0, stream>>>(g, reinterpret_cast<const float*>(imb),
-                                                                     chunk_partials);
+            k_loads_chunks<float><<<grid, LOAD_THREADS, lut, stream>>>(g, reinterpret_cast<const float*>(imb),
+                                                                       chunk_partials);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -84,7 +84,9 @@ __device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool mov
     }
 }
 
-template <int STORE, bool MOVING, int CPT>
+// RED: PSC_STEP_REDUCE as a compile-time switch, so launches without
+// reductions carry no loop-carried FP64 accumulators.
+template <int STORE, bool MOVING, int CPT, bool RED>
 __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __restrict__ wins, int nwin,
                                                              int64_t total_tiles, unsigned flags) {
     using TR = StoreTraits<STORE>;
@@ -96,7 +98,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
     const bool do_collide = flags & PSC_STEP_COLLIDE;
     const bool do_imb = do_collide && (flags & PSC_STEP_IMB);
     const bool do_mom = flags & PSC_STEP_MOMENTS;
-    const bool do_red = flags & PSC_STEP_REDUCE;
+    constexpr bool do_red = RED;
     const int64_t t0 = (total_tiles * (int64_t)blockIdx.x) / gridDim.x;
     const int64_t t1 = (total_tiles * ((int64_t)blockIdx.x + 1)) / gridDim.x;
     int64_t win_end = -1;
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __
         flush_segment<PSC_NRED>(red, sw.partials, sw.tile_begin, sw.tile_end - sw.tile_begin, total_tiles, gridDim.x);
 }
 
-template <int STORE, bool MOVING, int CPT>
+template <int STORE, bool MOVING, int CPT, bool RED>
 static cudaError_t launch_fast_t(const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,
                                  int grid_ctas, cudaStream_t stream) {
     if (grid_ctas <= 0) {
@@ -261,7 +263,7 @@ static cudaError_t launch_fast_t(const psc_window* d_windows, int nwin, int64_t 
         cudaGetDevice(&dev);
         int& occ = per_sm[dev & 7];
         if (occ == 0) {
-            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_fast<STORE, MOVING, CPT>,
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_fast<STORE, MOVING, CPT, RED>,
                                                                           STEP_THREADS, 0);
             if (e != cudaSuccess) return e;
             if (occ <= 0) occ = 1;
@@ -271,22 +273,29 @@ static cudaError_t launch_fast_t(const psc_window* d_windows, int nwin, int64_t 
     }
     if ((int64_t)grid_ctas > total_tiles) grid_ctas = (int)total_tiles;  // every CTA owns >= 1 tile
     if (grid_ctas <= 0) return cudaSuccess;
-    k_step_fast<STORE, MOVING, CPT><<<grid_ctas, STEP_THREADS, 0, stream>>>(d_windows, nwin, total_tiles, flags);
+    k_step_fast<STORE, MOVING, CPT, RED><<<grid_ctas, STEP_THREADS, 0, stream>>>(d_windows, nwin, total_tiles, flags);
     return cudaGetLastError();
+}
+
+template <int STORE, bool RED>
+static cudaError_t launch_fast_r(const psc_window* d, int nwin, int64_t tiles, unsigned flags, bool moving, int cpt,
+                                 int grid, cudaStream_t s) {
+    switch (cpt) {
+        case 1: return moving ? launch_fast_t<STORE, true, 1, RED>(d, nwin, tiles, flags, grid, s)
+                              : launch_fast_t<STORE, false, 1, RED>(d, nwin, tiles, flags, grid, s);
+        case 2: return moving ? launch_fast_t<STORE, true, 2, RED>(d, nwin, tiles, flags, grid, s)
+                              : launch_fast_t<STORE, false, 2, RED>(d, nwin, tiles, flags, grid, s);
+        case 4: return moving ? launch_fast_t<STORE, true, 4, RED>(d, nwin, tiles, flags, grid, s)
+                              : launch_fast_t<STORE, false, 4, RED>(d, nwin, tiles, flags, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <int STORE>
 static cudaError_t launch_fast_s(const psc_window* d, int nwin, int64_t tiles, unsigned flags, bool moving, int cpt,
                                  int grid, cudaStream_t s) {
-    switch (cpt) {
-        case 1: return moving ? launch_fast_t<STORE, true, 1>(d, nwin, tiles, flags, grid, s)
-                              : launch_fast_t<STORE, false, 1>(d, nwin, tiles, flags, grid, s);
-        case 2: return moving ? launch_fast_t<STORE, true, 2>(d, nwin, tiles, flags, grid, s)
-                              : launch_fast_t<STORE, false, 2>(d, nwin, tiles, flags, grid, s);
-        case 4: return moving ? launch_fast_t<STORE, true, 4>(d, nwin, tiles, flags, grid, s)
-                              : launch_fast_t<STORE, false, 4>(d, nwin, tiles, flags, grid, s);
-        default: return cudaErrorInvalidValue;
-    }
+    return (flags & PSC_STEP_REDUCE) ? launch_fast_r<STORE, true>(d, nwin, tiles, flags, moving, cpt, grid, s)
+                                     : launch_fast_r<STORE, false>(d, nwin, tiles, flags, moving, cpt, grid, s);
 }
 
 cudaError_t launch_step_fast(int store, const psc_window* d_windows, int nwin, int64_t total_tiles, unsigned flags,

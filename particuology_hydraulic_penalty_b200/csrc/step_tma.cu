@@ -109,7 +109,7 @@ __device__ __forceinline__ void row_tile(const psc_window& W, int64_t t, uint32_
     rows = min(ty, (uint32_t)W.ny - y0);
 }
 
-template <int STORE, bool MOVING, int STAGES>
+template <int STORE, bool MOVING, int STAGES, bool RED>
 __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* __restrict__ wins, int nwin,
                                                            int64_t total_tiles, unsigned flags, uint32_t stage_bytes) {
     using TR = StoreTraits<STORE>;
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
     const bool do_collide = flags & PSC_STEP_COLLIDE;
     const bool do_imb = do_collide && (flags & PSC_STEP_IMB);
     const bool do_mom = flags & PSC_STEP_MOMENTS;
-    const bool do_red = flags & PSC_STEP_REDUCE;
+    constexpr bool do_red = RED;
     int64_t win_end = -1;
     uint32_t k = 0;
     bool aborted = false;  // after a stuck wait: keep joining the barriers, skip the work
@@ -393,11 +393,11 @@ __global__ void __launch_bounds__(TMA_THREADS, 2) k_step_tma(const psc_window* _
         flush_segment<PSC_NRED>(red, sw.partials, sw.tile_begin, sw.tile_end - sw.tile_begin, total_tiles, gridDim.x);
 }
 
-template <int STORE, bool MOVING, int STAGES>
+template <int STORE, bool MOVING, int STAGES, bool RED>
 static cudaError_t launch_tma_t(const psc_window* d, int nwin, int64_t tiles, unsigned flags, int grid,
                                 uint32_t stage_bytes, cudaStream_t s) {
     const size_t smem = (size_t)STAGES * stage_bytes;
-    auto kern = k_step_tma<STORE, MOVING, STAGES>;
+    auto kern = k_step_tma<STORE, MOVING, STAGES, RED>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (grid <= 0) {
@@ -414,15 +414,22 @@ static cudaError_t launch_tma_t(const psc_window* d, int nwin, int64_t tiles, un
     return cudaGetLastError();
 }
 
+template <int STORE, bool MOVING, bool RED>
+static cudaError_t launch_tma_r(const psc_window* d, int nwin, int64_t tiles, unsigned flags, int grid, int stages,
+                                uint32_t stage_bytes, cudaStream_t s) {
+    switch (stages) {
+        case 2: return launch_tma_t<STORE, MOVING, 2, RED>(d, nwin, tiles, flags, grid, stage_bytes, s);
+        case 3: return launch_tma_t<STORE, MOVING, 3, RED>(d, nwin, tiles, flags, grid, stage_bytes, s);
+        case 4: return launch_tma_t<STORE, MOVING, 4, RED>(d, nwin, tiles, flags, grid, stage_bytes, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 template <int STORE, bool MOVING>
 static cudaError_t launch_tma_m(const psc_window* d, int nwin, int64_t tiles, unsigned flags, int grid, int stages,
                                 uint32_t stage_bytes, cudaStream_t s) {
-    switch (stages) {
-        case 2: return launch_tma_t<STORE, MOVING, 2>(d, nwin, tiles, flags, grid, stage_bytes, s);
-        case 3: return launch_tma_t<STORE, MOVING, 3>(d, nwin, tiles, flags, grid, stage_bytes, s);
-        case 4: return launch_tma_t<STORE, MOVING, 4>(d, nwin, tiles, flags, grid, stage_bytes, s);
-        default: return cudaErrorInvalidValue;
-    }
+    return (flags & PSC_STEP_REDUCE) ? launch_tma_r<STORE, MOVING, true>(d, nwin, tiles, flags, grid, stages, stage_bytes, s)
+                                     : launch_tma_r<STORE, MOVING, false>(d, nwin, tiles, flags, grid, stages, stage_bytes, s);
 }
 
 template <int STORE>
