@@ -341,12 +341,18 @@ constexpr int LOAD_THREADS = 256;
 // The block's table of inside / S^3 for every sample count (S <= 16) holds
 // the exact IEEE quotients of psc3d.py:88, computed once per block.
 constexpr int LOAD_UNROLL = 4;
+// Resident blocks per SM the register allocation of k_loads_chunks aims for
+// (the kernel is latency-bound: more resident warps, more loads in flight).
+#ifndef PSC_LOADS_MIN_BLOCKS
+#define PSC_LOADS_MIN_BLOCKS 3
+#endif
 
 // One block per chunk of one particle's bbox entries.  A thread visits the
 // entries e0 + tid, e0 + tid + 256, ...; their bbox coordinates advance by a
 // fixed mixed-radix stride with carries (one 32-bit division per chunk).
 template <typename I>
-__global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, const I* imb, double* part) {
+__global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_chunks(psc_geometry g, const I* imb,
+                                                                                 double* part) {
     __shared__ double s[LOAD_THREADS / 32][6];
     extern __shared__ double s_al[];  // S^3 + 1 entries (dynamic)
     const int64_t C = g.totals[1];
@@ -378,16 +384,28 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, c
             const uint32_t step_b = step_q % ey;
             const uint32_t step_a = step_q / ey;
             const double qx = q[0], qy = q[1], qz = q[2];
-            // LOAD_UNROLL entries per pass: their loads are issued together, then
-            // accumulated in entry order (the order of a one-entry loop)
+            // LOAD_UNROLL entries per pass: all their loads are issued together,
+            // then accumulated in entry order (the order of a one-entry loop)
             const uint32_t bx = (uint32_t)bb[0], by = (uint32_t)bb[1], bz = (uint32_t)bb[2];
             for (int64_t e = e0 + threadIdx.x; e < e1; e += (int64_t)LOAD_UNROLL * blockDim.x) {
                 uint16_t cnt[LOAD_UNROLL];
                 uint32_t cx[LOAD_UNROLL], cy[LOAD_UNROLL], cz[LOAD_UNROLL];
+                double as[LOAD_UNROLL];
+                I mx[LOAD_UNROLL], my[LOAD_UNROLL], mz[LOAD_UNROLL];  // the field's own type until used
 #pragma unroll
                 for (int u = 0; u < LOAD_UNROLL; ++u) {
                     const int64_t eu = e + (int64_t)u * blockDim.x;
-                    cnt[u] = eu < e1 ? g.ent_cnt[eu] : (uint16_t)0;
+                    cnt[u] = 0;
+                    if (eu < e1) {
+                        // every load of the entry at once (the cell lies in the clipped box, so
+                        // it exists even where the count is 0): one memory round trip per pass
+                        const uint32_t cell = ((bx + a) * ny + (by + b)) * nz + (bz + k);
+                        cnt[u] = g.ent_cnt[eu];
+                        as[u] = g.alpha_sum[cell];
+                        mx[u] = imb[cell];
+                        my[u] = imb[(size_t)N + cell];
+                        mz[u] = imb[2 * (size_t)N + cell];
+                    }
                     cx[u] = bx + a;
                     cy[u] = by + b;
                     cz[u] = bz + k;
@@ -400,26 +418,15 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, c
                     b -= cb ? ey : 0u;
                     a += step_a + cb;
                 }
-                double as[LOAD_UNROLL], mx[LOAD_UNROLL], my[LOAD_UNROLL], mz[LOAD_UNROLL];
-#pragma unroll
-                for (int u = 0; u < LOAD_UNROLL; ++u) {
-                    if (cnt[u] != 0) {
-                        const uint32_t cell = (cx[u] * ny + cy[u]) * nz + cz[u];
-                        as[u] = g.alpha_sum[cell];
-                        mx[u] = (double)imb[cell];
-                        my[u] = (double)imb[(size_t)N + cell];
-                        mz[u] = (double)imb[2 * (size_t)N + cell];
-                    }
-                }
 #pragma unroll
                 for (int u = 0; u < LOAD_UNROLL; ++u) {
                     if (cnt[u] == 0) continue;
                     // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
                     const double al = s_al[cnt[u]];
                     const double ow = xdiv(al, as[u] > 1.0e-14 ? as[u] : 1.0e-14);
-                    const double nfx = -xmul(ow, mx[u]);
-                    const double nfy = -xmul(ow, my[u]);
-                    const double nfz = -xmul(ow, mz[u]);
+                    const double nfx = -xmul(ow, (double)mx[u]);
+                    const double nfy = -xmul(ow, (double)my[u]);
+                    const double nfz = -xmul(ow, (double)mz[u]);
                     // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
                     const double rx = xsub(xadd((double)cx[u], 0.5), qx);
                     const double ry = xsub(xadd((double)cy[u], 0.5), qy);
@@ -441,29 +448,45 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks(psc_geometry g, c
     }
 }
 
-// One block: per-particle sums of chunk partials (fixed order), then the
-// closure residual |sum_p F_p + sum_x imb| and the max force / torque norms.
-__global__ void __launch_bounds__(1024) k_loads_final(psc_geometry g, const double* part, const double* imb_sums,
-                                                      double* forces, double* torques, double* diag) {
+// Per-particle sums of the chunk partials: one warp per particle, lane l
+// sums chunks l, l + 32, ... in order, then a fixed shuffle tree.
+__global__ void __launch_bounds__(256) k_loads_particles(psc_geometry g, const double* part, double* forces,
+                                                         double* torques) {
+    const int lane = threadIdx.x & 31;
+    const int p = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+    if (p >= g.nparticles) return;  // warp-uniform
+    double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const int64_t c1 = g.chunk_off[p + 1];
+    for (int64_t c = g.chunk_off[p] + lane; c < c1; c += 32) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) F[k] += part[c * 6 + k];
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) F[k] += __shfl_xor_sync(0xffffffffu, F[k], o);
+    }
+    if (lane < 3) {
+        forces[(size_t)p * 3 + lane] = F[lane];
+        torques[(size_t)p * 3 + lane] = F[3 + lane];
+    }
+}
+
+// One block: the closure residual |sum_p F_p + sum_x imb| and the max force /
+// torque norms (psc3d.py:247-253, :280-281) from the per-particle loads.
+__global__ void __launch_bounds__(1024) k_loads_diag(psc_geometry g, const double* imb_sums, const double* forces,
+                                                     const double* torques, double* diag) {
     __shared__ double s[32][5];
     const int P = g.nparticles;
     double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // sum Fx, Fy, Fz, max |F|^2, max |T|^2
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int64_t c = g.chunk_off[p]; c < g.chunk_off[p + 1]; ++c) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) F[k] += part[c * 6 + k];
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            forces[(size_t)p * 3 + k] = F[k];
-            torques[(size_t)p * 3 + k] = F[3 + k];
-        }
+        const double* F = forces + (size_t)p * 3;
+        const double* T = torques + (size_t)p * 3;
         v[0] += F[0];
         v[1] += F[1];
         v[2] += F[2];
         v[3] = fmax(v[3], F[0] * F[0] + F[1] * F[1] + F[2] * F[2]);
-        v[4] = fmax(v[4], F[3] * F[3] + F[4] * F[4] + F[5] * F[5]);
+        v[4] = fmax(v[4], T[0] * T[0] + T[1] * T[1] + T[2] * T[2]);
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
@@ -625,7 +648,12 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    k_loads_final<<<1, 1024, 0, stream>>>(g, chunk_partials, imb_sums, forces, torques, diag);
+    if (g.nparticles > 0) {
+        k_loads_particles<<<(g.nparticles + 7) / 8, 256, 0, stream>>>(g, chunk_partials, forces, torques);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    k_loads_diag<<<1, 1024, 0, stream>>>(g, imb_sums, forces, torques, diag);
     return cudaGetLastError();
 }
 

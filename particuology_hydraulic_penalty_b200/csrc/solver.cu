@@ -37,7 +37,7 @@ namespace {
     } while (0)
 
 constexpr int kQ = 19;
-constexpr int kChunkEntries = 1024;  // bbox entries per load-reduction chunk (4 per thread)
+constexpr int kChunkEntries = 4096;  // bbox entries per load-reduction chunk
 constexpr int kOutLen = 2 * PSC_NRED + PSC_NDIAG;  // [red_pre][red_post][diag]
 
 // Owned device array (contents are not kept when it grows).

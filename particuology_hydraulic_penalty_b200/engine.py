@@ -128,7 +128,7 @@ class DeviceGeometry:
     device-to-host read of the entry total per rebuild.
     """
 
-    CHUNK_ENTRIES = 1024  # bbox entries per load-reduction chunk (4 per thread of a 256-thread block)
+    CHUNK_ENTRIES = 4096
 
     def __init__(self, shape, subsamples: int, device, want_level: bool, smooth_eps: float = 0.0):
         self.smooth_eps = float(smooth_eps)
