@@ -134,6 +134,38 @@ __device__ __forceinline__ int owner_of(const int64_t* off, int P, int64_t e) {
     return lo;
 }
 
+// owner_of for a whole block (block-uniform call): the largest p < P with
+// off[p] <= e, found by counting instead of a serial binary search -- the
+// owner is (number of p with off[p] <= e) - 1 because off is non-decreasing.
+// Ranges wider than 4 x blockDim are first narrowed by one sampled round.
+__device__ __forceinline__ int block_owner_of(const int64_t* off, int P, int64_t e) {
+    int lo = 0, hi = P;  // invariant: off[lo] <= e and (hi == P or off[hi] > e)
+    const int bd = (int)blockDim.x, tid = (int)threadIdx.x;
+    while (hi - lo > 1) {
+        const int len = hi - lo;
+        if (len <= 4 * bd) {
+            bool f[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int p = lo + tid + k * bd;
+                f[k] = p < hi && off[p] <= e;
+            }
+            int n = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) n += __syncthreads_count(f[k]);
+            return lo + n - 1;
+        }
+        const int p = lo + (int)(((int64_t)tid * len) / bd);
+        const int n = __syncthreads_count(off[p] <= e);  // >= 1: sample 0 is lo
+        const int i = n - 1;
+        const int nlo = lo + (int)(((int64_t)i * len) / bd);
+        const int nhi = i + 1 < bd ? lo + (int)(((int64_t)(i + 1) * len) / bd) : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    return lo;
+}
+
 struct EntryCell {
     int p;
     int32_t ix, iy, iz;
@@ -362,8 +394,8 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
     const double S3d = (double)S3;
     for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
     __syncthreads();
-    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {
-        const int p = owner_of(g.chunk_off, g.nparticles, chunk);
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
+        const int p = block_owner_of(g.chunk_off, g.nparticles, chunk);
         const int64_t eb = g.ent_off[p];
         const int64_t e0 = eb + (chunk - g.chunk_off[p]) * g.chunk_entries;
         const int64_t e1 = min(e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
