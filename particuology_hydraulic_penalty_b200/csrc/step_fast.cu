@@ -86,8 +86,9 @@ __device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool mov
 
 // RED: PSC_STEP_REDUCE as a compile-time switch, so launches without
 // reductions carry no loop-carried FP64 accumulators.
+// FP64 arithmetic needs about twice the registers: keep two CTAs resident.
 template <int STORE, bool MOVING, int CPT, bool RED>
-__global__ void __launch_bounds__(STEP_THREADS) k_step_fast(const psc_window* __restrict__ wins, int nwin,
+__global__ void __launch_bounds__(STEP_THREADS, STORE == PSC_STORE_F64 ? 2 : 1) k_step_fast(const psc_window* __restrict__ wins, int nwin,
                                                              int64_t total_tiles, unsigned flags) {
     using TR = StoreTraits<STORE>;
     using T = typename TR::T;
