@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define PSC_ABI_VERSION 2
+#define PSC_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------- */
 #define PSC_OK 0
@@ -82,6 +82,16 @@ typedef struct psc_launch {
 /* ---- per-window flags --------------------------------------------------- */
 #define PSC_WIN_MOVING 1   /* read the solid velocity field us (else u_s = 0) */
 #define PSC_WIN_INACTIVE 2 /* skip the window's tiles: state frozen (e.g. converged); no partials written */
+/* Open along x (no counterpart in the reference, which is periodic in every
+ * direction, psc3d.py:239-242).  Velocity inlet at x = 0 by moving-wall
+ * bounce-back: a population entering from outside (c_x = +1) is the node's
+ * own post-collision population of the opposite direction plus
+ * 2 w_i inlet_rho (c_i . inlet_u) / cs^2 (mass flux inlet_rho * inlet_u per
+ * unit face area).  Zero-gradient outflow at x = nx - 1: a population
+ * entering from outside (c_x = -1) is the post-collision value of the plane
+ * x = nx - 1 itself.  y and z stay periodic.  Honoured by the exact and the
+ * direct kernels; psc_plan_row_tiles rejects such windows. */
+#define PSC_WIN_OPEN_X 4
 
 /* Reduction slots written per tile with PSC_STEP_REDUCE and summed per window
  * by psc_reduce_windows().  Velocities are the stored-moment velocities
@@ -141,6 +151,8 @@ typedef struct psc_window {
     double* partials;      /* [1 + tile_count * PSC_PARTIAL_ROWS][PSC_NRED] (header row first) */
     double tau_minus;      /* TRT: antisymmetric relaxation time (0 = BGK, the reference's collision);
                               deviation storage modes only */
+    double inlet_rho;      /* PSC_WIN_OPEN_X: inlet density */
+    double inlet_u[3];     /* PSC_WIN_OPEN_X: inlet velocity */
 } psc_window;
 
 /* Particle-derived geometry of ONE window (device arrays, caller-owned).
@@ -321,7 +333,13 @@ int psc_adjoint_geometry_grad(const psc_geometry* h_geo, const psc_adjoint_args*
  * populations for every storage mode. */
 int psc_stream_push(int store, double store_scale, const void* src, double* dst, int nx, int ny, int nz,
                     void* stream);
-/* Inverse: absolute FP64 post-stream f -> stored representation. */
+/* psc_stream_push for a PSC_WIN_OPEN_X window (bounce-back velocity inlet of
+ * (inlet_rho, h_inlet_u[3]) at x = 0, zero-gradient outflow at x = nx - 1;
+ * no counterpart in the reference). */
+int psc_stream_push_open(int store, double store_scale, const void* src, double* dst, int nx, int ny, int nz,
+                         double inlet_rho, const double* h_inlet_u, void* stream);
+/* Inverse: absolute FP64 post-stream f -> stored representation (also for
+ * open windows: the entries it cannot recover are never read by a step). */
 int psc_stream_pull_store(int store, double store_scale, const double* src, void* dst, int nx, int ny, int nz,
                           void* stream);
 
@@ -348,6 +366,11 @@ typedef struct psc_config {
     double store_scale;       /* PSC_STORE_F16 / BF16 stored-deviation scale; 0 = the mode's default */
     double conv_tol;          /* PSC_RUN_CONVERGE tolerance; 0 = 1e-8 (couple_psc_liggghts.py:168) */
     void* stream;             /* cudaStream_t for all work of the handle; NULL = a stream of its own */
+    int32_t open_x;           /* 1: velocity inlet at x = 0, zero-gradient outflow at x = nx - 1
+                                 (PSC_WIN_OPEN_X; not in the reference); 0: periodic */
+    int32_t reserved;         /* 0 */
+    double inlet_rho;         /* open_x: inlet density */
+    double inlet_u[3];        /* open_x: inlet velocity */
 } psc_config;
 
 /* Diagnostics of one step.  The first five are the reference's dictionary

@@ -286,6 +286,32 @@ def stream_push(f: np.ndarray) -> np.ndarray:
     return out
 
 
+def inlet_correction(i: int, inlet_rho: float, inlet_u) -> float:
+    """Moving-wall bounce-back term 2 w_i rho_in (c_i . u_in) / cs^2 of the velocity inlet."""
+    cx, cy, cz = (int(v) for v in C[i])
+    cu = cx * np.float64(inlet_u[0]) + cy * np.float64(inlet_u[1]) + cz * np.float64(inlet_u[2])
+    return 2.0 * (W[i] * np.float64(inlet_rho)) * cu / CS2
+
+
+def stream_push_open_x(f: np.ndarray, inlet_rho: float, inlet_u) -> np.ndarray:
+    """Push streaming open along x (an extension: the reference is periodic in
+    every direction, psc3d.py:239-242).  Velocity inlet at x = 0 by moving-wall
+    bounce-back (Ladd 1994): a population entering from outside (c_x = +1) is
+    the node's own post-collision population of the opposite direction plus
+    2 w_i rho_in (c_i . u_in) / cs^2, which injects exactly rho_in u_in per unit
+    face area.  Zero-gradient outflow at x = nx - 1: a population entering from
+    outside (c_x = -1) is the post-collision value of the plane x = nx - 1
+    itself, shifted in y and z like any other.  y and z stay periodic."""
+    out = stream_push(f)
+    for i in range(Q):
+        cx, cy, cz = (int(v) for v in C[i])
+        if cx == 1:
+            out[i, 0] = f[OPP[i], 0] + inlet_correction(i, inlet_rho, inlet_u)
+        elif cx == -1:
+            out[i, -1] = np.roll(f[i, -1], shift=(cy, cz), axis=(0, 1))
+    return out
+
+
 def unstream_pull(f: np.ndarray) -> np.ndarray:
     """Inverse of :func:`stream_push`."""
     out = np.empty_like(f)
@@ -350,8 +376,11 @@ class OracleSolver:
     """
 
     def __init__(self, n, particles, tau=0.72, subsamples=4, body_force_z=0.0,
-                 static_geometry=False, force=None):
+                 static_geometry=False, force=None, inlet=None):
         self.n = int(n)
+        # inlet = (rho_in, (ux, uy, uz)): open along x (stream_push_open_x), an
+        # extension beyond the reference; None: periodic, the reference
+        self.inlet = inlet
         self.particles = particles
         self.tau = float(tau)
         self.subsamples = int(subsamples)
@@ -383,7 +412,7 @@ class OracleSolver:
         post, self.imb = collide(self.f, self.solid, us, self.tau, self.force)
         self.hydro_forces, self.hydro_torques, self.momentum_residual = particle_loads(
             self.particles, self.geo, self.imb)
-        self.f = stream_push(post)
+        self.f = stream_push(post) if self.inlet is None else stream_push_open_x(post, *self.inlet)
         self.rho, self.ux, self.uy, self.uz = moments(self.f, self.force)
         hf, ht = self.hydro_forces, self.hydro_torques
         return {

@@ -14,7 +14,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libpscb200.so"
 HEADER_PATH = Path(__file__).resolve().parents[1] / "include" / "psc_b200.h"
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # status codes
 PSC_OK = 0
@@ -39,6 +39,7 @@ STEP_MOVING = 16
 
 WIN_MOVING = 1
 WIN_INACTIVE = 2
+WIN_OPEN_X = 4  # velocity inlet at x = 0, zero-gradient outflow at x = nx - 1
 
 # reduction slots
 RED_RHO, RED_UX, RED_UY, RED_UZ = 0, 1, 2, 3
@@ -77,7 +78,7 @@ class PscWindow(ctypes.Structure):
         ("tau", c_double), ("force", c_double * 3), ("store_scale", c_double),
         ("f_src", c_void_p), ("f_dst", c_void_p), ("solid", c_void_p), ("level", c_void_p),
         ("us", c_void_p), ("imb", c_void_p), ("moments", c_void_p), ("partials", c_void_p),
-        ("tau_minus", c_double),
+        ("tau_minus", c_double), ("inlet_rho", c_double), ("inlet_u", c_double * 3),
     ]
 
 
@@ -116,7 +117,8 @@ class PscConfig(ctypes.Structure):
         ("nx", c_int32), ("ny", c_int32), ("nz", c_int32), ("subsamples", c_int32), ("store", c_int32),
         ("static_geometry", c_int32), ("device", c_int32), ("conv_min_steps", c_int32),
         ("tau", c_double), ("tau_minus", c_double), ("force", c_double * 3), ("store_scale", c_double),
-        ("conv_tol", c_double), ("stream", c_void_p),
+        ("conv_tol", c_double), ("stream", c_void_p), ("open_x", c_int32), ("reserved", c_int32),
+        ("inlet_rho", c_double), ("inlet_u", c_double * 3),
     ]
 
 
@@ -174,6 +176,8 @@ SIGNATURES = {
                                     c_double, c_uint, c_void_p, c_void_p]),
     "psc_stream_push": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "psc_stream_pull_store": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "psc_stream_push_open": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_double,
+                                     POINTER(c_double), c_void_p]),
     # handle layer
     "psc_create": (c_int, [POINTER(PscConfig), POINTER(c_void_p)]),
     "psc_destroy": (c_int, [c_void_p]),

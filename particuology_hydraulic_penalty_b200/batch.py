@@ -36,6 +36,7 @@ class WindowSpec:
     subsamples: int = 4
     name: str = ""
     collision: str = "bgk"  # "bgk" (the reference) or "trt" (magic parameter 3/16)
+    inlet: tuple | None = None  # (rho_in, (ux, uy, uz)): velocity inlet at x = 0, outflow at x = nx - 1
 
 
 class PscBatch:
@@ -91,7 +92,7 @@ class PscBatch:
                     raise ValueError("collision must be 'bgk' or 'trt'")
                 tm = trt_tau_minus(s.tau) if s.collision == "trt" else 0.0
                 win = LatticeWindow(shape, s.tau, s.force, s.subsamples, self.store, store_scale, self.device,
-                                    tau_minus=tm)
+                                    tau_minus=tm, inlet=getattr(s, "inlet", None))
                 geo = DeviceGeometry(shape, s.subsamples, self.device, want_level=self.store != nat.STORE_F64_EXACT)
                 geo.set_particles(particles_array(s.particles))
                 geo.rebuild()

@@ -115,6 +115,9 @@ int psc_plan_row_tiles(psc_window* h_windows, int nwin, int rows, int elem_bytes
         psc_window& W = h_windows[w];
         int st = check_extent(W.nx, W.ny, W.nz, "psc_plan_row_tiles");
         if (st) return st;
+        if (W.flags & PSC_WIN_OPEN_X)
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: the TMA kernel runs periodic windows only (window " +
+                                               std::to_string(w) + " has PSC_WIN_OPEN_X)");
         const int64_t n = (int64_t)W.nx * W.ny * W.nz;
         if (n * 19 >= (1ll << 31))
             return fail(PSC_E_UNSUPPORTED, "psc_plan_row_tiles: a window must hold fewer than 2^31/19 cells");
@@ -358,6 +361,18 @@ int psc_stream_push(int store, double store_scale, const void* src, double* dst,
     if (store_scale == 0.0) return fail(PSC_E_INVALID, "psc_stream_push: zero store_scale");
     cudaError_t e = launch_stream_push(store, store_scale, src, dst, nx, ny, nz, as_stream(stream));
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_stream_push");
+}
+
+int psc_stream_push_open(int store, double store_scale, const void* src, double* dst, int nx, int ny, int nz,
+                         double inlet_rho, const double* h_inlet_u, void* stream) {
+    if (!valid_store(store) || !src || !dst || !h_inlet_u)
+        return fail(PSC_E_INVALID, "psc_stream_push_open: bad arguments");
+    int st = check_extent(nx, ny, nz, "psc_stream_push_open");
+    if (st) return st;
+    if (store_scale == 0.0) return fail(PSC_E_INVALID, "psc_stream_push_open: zero store_scale");
+    const double inlet[4] = {inlet_rho, h_inlet_u[0], h_inlet_u[1], h_inlet_u[2]};
+    cudaError_t e = launch_stream_push(store, store_scale, src, dst, nx, ny, nz, as_stream(stream), true, inlet);
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_stream_push_open");
 }
 
 int psc_stream_pull_store(int store, double store_scale, const double* src, void* dst, int nx, int ny, int nz,

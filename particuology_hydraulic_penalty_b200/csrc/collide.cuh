@@ -45,6 +45,18 @@ PSC_HD ExactMoments moments_exact(const double* f, double hfx, double hfy, doubl
 
 PSC_HD double cm(int c, double x) { return c == 0 ? 0.0 : (c > 0 ? x : -x); }
 
+// Velocity inlet by moving-wall bounce-back (Ladd 1994): the population i
+// entering x = 0 from outside is the node's post-collision population opp(i)
+// plus 2 w_i rho_in (c_i . u_in) / cs^2, which injects rho_in u_in per unit
+// face area.  This is that term, in the operation order of the oracle.
+PSC_HD double inlet_correction_exact(int i, double r, double x, double y, double z) {
+    const double cu = xadd(xadd(cm(cxv(i), x), cm(cyv(i), y)), cm(czv(i), z));
+    return xdiv(xmul(xmul(2.0, xmul(wgt(i), r)), cu), CS2);
+}
+
+// The directions entering x = 0 from outside (c_x = +1).
+PSC_HD constexpr bool enters_x0(int i) { return i == 1 || i == 7 || i == 9 || i == 11 || i == 13; }
+
 // Collide f in place.  solid: clipped solid fraction.  moving: use (usx, usy,
 // usz), else the solid velocity is zero.  imb receives sum_i c_i B Omega_s,i in
 // the reference's sequential order (psc3d.py:234-236).

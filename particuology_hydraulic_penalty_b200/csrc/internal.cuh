@@ -34,8 +34,9 @@ cudaError_t launch_step_tma(int store, const psc_window* d_windows, int nwin, in
 cudaError_t read_device_status(int* out, bool clear);
 cudaError_t launch_reduce_windows(const psc_window* d_windows, int nwin, double* out, cudaStream_t stream);
 cudaError_t launch_init_equilibrium(int store, double scale, void* f, int64_t ncells, cudaStream_t stream);
+// inlet = {rho, ux, uy, uz} when open_x (PSC_WIN_OPEN_X faces), else unused
 cudaError_t launch_stream_push(int store, double scale, const void* src, double* dst, int nx, int ny, int nz,
-                               cudaStream_t stream);
+                               cudaStream_t stream, bool open_x = false, const double* inlet = nullptr);
 cudaError_t launch_stream_pull_store(int store, double scale, const double* src, void* dst, int nx, int ny, int nz,
                                      cudaStream_t stream);
 

@@ -143,6 +143,9 @@ int check_config(const psc_config& c, const char* who) {
         return fail(PSC_E_INVALID, w + ": store_scale must be >= 0 (0 = default)");
     if (!(std::isfinite(c.conv_tol) && c.conv_tol >= 0.0)) return fail(PSC_E_INVALID, w + ": conv_tol must be >= 0");
     if (c.device < 0) return fail(PSC_E_INVALID, w + ": negative device ordinal");
+    if (c.open_x != 0 && c.open_x != 1) return fail(PSC_E_INVALID, w + ": open_x must be 0 or 1");
+    if (c.open_x && !(std::isfinite(c.inlet_rho) && c.inlet_rho > 0.0 && finite3(c.inlet_u)))
+        return fail(PSC_E_INVALID, w + ": open_x needs a positive inlet_rho and a finite inlet_u");
     return PSC_OK;
 }
 
@@ -237,7 +240,7 @@ struct Window {
         d.ny = cfg.ny;
         d.nz = cfg.nz;
         d.subsamples = cfg.subsamples;
-        d.flags = moving ? PSC_WIN_MOVING : 0;
+        d.flags = (moving ? PSC_WIN_MOVING : 0) | (cfg.open_x ? PSC_WIN_OPEN_X : 0);
         d.tau = cfg.tau;
         d.force[0] = cfg.force[0];
         d.force[1] = cfg.force[1];
@@ -252,6 +255,10 @@ struct Window {
         d.moments = moments.p;
         d.partials = partials.p;
         d.tau_minus = cfg.tau_minus;
+        d.inlet_rho = cfg.open_x ? cfg.inlet_rho : 1.0;
+        d.inlet_u[0] = cfg.open_x ? cfg.inlet_u[0] : 0.0;
+        d.inlet_u[1] = cfg.open_x ? cfg.inlet_u[1] : 0.0;
+        d.inlet_u[2] = cfg.open_x ? cfg.inlet_u[2] : 0.0;
         return d;
     }
 };
@@ -539,7 +546,10 @@ int window_get_field(Window& w, int which, double* dst, cudaStream_t s, HArray<i
         case PSC_FIELD_F: {
             double* tmp = nullptr;
             PSC_CUDA(cudaMalloc(reinterpret_cast<void**>(&tmp), (size_t)kQ * N * 8), who);
-            int st = psc_stream_push(w.cfg.store, w.scale, w.f[w.cur].p, tmp, w.cfg.nx, w.cfg.ny, w.cfg.nz, s);
+            int st = w.cfg.open_x ? psc_stream_push_open(w.cfg.store, w.scale, w.f[w.cur].p, tmp, w.cfg.nx, w.cfg.ny,
+                                                         w.cfg.nz, w.cfg.inlet_rho, w.cfg.inlet_u, s)
+                                  : psc_stream_push(w.cfg.store, w.scale, w.f[w.cur].p, tmp, w.cfg.nx, w.cfg.ny,
+                                                    w.cfg.nz, s);
             cudaError_t e = cudaSuccess;
             if (st == PSC_OK) e = cudaMemcpyAsync(dst, tmp, (size_t)kQ * N * 8, cudaMemcpyDeviceToHost, s);
             if (st == PSC_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1039,7 +1049,7 @@ int batch_freeze(psc_batch& b, int k, const double* row) {
     std::memcpy(b.frozen_red.data() + (size_t)k * PSC_NRED, row, PSC_NRED * sizeof(double));
     // set the flag in both device tables in place: captured graphs stay valid
     const size_t off = (size_t)k * sizeof(psc_window) + offsetof(psc_window, flags);
-    int32_t flags = b.w[(size_t)k]->moving ? PSC_WIN_MOVING : 0;
+    int32_t flags = (b.w[(size_t)k]->moving ? PSC_WIN_MOVING : 0) | (b.w[(size_t)k]->cfg.open_x ? PSC_WIN_OPEN_X : 0);
     flags |= PSC_WIN_INACTIVE;
     for (int p = 0; p < 2; ++p)
         PSC_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(b.table[p].p) + off, &flags, sizeof(flags),

@@ -57,11 +57,24 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restr
             const uint32_t rr = cell / (uint32_t)nz;
             const uint32_t iy = rr % (uint32_t)ny;
             const uint32_t ix = rr / (uint32_t)ny;
-            const NbrOffsets nb = nbr_offsets(ix, iy, iz, nx, ny, nz);
+            const bool open_x = (W.flags & PSC_WIN_OPEN_X) != 0;
+            const NbrOffsets nb = nbr_offsets(ix, iy, iz, nx, ny, nz, open_x);
             const bool moving = MOVING && (W.flags & PSC_WIN_MOVING) && W.us != nullptr;
             R f[Q];
             const R scale = TR::scaled ? (R)W.store_scale : R(1);
             PullLoop<T, R, Q>::run(f, reinterpret_cast<const T*>(W.f_src), N, cell, nb, R(1) / scale, TR::scaled);
+            if (open_x && ix == 0) {  // velocity inlet: bounce-back of the node's own opp(i) + momentum term
+                const T* srcT = reinterpret_cast<const T*>(W.f_src);
+#pragma unroll
+                for (int i = 0; i < Q; ++i) {
+                    if (!enters_x0(i)) continue;
+                    const R back = ld_pop(srcT + (size_t)opp(i) * N + cell);
+                    const double corr =
+                        inlet_correction_exact(i, W.inlet_rho, W.inlet_u[0], W.inlet_u[1], W.inlet_u[2]);
+                    if constexpr (TR::exact) f[i] = xadd((double)back, corr);
+                    else f[i] = (TR::scaled ? back / scale : back) + (R)corr;
+                }
+            }
             O* mom = reinterpret_cast<O*>(W.moments);
             O* imbp = reinterpret_cast<O*>(W.imb);
             const O* usp = reinterpret_cast<const O*>(W.us);
@@ -254,16 +267,19 @@ __device__ __forceinline__ double to_abs(T v, int i, bool exact, bool scaled, do
     return d + wgt(i);
 }
 
-// dst_i(x) = src_i(x - c_i) in absolute FP64 (the reference's post-stream f).
+// dst_i(x) = src_i(x - c_i) in absolute FP64 (the reference's post-stream f);
+// with open_x the x faces follow PSC_WIN_OPEN_X (bounce-back velocity inlet
+// at x = 0, zero-gradient outflow at x = nx - 1).
 template <int STORE>
-__global__ void k_stream_push(const void* src, double* dst, int nx, int ny, int nz, double scale) {
+__global__ void k_stream_push(const void* src, double* dst, int nx, int ny, int nz, double scale, bool open_x,
+                              double in_rho, double in_ux, double in_uy, double in_uz) {
     using TR = StoreTraits<STORE>;
     using T = typename TR::T;
     const uint32_t N = (uint32_t)nx * ny * nz;
     const T* s = reinterpret_cast<const T*>(src);
     for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < N; cell += gridDim.x * blockDim.x) {
         const uint32_t iz = cell % nz, rr = cell / nz, iy = rr % ny, ix = rr / ny;
-        const NbrOffsets nb = nbr_offsets(ix, iy, iz, nx, ny, nz);
+        const NbrOffsets nb = nbr_offsets(ix, iy, iz, nx, ny, nz, open_x);
         int32_t off[Q];
         off[0] = 0;
         off[1] = pull_offset<1>(nb); off[2] = pull_offset<2>(nb); off[3] = pull_offset<3>(nb);
@@ -275,7 +291,12 @@ __global__ void k_stream_push(const void* src, double* dst, int nx, int ny, int 
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const T v = s[(size_t)i * N + (size_t)((int64_t)cell + off[i])];
-            dst[(size_t)i * N + cell] = to_abs(v, i, TR::exact, TR::scaled, 1.0 / scale);
+            double a = to_abs(v, i, TR::exact, TR::scaled, 1.0 / scale);
+            if (open_x && ix == 0 && enters_x0(i)) {  // inlet: bounce-back of opp(i) at the node + momentum term
+                const double back = to_abs(s[(size_t)opp(i) * N + cell], opp(i), TR::exact, TR::scaled, 1.0 / scale);
+                a = xadd(back, inlet_correction_exact(i, in_rho, in_ux, in_uy, in_uz));
+            }
+            dst[(size_t)i * N + cell] = a;
         }
     }
 }
@@ -387,16 +408,21 @@ cudaError_t launch_init_equilibrium(int store, double scale, void* f, int64_t nc
 }
 
 cudaError_t launch_stream_push(int store, double scale, const void* src, double* dst, int nx, int ny, int nz,
-                               cudaStream_t stream) {
+                               cudaStream_t stream, bool open_x, const double* inlet) {
     const int g = grid_for((int64_t)nx * ny * nz, 256);
+    const double r = open_x ? inlet[0] : 1.0, ux = open_x ? inlet[1] : 0.0, uy = open_x ? inlet[2] : 0.0,
+                 uz = open_x ? inlet[3] : 0.0;
+#define PSC_PUSH_CASE(S) \
+    case S: k_stream_push<S><<<g, 256, 0, stream>>>(src, dst, nx, ny, nz, scale, open_x, r, ux, uy, uz); break;
     switch (store) {
-        case PSC_STORE_F64_EXACT: k_stream_push<PSC_STORE_F64_EXACT><<<g, 256, 0, stream>>>(src, dst, nx, ny, nz, scale); break;
-        case PSC_STORE_F64: k_stream_push<PSC_STORE_F64><<<g, 256, 0, stream>>>(src, dst, nx, ny, nz, scale); break;
-        case PSC_STORE_F32: k_stream_push<PSC_STORE_F32><<<g, 256, 0, stream>>>(src, dst, nx, ny, nz, scale); break;
-        case PSC_STORE_F16: k_stream_push<PSC_STORE_F16><<<g, 256, 0, stream>>>(src, dst, nx, ny, nz, scale); break;
-        case PSC_STORE_BF16: k_stream_push<PSC_STORE_BF16><<<g, 256, 0, stream>>>(src, dst, nx, ny, nz, scale); break;
+        PSC_PUSH_CASE(PSC_STORE_F64_EXACT)
+        PSC_PUSH_CASE(PSC_STORE_F64)
+        PSC_PUSH_CASE(PSC_STORE_F32)
+        PSC_PUSH_CASE(PSC_STORE_F16)
+        PSC_PUSH_CASE(PSC_STORE_BF16)
         default: return cudaErrorInvalidValue;
     }
+#undef PSC_PUSH_CASE
     return cudaGetLastError();
 }
 

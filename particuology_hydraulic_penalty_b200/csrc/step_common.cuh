@@ -90,11 +90,15 @@ struct NbrOffsets {
     int32_t xm, xp, ym, yp, zm, zp;  // to ix-1, ix+1, iy-1, iy+1, iz-1, iz+1
 };
 
-__device__ __forceinline__ NbrOffsets nbr_offsets(uint32_t ix, uint32_t iy, uint32_t iz, int nx, int ny, int nz) {
+// Offsets to the six face neighbours, periodic; with open_x the x faces
+// point at the cell's own plane instead of wrapping (zero-gradient outflow at
+// x = nx - 1; at x = 0 the inlet replaces the pulled values afterwards).
+__device__ __forceinline__ NbrOffsets nbr_offsets(uint32_t ix, uint32_t iy, uint32_t iz, int nx, int ny, int nz,
+                                                  bool open_x = false) {
     NbrOffsets o;
     const int32_t nyz = ny * nz;
-    o.xm = ix == 0 ? (nx - 1) * nyz : -nyz;
-    o.xp = ix == (uint32_t)(nx - 1) ? -(nx - 1) * nyz : nyz;
+    o.xm = ix == 0 ? (open_x ? 0 : (nx - 1) * nyz) : -nyz;
+    o.xp = ix == (uint32_t)(nx - 1) ? (open_x ? 0 : -(nx - 1) * nyz) : nyz;
     o.ym = iy == 0 ? (ny - 1) * nz : -nz;
     o.yp = iy == (uint32_t)(ny - 1) ? -(ny - 1) * nz : nz;
     o.zm = iz == 0 ? nz - 1 : -1;

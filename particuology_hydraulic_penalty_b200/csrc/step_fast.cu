@@ -32,8 +32,10 @@ struct FastWin {
     int32_t moving;
     int32_t inactive;
     int32_t trt;
+    int32_t open_x;  // PSC_WIN_OPEN_X
     R scale, inv_scale;
     WinConst<R> c;
+    R corr[Q];       // open_x: bounce-back inlet term 2 w_i rho_in (c_i . u_in) / cs^2
     R Blut[256];
     R kblut[256];
     R alut[256];  // clipped solid fraction per level
@@ -70,6 +72,11 @@ __device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool mov
         s.tau = (R)W.tau;
         make_win_const(s.c, W.tau, W.force[0], W.force[1], W.force[2], W.tau_minus);
         s.trt = W.tau_minus > 0.0 ? 1 : 0;
+        s.open_x = (W.flags & PSC_WIN_OPEN_X) ? 1 : 0;
+    }
+    if ((W.flags & PSC_WIN_OPEN_X) && threadIdx.x < Q) {
+        const int i = threadIdx.x;
+        s.corr[i] = (R)inlet_correction_exact(i, W.inlet_rho, W.inlet_u[0], W.inlet_u[1], W.inlet_u[2]);
     }
     const int S = W.subsamples;
     const int S3 = S * S * S;
@@ -86,9 +93,18 @@ __device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool mov
 
 // RED: PSC_STEP_REDUCE as a compile-time switch, so launches without
 // reductions carry no loop-carried FP64 accumulators.
-// FP64 arithmetic needs about twice the registers: keep two CTAs resident.
+// Resident CTAs the register allocation aims for: four (64 registers) for
+// FP32/FP16/BF16 storage, three with moving particles (the solid-velocity
+// terms), two for FP64, whose arithmetic needs about twice the registers, and
+// two with reductions (13 FP64 accumulators per thread).  An explicit target
+// matters: ptxas allocates differently without one.
+template <int STORE, bool MOVING, bool RED>
+struct StepOccupancy {
+    static constexpr int value = (STORE == PSC_STORE_F64 || RED) ? 2 : (MOVING ? 3 : 4);
+};
+
 template <int STORE, bool MOVING, int CPT, bool RED>
-__global__ void __launch_bounds__(STEP_THREADS, STORE == PSC_STORE_F64 ? 2 : 1) k_step_fast(const psc_window* __restrict__ wins, int nwin,
+__global__ void __launch_bounds__(STEP_THREADS, (StepOccupancy<STORE, MOVING, RED>::value)) k_step_fast(const psc_window* __restrict__ wins, int nwin,
                                                              int64_t total_tiles, unsigned flags) {
     using TR = StoreTraits<STORE>;
     using T = typename TR::T;
@@ -128,13 +144,17 @@ __global__ void __launch_bounds__(STEP_THREADS, STORE == PSC_STORE_F64 ? 2 : 1) 
         const T* src = sw.src;
         R f[CPT][Q];
         uint32_t cells[CPT];
+        bool inlet[CPT];
+        const bool open_x = sw.open_x;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             cells[k] = cell;
+            inlet[k] = open_x && ix == 0;
             if (cell < N) {
                 const int32_t nyz = (int32_t)(ny * nz);
-                const int32_t xm = ix == 0 ? (int32_t)(nx - 1) * nyz : -nyz;
-                const int32_t xp = ix == nx - 1 ? -(int32_t)(nx - 1) * nyz : nyz;
+                // open x: the x faces read the cell's own plane (zero-gradient outflow)
+                const int32_t xm = ix == 0 ? (open_x ? 0 : (int32_t)(nx - 1) * nyz) : -nyz;
+                const int32_t xp = ix == nx - 1 ? (open_x ? 0 : -(int32_t)(nx - 1) * nyz) : nyz;
                 const int32_t ym = iy == 0 ? (int32_t)(ny - 1) * (int32_t)nz : -(int32_t)nz;
                 const int32_t yp = iy == ny - 1 ? -(int32_t)(ny - 1) * (int32_t)nz : (int32_t)nz;
                 const int32_t zm = iz == 0 ? (int32_t)nz - 1 : -1;
@@ -168,6 +188,16 @@ __global__ void __launch_bounds__(STEP_THREADS, STORE == PSC_STORE_F64 ? 2 : 1) 
             if (TR::scaled) {
 #pragma unroll
                 for (int i = 0; i < Q; ++i) g[i] *= sw.inv_scale;
+            }
+            if (inlet[k]) {  // velocity inlet at x = 0 (the x = 0 plane only): bounce-back of the node's own
+                             // opp(i) + 2 w_i rho_in (c_i . u_in) / cs^2
+#pragma unroll
+                for (int i = 0; i < Q; ++i) {
+                    if (!enters_x0(i)) continue;
+                    R back = ld_pop(sw.src + (size_t)opp(i) * N + c);
+                    if (TR::scaled) back *= sw.inv_scale;
+                    g[i] = back + sw.corr[i];
+                }
             }
             R B, kb, al;
             if (sw.level) {

@@ -56,6 +56,18 @@ def trt_tau_minus(tau: float, magic: float = 3.0 / 16.0) -> float:
     return 0.5 + magic / (tau - 0.5)
 
 
+def check_inlet(inlet):
+    """Normalise an inlet specification ``(rho_in, (ux, uy, uz))`` (None: periodic along x)."""
+    if inlet is None:
+        return None
+    rho, u = inlet
+    rho = float(rho)
+    u = tuple(float(v) for v in u)
+    if len(u) != 3 or not np.isfinite(rho) or rho <= 0.0 or not np.all(np.isfinite(u)):
+        raise ValueError("inlet must be (rho_in > 0, (ux, uy, uz)) with finite values")
+    return rho, u
+
+
 def store_mode(precision: str) -> int:
     try:
         return PRECISIONS[precision]
@@ -324,8 +336,10 @@ class LatticeWindow:
     """Populations and per-cell fields of one periodic window on the device."""
 
     def __init__(self, shape, tau: float, force, subsamples: int, store: int, store_scale: float | None,
-                 device, tau_minus: float = 0.0):
+                 device, tau_minus: float = 0.0, inlet=None):
         self.nx, self.ny, self.nz = (int(v) for v in shape)
+        # inlet = (rho_in, (ux, uy, uz)): open along x (PSC_WIN_OPEN_X), else periodic
+        self.inlet = check_inlet(inlet)
         self.N = self.nx * self.ny * self.nz
         self.tau = float(tau)
         self.tau_minus = float(tau_minus)
@@ -390,9 +404,14 @@ class LatticeWindow:
         w = nat.PscWindow()
         w.nx, w.ny, w.nz = self.nx, self.ny, self.nz
         w.subsamples = self.subsamples
-        w.flags = nat.WIN_MOVING if self.moving else 0
+        w.flags = (nat.WIN_MOVING if self.moving else 0) | (nat.WIN_OPEN_X if self.inlet else 0)
         w.tau = self.tau
         w.tau_minus = self.tau_minus
+        if self.inlet:
+            w.inlet_rho = self.inlet[0]
+            w.inlet_u[0], w.inlet_u[1], w.inlet_u[2] = self.inlet[1]
+        else:
+            w.inlet_rho = 1.0
         w.force[0], w.force[1], w.force[2] = self.force
         w.store_scale = self.store_scale
         w.f_src = vp(self.f[src])
@@ -447,8 +466,13 @@ class LatticeWindow:
     def post_stream_f(self) -> torch.Tensor:
         """Absolute FP64 post-stream populations (19, nx, ny, nz) on the device."""
         out = torch.empty(Q * self.N, dtype=torch.float64, device=self.device)
-        nat.call("psc_stream_push", self.store, self.store_scale, vp(self.f[self.cur]), vp(out), self.nx, self.ny,
-                 self.nz, stream_handle(self.device))
+        if self.inlet:
+            u = (ctypes.c_double * 3)(*self.inlet[1])
+            nat.call("psc_stream_push_open", self.store, self.store_scale, vp(self.f[self.cur]), vp(out), self.nx,
+                     self.ny, self.nz, self.inlet[0], u, stream_handle(self.device))
+        else:
+            nat.call("psc_stream_push", self.store, self.store_scale, vp(self.f[self.cur]), vp(out), self.nx, self.ny,
+                     self.nz, stream_handle(self.device))
         return out.view(Q, self.nx, self.ny, self.nz)
 
     def load_post_stream_f(self, f: torch.Tensor) -> None:

@@ -31,7 +31,7 @@ def _diag_dict(d: nat.PscDiag) -> dict:
 
 def make_config(shape, *, tau: float, force, subsamples: int, store: int, static_geometry: bool = True,
                 device_index: int = 0, tau_minus: float = 0.0, store_scale: float | None = None,
-                conv_tol: float = 0.0, conv_min_steps: int = 1) -> nat.PscConfig:
+                conv_tol: float = 0.0, conv_min_steps: int = 1, inlet=None) -> nat.PscConfig:
     c = nat.PscConfig()
     c.nx, c.ny, c.nz = (int(v) for v in shape)
     c.subsamples = int(subsamples)
@@ -48,6 +48,10 @@ def make_config(shape, *, tau: float, force, subsamples: int, store: int, static
     c.store_scale = 0.0 if store_scale is None else float(store_scale)
     c.conv_tol = float(conv_tol)
     c.stream = None
+    if inlet is not None:  # (rho_in, (ux, uy, uz)): open along x
+        c.open_x = 1
+        c.inlet_rho = float(inlet[0])
+        c.inlet_u[0], c.inlet_u[1], c.inlet_u[2] = (float(v) for v in inlet[1])
     return c
 
 

@@ -17,6 +17,9 @@ Extra keyword-only arguments (absent from the reference):
     device      CUDA device
     collision   "bgk" (default, the reference) or "trt" (two relaxation times,
                 magic parameter 3/16; deviation storage modes only)
+    inlet       None (default: periodic, the reference) or (rho_in, (ux, uy, uz)):
+                open along x with a velocity inlet at x = 0 and a zero-gradient
+                outflow at x = n - 1 (y and z stay periodic)
 """
 
 from __future__ import annotations
@@ -27,7 +30,7 @@ import numpy as np
 import torch
 
 from . import _native as nat
-from .engine import particles_array, require_cuda, store_mode, trt_tau_minus
+from .engine import check_inlet, particles_array, require_cuda, store_mode, trt_tau_minus
 from .handle import SolverHandle, make_config
 
 # D3Q19 velocity set in the reference's index order (psc3d.py:17-43).
@@ -96,7 +99,7 @@ class PscD3Q19:
 
     def __init__(self, n: int, particles, tau: float = 0.72, subsamples: int = 4, body_force_z: float = 0.0,
                  static_geometry: bool = False, *, precision: str = "fp64-exact", force=None,
-                 store_scale: float | None = None, device=None, collision: str = "bgk"):
+                 store_scale: float | None = None, device=None, collision: str = "bgk", inlet=None):
         self._device = require_cuda(device)
         self.n = int(n)
         if self.n <= 0:
@@ -121,10 +124,12 @@ class PscD3Q19:
         if store_scale is not None and not (np.isfinite(store_scale) and store_scale > 0.0):
             raise ValueError("store_scale must be a positive finite number")
         self.collision = collision
+        self.inlet = check_inlet(inlet)
         index = self._device.index if self._device.index is not None else torch.cuda.current_device()
         cfg = make_config((self.n,) * 3, tau=self.tau, force=self.force, subsamples=self.subsamples,
                           store=self._store, static_geometry=self.static_geometry, device_index=index,
-                          tau_minus=trt_tau_minus(self.tau) if collision == "trt" else 0.0, store_scale=store_scale)
+                          tau_minus=trt_tau_minus(self.tau) if collision == "trt" else 0.0, store_scale=store_scale,
+                          inlet=self.inlet)
         self._h = SolverHandle(cfg)
         parr = particles_array(particles)
         self._h.set_particles(parr)

@@ -133,3 +133,19 @@ def test_batch_config_mismatch_rejected(lib):
     cfgs = (nat.PscConfig * 2)(_config(), _config())
     assert lib.psc_batch_create(cfgs, 2, None, 3, ctypes.byref(b)) == nat.PSC_E_INVALID
     assert b"even" in lib.psc_last_error()
+
+
+def test_row_planner_rejects_open_windows(lib):
+    w = (nat.PscWindow * 1)()
+    w[0].nx, w[0].ny, w[0].nz = 16, 16, 16
+    w[0].flags = nat.WIN_OPEN_X
+    total, sb = ctypes.c_int64(0), ctypes.c_int32(0)
+    assert lib.psc_plan_row_tiles(w, 1, 0, 4, ctypes.byref(total), ctypes.byref(sb)) == nat.PSC_E_UNSUPPORTED
+    assert b"periodic" in lib.psc_last_error()
+
+
+def test_open_window_config_checked(lib):
+    h = ctypes.c_void_p()
+    cfg = _config(open_x=1, inlet_rho=0.0)
+    assert lib.psc_create(ctypes.byref(cfg), ctypes.byref(h)) == nat.PSC_E_INVALID
+    assert b"inlet" in lib.psc_last_error()
