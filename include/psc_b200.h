@@ -338,10 +338,14 @@ int psc_stream_push(int store, double store_scale, const void* src, double* dst,
  * no counterpart in the reference). */
 int psc_stream_push_open(int store, double store_scale, const void* src, double* dst, int nx, int ny, int nz,
                          double inlet_rho, const double* h_inlet_u, void* stream);
-/* Inverse: absolute FP64 post-stream f -> stored representation (also for
- * open windows: the entries it cannot recover are never read by a step). */
+/* Inverse: absolute FP64 post-stream f -> stored representation. */
 int psc_stream_pull_store(int store, double store_scale, const double* src, void* dst, int nx, int ny, int nz,
                           void* stream);
+/* psc_stream_pull_store for a PSC_WIN_OPEN_X window: also sets the stored
+ * populations that only the inlet's bounce-back reads, so the next pull
+ * reproduces src at x = 0 (to rounding in the exact mode). */
+int psc_stream_pull_store_open(int store, double store_scale, const double* src, void* dst, int nx, int ny, int nz,
+                               double inlet_rho, const double* h_inlet_u, void* stream);
 
 /* ======================================================================== *
  * Handle layer: the reference's solver object (PscD3Q19 / SparsePscD3Q19,  *

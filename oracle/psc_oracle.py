@@ -379,7 +379,10 @@ class OracleSolver:
                  static_geometry=False, force=None, inlet=None):
         self.n = int(n)
         # inlet = (rho_in, (ux, uy, uz)): open along x (stream_push_open_x), an
-        # extension beyond the reference; None: periodic, the reference
+        # extension beyond the reference; None: periodic, the reference.  An
+        # open window starts from the rest equilibrium taken as the
+        # post-collision state and streamed with its open boundaries (for a
+        # periodic window that is the equilibrium itself).
         self.inlet = inlet
         self.particles = particles
         self.tau = float(tau)
@@ -393,6 +396,8 @@ class OracleSolver:
         self.uy = np.zeros(shape)
         self.uz = np.zeros(shape)
         self.f = equilibrium(self.rho, self.ux, self.uy, self.uz)
+        if self.inlet is not None:
+            self.f = stream_push_open_x(self.f, *self.inlet)
         self.solid = np.zeros(shape)
         self.imb = np.zeros((3, *shape))
         P = len(particles_to_array(particles))

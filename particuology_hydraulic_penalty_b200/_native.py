@@ -178,6 +178,8 @@ SIGNATURES = {
     "psc_stream_pull_store": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "psc_stream_push_open": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_double,
                                      POINTER(c_double), c_void_p]),
+    "psc_stream_pull_store_open": (c_int, [c_int, c_double, c_void_p, c_void_p, c_int, c_int, c_int, c_double,
+                                           POINTER(c_double), c_void_p]),
     # handle layer
     "psc_create": (c_int, [POINTER(PscConfig), POINTER(c_void_p)]),
     "psc_destroy": (c_int, [c_void_p]),

@@ -384,4 +384,16 @@ int psc_stream_pull_store(int store, double store_scale, const double* src, void
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_stream_pull_store");
 }
 
+int psc_stream_pull_store_open(int store, double store_scale, const double* src, void* dst, int nx, int ny, int nz,
+                               double inlet_rho, const double* h_inlet_u, void* stream) {
+    if (!valid_store(store) || !src || !dst || !h_inlet_u)
+        return fail(PSC_E_INVALID, "psc_stream_pull_store_open: bad arguments");
+    int st = check_extent(nx, ny, nz, "psc_stream_pull_store_open");
+    if (st) return st;
+    const double inlet[4] = {inlet_rho, h_inlet_u[0], h_inlet_u[1], h_inlet_u[2]};
+    cudaError_t e =
+        launch_stream_pull_store(store, store_scale, src, dst, nx, ny, nz, as_stream(stream), true, inlet);
+    return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_stream_pull_store_open");
+}
+
 }  // extern "C"

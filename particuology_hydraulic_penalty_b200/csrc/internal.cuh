@@ -38,7 +38,7 @@ cudaError_t launch_init_equilibrium(int store, double scale, void* f, int64_t nc
 cudaError_t launch_stream_push(int store, double scale, const void* src, double* dst, int nx, int ny, int nz,
                                cudaStream_t stream, bool open_x = false, const double* inlet = nullptr);
 cudaError_t launch_stream_pull_store(int store, double scale, const double* src, void* dst, int nx, int ny, int nz,
-                                     cudaStream_t stream);
+                                     cudaStream_t stream, bool open_x = false, const double* inlet = nullptr);
 
 cudaError_t launch_geometry_plan(const psc_geometry& g, cudaStream_t stream);
 cudaError_t launch_geometry_build(const psc_geometry& g, cudaStream_t stream);

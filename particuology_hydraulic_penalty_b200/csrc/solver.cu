@@ -570,7 +570,10 @@ int window_set_populations(Window& w, const double* hf, cudaStream_t s, const ch
     cudaError_t e = cudaMemcpyAsync(tmp, hf, (size_t)n * 8, cudaMemcpyHostToDevice, s);
     int st = PSC_OK;
     if (e == cudaSuccess)
-        st = psc_stream_pull_store(w.cfg.store, w.scale, tmp, w.f[w.cur].p, w.cfg.nx, w.cfg.ny, w.cfg.nz, s);
+        st = w.cfg.open_x ? psc_stream_pull_store_open(w.cfg.store, w.scale, tmp, w.f[w.cur].p, w.cfg.nx, w.cfg.ny,
+                                                       w.cfg.nz, w.cfg.inlet_rho, w.cfg.inlet_u, s)
+                          : psc_stream_pull_store(w.cfg.store, w.scale, tmp, w.f[w.cur].p, w.cfg.nx, w.cfg.ny,
+                                                  w.cfg.nz, s);
     if (e == cudaSuccess && st == PSC_OK) e = cudaStreamSynchronize(s);
     cudaFree(tmp);
     if (e != cudaSuccess) return cuda_fail(e, who);

@@ -426,8 +426,37 @@ cudaError_t launch_stream_push(int store, double scale, const void* src, double*
     return cudaGetLastError();
 }
 
+// Open-x inverse at the inlet plane: the populations that only the inlet's
+// bounce-back reads (c_x = -1 at x = 0) are set so that the pulled value of
+// the entering direction i = opp(j) is f_i(0): stored_j = f_i - term_i (to
+// rounding in the exact mode).
+template <int STORE>
+__global__ void k_open_x_unpull(const double* src, void* dst, int nx, int ny, int nz, double scale, double in_rho,
+                                double in_ux, double in_uy, double in_uz) {
+    using TR = StoreTraits<STORE>;
+    using T = typename TR::T;
+    const uint32_t N = (uint32_t)nx * ny * nz;
+    const uint32_t plane = (uint32_t)ny * nz;  // the cells of x = 0
+    T* d = reinterpret_cast<T*>(dst);
+    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < plane; cell += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            if (!enters_x0(i)) continue;
+            const int j = opp(i);
+            double v = xsub(src[(size_t)i * N + cell], inlet_correction_exact(i, in_rho, in_ux, in_uy, in_uz));
+            if (!TR::exact) {
+                v -= wgt(j);
+                if (TR::scaled) v *= scale;
+            }
+            if constexpr (sizeof(T) == 8) d[(size_t)j * N + cell] = (T)v;
+            else if constexpr (sizeof(T) == 4) d[(size_t)j * N + cell] = (T)v;
+            else st_pop(d + (size_t)j * N + cell, (float)v);
+        }
+    }
+}
+
 cudaError_t launch_stream_pull_store(int store, double scale, const double* src, void* dst, int nx, int ny, int nz,
-                                     cudaStream_t stream) {
+                                     cudaStream_t stream, bool open_x, const double* inlet) {
     const int g = grid_for((int64_t)nx * ny * nz, 256);
     switch (store) {
         case PSC_STORE_F64_EXACT: k_stream_pull_store<PSC_STORE_F64_EXACT><<<g, 256, 0, stream>>>(src, dst, nx, ny, nz, scale); break;
@@ -437,6 +466,21 @@ cudaError_t launch_stream_pull_store(int store, double scale, const double* src,
         case PSC_STORE_BF16: k_stream_pull_store<PSC_STORE_BF16><<<g, 256, 0, stream>>>(src, dst, nx, ny, nz, scale); break;
         default: return cudaErrorInvalidValue;
     }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !open_x) return e;
+    const int gp = grid_for((int64_t)ny * nz, 256);
+    const double r = inlet[0], ux = inlet[1], uy = inlet[2], uz = inlet[3];
+#define PSC_UNPULL_CASE(S) \
+    case S: k_open_x_unpull<S><<<gp, 256, 0, stream>>>(src, dst, nx, ny, nz, scale, r, ux, uy, uz); break;
+    switch (store) {
+        PSC_UNPULL_CASE(PSC_STORE_F64_EXACT)
+        PSC_UNPULL_CASE(PSC_STORE_F64)
+        PSC_UNPULL_CASE(PSC_STORE_F32)
+        PSC_UNPULL_CASE(PSC_STORE_F16)
+        PSC_UNPULL_CASE(PSC_STORE_BF16)
+        default: return cudaErrorInvalidValue;
+    }
+#undef PSC_UNPULL_CASE
     return cudaGetLastError();
 }
 

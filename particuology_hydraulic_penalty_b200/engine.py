@@ -480,5 +480,10 @@ class LatticeWindow:
         src = f.to(device=self.device, dtype=torch.float64).contiguous().view(-1)
         if src.numel() != Q * self.N:
             raise ValueError(f"f must have {Q}x{self.nx}x{self.ny}x{self.nz} elements")
-        nat.call("psc_stream_pull_store", self.store, self.store_scale, vp(src), vp(self.f[self.cur]), self.nx,
-                 self.ny, self.nz, stream_handle(self.device))
+        if self.inlet:
+            u = (ctypes.c_double * 3)(*self.inlet[1])
+            nat.call("psc_stream_pull_store_open", self.store, self.store_scale, vp(src), vp(self.f[self.cur]),
+                     self.nx, self.ny, self.nz, self.inlet[0], u, stream_handle(self.device))
+        else:
+            nat.call("psc_stream_pull_store", self.store, self.store_scale, vp(src), vp(self.f[self.cur]), self.nx,
+                     self.ny, self.nz, stream_handle(self.device))
