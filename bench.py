@@ -385,7 +385,7 @@ def run_ours(args):
     specs = [WindowSpec(w.n, w.particles, TAU, FORCE, SUBSAMPLES, name=w.kind) for w in wins]
     from particuology_hydraulic_penalty_b200 import _native as nat
 
-    kernel = {"direct": nat.KERNEL_DIRECT, "tma": nat.KERNEL_TMA}[args.kernel]
+    kernel = {"direct": nat.KERNEL_DIRECT, "tma": nat.KERNEL_TMA, "pair": nat.KERNEL_PAIR}[args.kernel]
     batch = PscBatch(specs, precision=args.precision, graph_steps=args.graph_steps, kernel=kernel)
     tuned = None
     if args.autotune:
@@ -518,7 +518,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="batch24")
     ap.add_argument("--precision", choices=["fp32", "fp64", "fp16", "bf16"], default="fp32")
     ap.add_argument("--graph-steps", type=int, default=20)
-    ap.add_argument("--kernel", choices=["direct", "tma"], default="direct")
+    ap.add_argument("--kernel", choices=["direct", "tma", "pair"], default="direct")
     ap.add_argument("--autotune", action="store_true", help="pick the launch with the project autotuner first")
     ap.add_argument("--fp64-steps", type=int, default=20)
     ap.add_argument("--e2e-steps", type=int, default=20)

@@ -69,6 +69,8 @@ extern "C" {
 #define PSC_KERNEL_AUTO 0   /* the library's choice */
 #define PSC_KERNEL_DIRECT 1 /* per-thread coalesced pulls (any window) */
 #define PSC_KERNEL_TMA 2    /* bulk-copy (TMA) row staging in shared memory */
+#define PSC_KERNEL_PAIR 3   /* two consecutive z cells per thread, 2-element loads and stores; windows planned
+                               by psc_plan_pair_tiles (nz even, population buffers 16-byte aligned) */
 
 /* Launch configuration of psc_step_windows_ex(). */
 typedef struct psc_launch {
@@ -231,8 +233,13 @@ int psc_plan_tiles(struct psc_window* h_windows, int nwin, int tile_cells, int64
  * tile count and the shared-memory bytes one stage needs. */
 int psc_plan_row_tiles(struct psc_window* h_windows, int nwin, int rows, int elem_bytes, int64_t* h_total_tiles,
                        int32_t* h_stage_bytes);
+/* Tiles for PSC_KERNEL_PAIR: 512-cell tiles (two cells per thread); every
+ * window needs an even nz (a cell pair never crosses a z row). */
+int psc_plan_pair_tiles(struct psc_window* h_windows, int nwin, int64_t* h_total_tiles);
 /* Device-side status word: non-zero after a kernel gave up a bounded wait
- * (0x101 producer, 0x102 drain, 0x103 consumer).  Synchronises. */
+ * (0x101 producer, 0x102 drain, 0x103 consumer) or skipped a window it
+ * cannot run (0x201 odd nz, 0x202 tiles not planned for the pair kernel).
+ * Synchronises. */
 int psc_device_status(int* h_status, int clear);
 
 /* Equilibrium at rho = 1, u = 0 in the given storage mode

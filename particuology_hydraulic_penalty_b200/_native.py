@@ -104,7 +104,7 @@ class PscAdjointArgs(ctypes.Structure):
     ]
 
 
-KERNEL_AUTO, KERNEL_DIRECT, KERNEL_TMA = 0, 1, 2
+KERNEL_AUTO, KERNEL_DIRECT, KERNEL_TMA, KERNEL_PAIR = 0, 1, 2, 3
 
 
 class PscLaunch(ctypes.Structure):
@@ -152,6 +152,7 @@ SIGNATURES = {
     "psc_plan_tiles": (c_int, [POINTER(PscWindow), c_int, c_int, POINTER(c_int64)]),
     "psc_plan_row_tiles": (c_int, [POINTER(PscWindow), c_int, c_int, c_int, POINTER(c_int64), POINTER(c_int32)]),
     "psc_device_status": (c_int, [POINTER(c_int), c_int]),
+    "psc_plan_pair_tiles": (c_int, [POINTER(PscWindow), c_int, POINTER(c_int64)]),
     "psc_init_equilibrium": (c_int, [c_int, c_double, c_void_p, c_int64, c_void_p]),
     "psc_geometry_plan": (c_int, [POINTER(PscGeometry), c_void_p]),
     "psc_geometry_build": (c_int, [POINTER(PscGeometry), c_void_p]),

@@ -60,8 +60,8 @@ class PscBatch:
         if self.cells_per_thread not in (1, 2, 4):
             raise ValueError("cells_per_thread must be 1, 2 or 4")
         self.kernel = int(kernel)
-        if self.kernel == nat.KERNEL_TMA and self.store == nat.STORE_F64_EXACT:
-            raise ValueError("the TMA kernel runs the deviation storage modes")
+        if self.kernel in (nat.KERNEL_TMA, nat.KERNEL_PAIR) and self.store == nat.STORE_F64_EXACT:
+            raise ValueError("the TMA and pair kernels run the deviation storage modes")
         self.tile_rows = int(tile_rows)
         self.rows_per_window: list[int] | None = None  # per-window TMA rows (autotuner), else tile_rows
         self.stages = int(stages)
@@ -129,6 +129,8 @@ class PscBatch:
                 rows = -1 if self.rows_per_window is not None else self.tile_rows
                 nat.call("psc_plan_row_tiles", arr, nwin, rows, elem, ctypes.byref(total), ctypes.byref(sb))
                 self.stage_bytes = int(sb.value)
+            elif self.kernel == nat.KERNEL_PAIR:
+                nat.call("psc_plan_pair_tiles", arr, nwin, ctypes.byref(total))
             else:
                 nat.call("psc_plan_tiles", arr, nwin, nat.STEP_THREADS * self.cells_per_thread, ctypes.byref(total))
             if self.partials is None:
@@ -146,8 +148,8 @@ class PscBatch:
     def configure(self, kernel: int, cells_per_thread: int = 1, tile_rows: int = 0, stages: int = 3,
                   rows_per_window=None, grid_ctas: int | None = None) -> None:
         """Switch the launch configuration (populations are kept; graphs are re-captured)."""
-        if kernel == nat.KERNEL_TMA and self.store == nat.STORE_F64_EXACT:
-            raise ValueError("the TMA kernel runs the deviation storage modes")
+        if kernel in (nat.KERNEL_TMA, nat.KERNEL_PAIR) and self.store == nat.STORE_F64_EXACT:
+            raise ValueError("the TMA and pair kernels run the deviation storage modes")
         self.kernel = int(kernel)
         self.cells_per_thread = int(cells_per_thread)
         self.tile_rows = int(tile_rows)
@@ -158,7 +160,8 @@ class PscBatch:
         self._build_tables()
 
     def launch_config(self) -> dict:
-        return {"kernel": {nat.KERNEL_AUTO: "direct", nat.KERNEL_DIRECT: "direct", nat.KERNEL_TMA: "tma"}[self.kernel],
+        return {"kernel": {nat.KERNEL_AUTO: "direct", nat.KERNEL_DIRECT: "direct", nat.KERNEL_TMA: "tma",
+                           nat.KERNEL_PAIR: "pair"}[self.kernel],
                 "cells_per_thread": self.cells_per_thread, "tile_rows": self.tile_rows, "stages": self.stages,
                 "rows_per_window": self.rows_per_window, "stage_bytes": self.stage_bytes}
 

@@ -163,8 +163,20 @@ int psc_plan_row_tiles(psc_window* h_windows, int nwin, int rows, int elem_bytes
 
 int psc_device_status(int* h_status, int clear) {
     if (!h_status) return fail(PSC_E_INVALID, "psc_device_status: null output");
-    cudaError_t e = read_device_status(h_status, clear != 0);
+    int tma = 0, pair = 0;
+    cudaError_t e = read_device_status(&tma, clear != 0);
+    if (e == cudaSuccess) e = read_pair_status(&pair, clear != 0);
+    *h_status = tma ? tma : pair;
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_device_status");
+}
+
+int psc_plan_pair_tiles(psc_window* h_windows, int nwin, int64_t* h_total_tiles) {
+    if (!h_windows || nwin <= 0 || !h_total_tiles) return fail(PSC_E_INVALID, "psc_plan_pair_tiles: bad arguments");
+    for (int w = 0; w < nwin; ++w)
+        if (h_windows[w].nz % 2 != 0)
+            return fail(PSC_E_UNSUPPORTED, "psc_plan_pair_tiles: the pair kernel needs an even nz (window " +
+                                               std::to_string(w) + ")");
+    return psc_plan_tiles(h_windows, nwin, 2 * STEP_THREADS, h_total_tiles);
 }
 
 int psc_init_equilibrium(int store, double store_scale, void* f, int64_t ncells, void* stream) {
@@ -228,6 +240,8 @@ int psc_step_windows_ex(int store, const psc_window* d_windows, int nwin, int64_
     } else if (c.kernel == PSC_KERNEL_AUTO || c.kernel == PSC_KERNEL_DIRECT) {
         e = launch_step_fast(store, d_windows, nwin, total_tiles, flags, moving, c.cells_per_thread, c.grid_ctas,
                              as_stream(stream));
+    } else if (c.kernel == PSC_KERNEL_PAIR) {
+        e = launch_step_pair(store, d_windows, nwin, total_tiles, flags, moving, c.grid_ctas, as_stream(stream));
     } else if (c.kernel == PSC_KERNEL_TMA) {
         const int stages = c.stages == 0 ? 3 : c.stages;
         if (stages < 2 || stages > 4) return fail(PSC_E_INVALID, "psc_step_windows: TMA stages must be 2, 3 or 4");

@@ -937,6 +937,8 @@ int batch_build_tables(psc_batch& b) {
             int32_t sb = 0;
             PSC_TRY(psc_plan_row_tiles(tab[p].data(), nwin, 0, store_elem_bytes(b.store), &total, &sb));
             b.launch.stage_bytes = sb;
+        } else if (b.launch.kernel == PSC_KERNEL_PAIR) {
+            PSC_TRY(psc_plan_pair_tiles(tab[p].data(), nwin, &total));
         } else {
             PSC_TRY(psc_plan_tiles(tab[p].data(), nwin, 256 * b.launch.cells_per_thread, &total));
         }
@@ -1084,7 +1086,8 @@ int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_lau
     if (lc.grid_ctas < 0) return fail(PSC_E_INVALID, "psc_batch_create: grid_ctas must be >= 0");
     if (lc.cells_per_thread != 1 && lc.cells_per_thread != 2 && lc.cells_per_thread != 4)
         return fail(PSC_E_INVALID, "psc_batch_create: cells_per_thread must be 1, 2 or 4");
-    if (h_cfgs[0].store == PSC_STORE_F64_EXACT && (lc.cells_per_thread != 1 || lc.kernel == PSC_KERNEL_TMA))
+    if (h_cfgs[0].store == PSC_STORE_F64_EXACT &&
+        (lc.cells_per_thread != 1 || lc.kernel == PSC_KERNEL_TMA || lc.kernel == PSC_KERNEL_PAIR))
         return fail(PSC_E_UNSUPPORTED, "psc_batch_create: PSC_STORE_F64_EXACT runs the one-cell-per-thread kernel");
     if (lc.kernel == PSC_KERNEL_TMA && lc.stages == 0) lc.stages = 3;
     DeviceScope ds(h_cfgs[0].device);

@@ -198,3 +198,33 @@ def test_trt_matches_oracle(kernel):
     bb = PscBatch([WindowSpec(w.n, w.particles, tau=tau, force=F, subsamples=2)], precision="fp64", graph_steps=0)
     bb.run(6)
     assert np.abs(bb.velocity_field(0)[1] - mom[1]).max() > 1e-3 * np.abs(ux).max()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64", "fp16", "bf16"])
+def test_pair_kernel_matches_direct(precision):
+    """Two cells per thread with paired loads/stores: the same arithmetic per cell, identical populations."""
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    wins = [wgen.make_window(16, "skeleton", 1), wgen.make_window(26, "passive", 2),
+            wgen.make_window(48, "preloaded", 3)]
+    moving = wins[1].particles.copy()
+    moving[:, 4:7] = 2e-4  # the moving-particle path too
+    specs = [WindowSpec(wins[0].n, wins[0].particles, tau=0.8, force=(1e-6, 0.0, 3e-7), subsamples=4),
+             WindowSpec(wins[1].n, moving, tau=0.7, force=(0.0, 2e-6, 0.0), subsamples=4, collision="trt"),
+             WindowSpec(wins[2].n, wins[2].particles, tau=0.9, force=(0.0, 0.0, 0.0), subsamples=4,
+                        inlet=(1.0, (0.003, 0.0, 0.0005)))]
+    d = PscBatch(specs, precision=precision, graph_steps=0)
+    d.run(9)
+    p = PscBatch(specs, precision=precision, graph_steps=4, kernel=nat.KERNEL_PAIR)
+    p.run(9)
+    for k in range(len(specs)):
+        assert np.array_equal(p.velocity_field(k), d.velocity_field(k))
+        assert np.array_equal(p.windows[k].post_stream_f().cpu().numpy(), d.windows[k].post_stream_f().cpu().numpy())
+    rd, rp = d.observe(), p.observe()
+    assert np.allclose(rp, rd, rtol=1e-13, atol=1e-13 * np.abs(rd).max())
+    Fd, Td = d.loads()[1]
+    Fp, Tp = p.loads()[1]
+    assert np.array_equal(Fd, Fp) and np.array_equal(Td, Tp)
+    assert ctypes_status() == 0

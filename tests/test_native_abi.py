@@ -149,3 +149,15 @@ def test_open_window_config_checked(lib):
     cfg = _config(open_x=1, inlet_rho=0.0)
     assert lib.psc_create(ctypes.byref(cfg), ctypes.byref(h)) == nat.PSC_E_INVALID
     assert b"inlet" in lib.psc_last_error()
+
+
+def test_pair_planner_needs_even_nz(lib):
+    w = (nat.PscWindow * 2)()
+    w[0].nx, w[0].ny, w[0].nz = 8, 8, 8
+    w[1].nx, w[1].ny, w[1].nz = 8, 8, 9
+    total = ctypes.c_int64(0)
+    assert lib.psc_plan_pair_tiles(w, 2, ctypes.byref(total)) == nat.PSC_E_UNSUPPORTED
+    assert b"even nz" in lib.psc_last_error()
+    w[1].nz = 10
+    assert lib.psc_plan_pair_tiles(w, 2, ctypes.byref(total)) == nat.PSC_OK
+    assert w[0].tile_cells == 512 and total.value == 1 + (640 + 511) // 512
