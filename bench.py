@@ -169,10 +169,17 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel_tag: str):
+STEP_KERNELS = {
+    "direct": ("psc::k_step_fast", "k_step_batch24.txt"),
+    "pair": ("psc::k_step_pair", "k_step_pair_batch24.txt"),
+    "tma": ("psc::k_step_tma", "k_step_batch24.txt"),
+}
+
+
+def ncu_traffic(kernel_tag: str, launch_kernel: str = "direct"):
     """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "k_step_batch24.txt"
-    if not p.exists():
+    p = ROOT / "profiles" / STEP_KERNELS.get(launch_kernel, STEP_KERNELS["direct"])[1]
+    if not p.exists() or launch_kernel == "tma":
         return None
     for line in p.read_text().splitlines():
         if line.startswith(f"traffic_bytes_per_launch[{kernel_tag}]"):
@@ -385,7 +392,8 @@ def run_ours(args):
     specs = [WindowSpec(w.n, w.particles, TAU, FORCE, SUBSAMPLES, name=w.kind) for w in wins]
     from particuology_hydraulic_penalty_b200 import _native as nat
 
-    kernel = {"direct": nat.KERNEL_DIRECT, "tma": nat.KERNEL_TMA, "pair": nat.KERNEL_PAIR}[args.kernel]
+    kernel = {"auto": nat.KERNEL_AUTO, "direct": nat.KERNEL_DIRECT, "tma": nat.KERNEL_TMA,
+              "pair": nat.KERNEL_PAIR}[args.kernel]
     batch = PscBatch(specs, precision=args.precision, graph_steps=args.graph_steps, kernel=kernel)
     tuned = None
     if args.autotune:
@@ -410,7 +418,8 @@ def run_ours(args):
     bpl = BYTES_PER_LUP[args.precision]
     peak, peak_kind = measured_peak_hbm()
     achieved = bpl * lups_rank / 1e9
-    traffic = ncu_traffic(args.precision)
+    launch_kernel = batch.launch_config()["kernel"]
+    traffic = ncu_traffic(args.precision, launch_kernel)
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
@@ -425,8 +434,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                      "traffic": traffic, "bytes_per_lup": bpl,
-                     "kernel": "psc::k_step_fast (fused pull-stream + PSC collide, deviation storage); avg launch = "
-                  "timed region / steps"},
+                     "kernel": STEP_KERNELS[launch_kernel][0] + " (fused pull-stream + PSC collide, deviation "
+                               "storage); avg launch = timed region / steps"},
         "clocks": clk,
         "nonfinite": nonfinite,
     }
@@ -518,7 +527,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="batch24")
     ap.add_argument("--precision", choices=["fp32", "fp64", "fp16", "bf16"], default="fp32")
     ap.add_argument("--graph-steps", type=int, default=20)
-    ap.add_argument("--kernel", choices=["direct", "tma", "pair"], default="direct")
+    ap.add_argument("--kernel", choices=["auto", "direct", "tma", "pair"], default="auto",
+                    help="auto: the pair kernel when every window has an even nz, else direct")
     ap.add_argument("--autotune", action="store_true", help="pick the launch with the project autotuner first")
     ap.add_argument("--fp64-steps", type=int, default=20)
     ap.add_argument("--e2e-steps", type=int, default=20)

@@ -66,7 +66,8 @@ extern "C" {
 #define PSC_STEP_MOVING 16u /* some window has PSC_WIN_MOVING: compile in the u_s path */
 
 /* ---- kernel variants of the deviation modes ----------------------------- */
-#define PSC_KERNEL_AUTO 0   /* the library's choice */
+#define PSC_KERNEL_AUTO 0   /* psc_step_windows_ex: the direct kernel; the handle layer picks the pair
+                               kernel for FP32/FP16/BF16 storage when every window has an even nz */
 #define PSC_KERNEL_DIRECT 1 /* per-thread coalesced pulls (any window) */
 #define PSC_KERNEL_TMA 2    /* bulk-copy (TMA) row staging in shared memory */
 #define PSC_KERNEL_PAIR 3   /* two consecutive z cells per thread, 2-element loads and stores; windows planned

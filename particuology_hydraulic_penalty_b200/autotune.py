@@ -3,6 +3,8 @@
 Candidates (all compute identical per-cell arithmetic, so the choice only
 changes speed):
   * direct kernel, 1 or 2 cells per thread;
+  * pair kernel (two consecutive z cells per thread, 2-element accesses),
+    when every window has an even nz;
   * TMA row-staged kernel, 2 / 3 / 4 pipeline stages, with the rows per tile
     chosen per window SIZE CLASS (windows of equal extent share a class).
 
@@ -100,6 +102,10 @@ def tune(batch, steps: int = 20, use_cache: bool = True, verbose: bool = False) 
             batch.configure(nat.KERNEL_DIRECT, cells_per_thread=cpt)
             results.append(({"kernel": "direct", "cells_per_thread": cpt}, _time(batch, steps)))
             _restore(batch, snap)
+        if all(w.nz % 2 == 0 for w in batch.windows):
+            batch.configure(nat.KERNEL_PAIR)
+            results.append(({"kernel": "pair"}, _time(batch, steps)))
+            _restore(batch, snap)
         if tma_ok:
             # per size class: best rows (2 stages), timed on a batch of that class only
             classes = sorted({(w.nx, w.ny, w.nz) for w in batch.windows})
@@ -147,6 +153,8 @@ def _apply(batch, cfg: dict) -> None:
         batch.configure(nat.KERNEL_TMA, stages=int(cfg["stages"]), rows_per_window=cfg["rows_per_window"])
     elif cfg.get("kernel") == "direct":
         batch.configure(nat.KERNEL_DIRECT, cells_per_thread=int(cfg["cells_per_thread"]))
+    elif cfg.get("kernel") == "pair":
+        batch.configure(nat.KERNEL_PAIR)
 
 
 class _SubBatch:

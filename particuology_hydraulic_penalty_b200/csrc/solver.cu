@@ -166,6 +166,7 @@ struct Window {
     int64_t partials_cap = 0;  // tiles the partial buffer holds
     int64_t solo_tiles = 0;
     DArray<psc_window> solo[2];  // single-window descriptor table per parity
+    int solo_kernel = PSC_KERNEL_AUTO;  // kernel of the single-window launches
     bool solo_dirty = true;
     uint64_t desc_version = 1;   // bumped whenever a descriptor field changes
     // particles and geometry
@@ -410,8 +411,15 @@ int window_upload_solo(Window& w, cudaStream_t s) {
     if (!w.solo_dirty) return PSC_OK;
     psc_window d[2] = {w.descriptor(0), w.descriptor(1)};
     int64_t total = 0;
-    PSC_TRY(psc_plan_tiles(d, 1, 0, &total));
-    PSC_TRY(psc_plan_tiles(d + 1, 1, 0, &total));
+    // FP32/FP16/BF16 storage with an even nz: the pair kernel (two z cells per thread)
+    w.solo_kernel = (w.cfg.store >= PSC_STORE_F32 && w.cfg.nz % 2 == 0) ? PSC_KERNEL_PAIR : PSC_KERNEL_AUTO;
+    if (w.solo_kernel == PSC_KERNEL_PAIR) {
+        PSC_TRY(psc_plan_pair_tiles(d, 1, &total));
+        PSC_TRY(psc_plan_pair_tiles(d + 1, 1, &total));
+    } else {
+        PSC_TRY(psc_plan_tiles(d, 1, 0, &total));
+        PSC_TRY(psc_plan_tiles(d + 1, 1, 0, &total));
+    }
     if (total > w.partials_cap) return fail(PSC_E_CAPACITY, "window descriptor: tile partials too small");
     d[0].partials = w.partials.p;
     d[1].partials = w.partials.p;
@@ -428,7 +436,7 @@ int window_upload_solo(Window& w, cudaStream_t s) {
 int launch_solo(Window& w, unsigned flags, cudaStream_t s) {
     PSC_TRY(window_upload_solo(w, s));
     if (w.moving) flags |= PSC_STEP_MOVING;
-    psc_launch c = {0, 1, PSC_KERNEL_AUTO, 0, 0};
+    psc_launch c = {0, 1, w.solo_kernel, 0, 0};
     return psc_step_windows_ex(w.cfg.store, w.solo[w.cur].p, 1, w.solo_tiles, flags, &c, s);
 }
 
@@ -1090,6 +1098,12 @@ int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_lau
         (lc.cells_per_thread != 1 || lc.kernel == PSC_KERNEL_TMA || lc.kernel == PSC_KERNEL_PAIR))
         return fail(PSC_E_UNSUPPORTED, "psc_batch_create: PSC_STORE_F64_EXACT runs the one-cell-per-thread kernel");
     if (lc.kernel == PSC_KERNEL_TMA && lc.stages == 0) lc.stages = 3;
+    if (lc.kernel == PSC_KERNEL_AUTO && h_cfgs[0].store >= PSC_STORE_F32 && lc.cells_per_thread == 1) {
+        // the pair kernel when every window has an even nz (as the Python batch decides)
+        bool even = true;
+        for (int k = 0; k < nwin; ++k) even = even && h_cfgs[k].nz % 2 == 0;
+        if (even) lc.kernel = PSC_KERNEL_PAIR;
+    }
     DeviceScope ds(h_cfgs[0].device);
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_batch_create: cudaSetDevice");
     std::unique_ptr<psc_batch> b(new (std::nothrow) psc_batch());
