@@ -112,6 +112,51 @@ struct DeviceScope {
     }
 };
 
+// Auxiliary streams of a handle for work of one step that is independent of
+// the main stream's (particle loads beside the post-stream reduction pass):
+// begin() makes every lane wait for the main stream's work so far, end()
+// makes the main stream wait for every lane.
+struct Lanes {
+    static constexpr int kMax = 4;
+    int n = 0;
+    cudaStream_t s[kMax] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kMax] = {};
+    Lanes() = default;
+    Lanes(const Lanes&) = delete;
+    Lanes& operator=(const Lanes&) = delete;
+    ~Lanes() {
+        for (int i = 0; i < n; ++i) {
+            if (s[i]) cudaStreamDestroy(s[i]);
+            if (join[i]) cudaEventDestroy(join[i]);
+        }
+        if (fork) cudaEventDestroy(fork);
+    }
+    cudaError_t init(int count) {
+        cudaError_t e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        for (int i = 0; i < count && i < kMax && e == cudaSuccess; ++i) {
+            e = cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) n = i + 1;
+        }
+        return e;
+    }
+    cudaStream_t lane(int k) const { return s[k % n]; }
+    cudaError_t begin(cudaStream_t main) {
+        cudaError_t e = cudaEventRecord(fork, main);
+        for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(s[i], fork, 0);
+        return e;
+    }
+    cudaError_t end(cudaStream_t main) {
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < n && e == cudaSuccess; ++i) {
+            e = cudaEventRecord(join[i], s[i]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(main, join[i], 0);
+        }
+        return e;
+    }
+};
+
 int store_elem_bytes(int store) {
     switch (store) {
         case PSC_STORE_F64_EXACT:
@@ -651,6 +696,7 @@ struct psc_solver {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    Lanes lanes;  // one lane: particle loads beside the post-stream reduction pass
     Window w;
     HArray<int64_t> tot;
     HArray<double> host_out;
@@ -664,13 +710,18 @@ namespace {
 int solver_report(psc_solver& h, bool loads, bool fields, bool post = true) {
     Window& w = h.w;
     cudaStream_t s = h.stream;
-    if (loads) PSC_TRY(window_loads(w, s));
     if (fields) PSC_TRY(window_ensure_moments(w, s));
+    if (post || fields) PSC_TRY(window_upload_solo(w, s));  // (synchronises when a descriptor changed)
+    if (loads) {  // the loads read the IMB field and geometry only: beside the reduction pass
+        PSC_CUDA(h.lanes.begin(s), "psc_step");
+        PSC_TRY(window_loads(w, h.lanes.lane(0)));
+    }
     if (post || fields) {
         // the step's own partials (pre-collision state) were reduced into red_pre already
         PSC_TRY(launch_solo(w, PSC_STEP_REDUCE | (fields ? PSC_STEP_MOMENTS : 0u), s));
         PSC_TRY(psc_reduce_windows(w.solo[w.cur].p, 1, red_post(w), s));
     }
+    if (loads) PSC_CUDA(h.lanes.end(s), "psc_step");
     PSC_CUDA(h.host_out.ensure(kOutLen), "psc_step");
     PSC_CUDA(cudaMemcpyAsync(h.host_out.p, w.out.p, kOutLen * sizeof(double), cudaMemcpyDeviceToHost, s), "psc_step");
     PSC_CUDA(cudaStreamSynchronize(s), "psc_step");
@@ -721,6 +772,10 @@ int psc_create(const psc_config* h_cfg, psc_solver** out) {
         h->own_stream = true;
     }
     int st = window_init(h->w, *h_cfg, h->stream, "psc_create");
+    if (st == PSC_OK) {
+        cudaError_t e = h->lanes.init(1);
+        if (e != cudaSuccess) st = cuda_fail(e, "psc_create");
+    }
     if (st == PSC_OK) st = window_set_particles(h->w, nullptr, 0, h->stream, "psc_create");
     if (st == PSC_OK) {
         cudaError_t e = cudaStreamSynchronize(h->stream);
@@ -910,6 +965,7 @@ struct psc_batch {
     std::vector<char> have_diag;
     std::vector<uint64_t> built_desc;  // descriptor versions the tables were built from
     bool moving_any = false;
+    Lanes lanes;  // particle loads of the windows beside the post-stream reduction pass
 
     ~psc_batch() {
         for (auto& g : graph)
@@ -1138,6 +1194,7 @@ int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_lau
         if (e == cudaSuccess) e = b->red_post.ensure((int64_t)nwin * PSC_NRED, true, b->stream);
         if (e == cudaSuccess) e = b->diag.ensure((int64_t)nwin * PSC_NDIAG, true, b->stream);
         if (e == cudaSuccess) e = b->host.ensure((int64_t)nwin * kOutLen);
+        if (e == cudaSuccess) e = b->lanes.init(Lanes::kMax);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) st = cuda_fail(e, "psc_batch_create");
     }
@@ -1184,17 +1241,20 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
         b->parity ^= 1;
         batch_sync_cur(*b);
         PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_pre.p, b->stream));
+        // the loads read the IMB field and geometry only: on the lanes, beside the reduction pass
+        PSC_CUDA(b->lanes.begin(b->stream), "psc_batch_step");
         for (int k = 0; k < nwin; ++k) {
             Window& w = *b->w[(size_t)k];
             if (b->frozen[(size_t)k] >= 0) continue;
             psc_geometry g = w.geometry();
             PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p,
                                        b->red_pre.p + (size_t)k * PSC_NRED + PSC_RED_IMBX, w.forces.p, w.torques.p,
-                                       b->diag.p + (size_t)k * PSC_NDIAG, b->stream));
+                                       b->diag.p + (size_t)k * PSC_NDIAG, b->lanes.lane(k)));
             w.loads_ready = true;
         }
         PSC_TRY(batch_launch(*b, PSC_STEP_REDUCE | (fields ? PSC_STEP_MOMENTS : 0u)));
         PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_post.p, b->stream));
+        PSC_CUDA(b->lanes.end(b->stream), "psc_batch_step");
         double* host = b->host.p;
         const size_t rows = (size_t)nwin * PSC_NRED;
         PSC_CUDA(cudaMemcpyAsync(host, b->red_pre.p, rows * 8, cudaMemcpyDeviceToHost, b->stream), "psc_batch_step");
