@@ -326,7 +326,7 @@ def run_e2e_dropin(windows, steps: int):
 
 def run_e2e_batch(windows, steps: int, graph_steps: int):
     """MLUPS through the batched C ABI with host buffers: every step uploads each window's particle
-    array (psc_batch_set_particles) and reads back every window's diagnostics (psc_batch_step with
+    array (psc_batch_set_particles_all) and reads back every window's diagnostics (psc_batch_step with
     PSC_RUN_DIAG: particle loads, post-stream reductions, Darcy K)."""
     import torch
 
@@ -343,9 +343,9 @@ def run_e2e_batch(windows, steps: int, graph_steps: int):
     d2h = len(windows) * (2 * nat.NRED + nat.NDIAG) * 8
     k_sum = 0.0
     t0 = time.perf_counter()
+    arrays = [w.particles for w in windows]
     for _ in range(steps):
-        for k, w in enumerate(windows):
-            b.set_particles(k, w.particles)
+        b.set_particles_all(arrays)
         st = b.step(1, nat.RUN_DIAG)
         k_sum += st[0].diag.permeability
     wall = time.perf_counter() - t0
@@ -354,7 +354,7 @@ def run_e2e_batch(windows, steps: int, graph_steps: int):
     torch.cuda.empty_cache()
     return {"value": round(cells * steps / wall / 1e6, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "finite": bool(np.isfinite(k_sum)),
-            "api": "C ABI psc_batch_set_particles (every window) + psc_batch_step(1, PSC_RUN_DIAG) per step: "
+            "api": "C ABI psc_batch_set_particles_all (every window) + psc_batch_step(1, PSC_RUN_DIAG) per step: "
                    "host particle arrays in, per-window diagnostics and Darcy K out, one persistent launch for "
                    "all windows", "steps": steps}
 

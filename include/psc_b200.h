@@ -487,6 +487,9 @@ int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_lau
 int psc_batch_destroy(psc_batch* b);
 /* Particles of window `win`; a changed array re-voxelises that window before the next step. */
 int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, int nparticles);
+/* psc_batch_set_particles for every window in one call: h_particles[k] is window k's [P_k][10]
+ * array (may be NULL when nparticles[k] is 0). */
+int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, const int* h_nparticles);
 /* nsteps steps of every active window.  PSC_RUN_DIAG: diagnostics and loads
  * of every window at the final step into h_status[nwin] (may be NULL). */
 int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_status);

@@ -200,6 +200,7 @@ SIGNATURES = {
     "psc_batch_create": (c_int, [POINTER(PscConfig), c_int, POINTER(PscLaunch), c_int, POINTER(c_void_p)]),
     "psc_batch_destroy": (c_int, [c_void_p]),
     "psc_batch_set_particles": (c_int, [c_void_p, c_int, c_void_p, c_int]),
+    "psc_batch_set_particles_all": (c_int, [c_void_p, POINTER(c_void_p), POINTER(c_int)]),
     "psc_batch_step": (c_int, [c_void_p, c_int, c_uint, POINTER(PscStatus)]),
     "psc_batch_converge": (c_int, [c_void_p, c_double, c_int, c_int, c_int, c_int, POINTER(PscStatus)]),
     "psc_batch_get_diag": (c_int, [c_void_p, c_int, POINTER(PscDiag)]),

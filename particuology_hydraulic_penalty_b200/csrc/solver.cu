@@ -1223,6 +1223,14 @@ int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, in
     return window_set_particles(*b->w[(size_t)win], h_particles, nparticles, b->stream, "psc_batch_set_particles");
 }
 
+int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, const int* h_nparticles) {
+    if (!b || !h_particles || !h_nparticles) return fail(PSC_E_INVALID, "psc_batch_set_particles_all: null argument");
+    DeviceScope ds(b->device);
+    for (size_t k = 0; k < b->w.size(); ++k)
+        PSC_TRY(window_set_particles(*b->w[k], h_particles[k], h_nparticles[k], b->stream, "psc_batch_set_particles_all"));
+    return PSC_OK;
+}
+
 int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_status) {
     if (!b) return fail(PSC_E_INVALID, "psc_batch_step: null handle");
     if (nsteps < 0) return fail(PSC_E_INVALID, "psc_batch_step: negative step count");

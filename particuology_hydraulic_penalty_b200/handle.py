@@ -174,6 +174,16 @@ class BatchHandle:
                   "psc_batch_set_particles")
         self.P[k] = int(arr.shape[0])
 
+    def set_particles_all(self, arrays) -> None:
+        """Every window's (P_k, 10) particle array in one call."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrays]
+        if len(arrs) != self.nwin:
+            raise ValueError(f"expected {self.nwin} particle arrays")
+        ptrs = (_VP * self.nwin)(*[a.ctypes.data if a.size else None for a in arrs])
+        counts = (ctypes.c_int * self.nwin)(*[int(a.shape[0]) for a in arrs])
+        nat.check(self._lib.psc_batch_set_particles_all(self._h, ptrs, counts), "psc_batch_set_particles_all")
+        self.P = [int(a.shape[0]) for a in arrs]
+
     def step(self, nsteps: int, flags: int = 0):
         nat.check(self._lib.psc_batch_step(self._h, int(nsteps), int(flags), self._status), "psc_batch_step")
         return self._status

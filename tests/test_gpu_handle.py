@@ -183,3 +183,22 @@ def test_batch_handle_converge_matches_python():
         if res["converged"][k]:
             assert st[k].steps_done == int(res["steps"][k])
         assert st[k].diag.permeability == res["permeability"][k]
+
+
+def test_batch_set_particles_all_equals_per_window():
+    from particuology_hydraulic_penalty_b200 import _native as nat
+
+    wins = _three()
+    a = _batch(wins)
+    b = _batch(wins)
+    moved = [w.particles.copy() for w in wins]
+    for m in moved:
+        m[:, 0] += 0.25
+    for k, m in enumerate(moved):
+        a.set_particles(k, m)
+    b.set_particles_all(moved)
+    a.step(3, nat.RUN_DIAG)
+    b.step(3, nat.RUN_DIAG)
+    for k in range(len(wins)):
+        assert np.array_equal(a.field(k, nat.FIELD_F), b.field(k, nat.FIELD_F))
+        assert np.array_equal(a.loads(k)[0], b.loads(k)[0])
