@@ -134,38 +134,6 @@ __device__ __forceinline__ int owner_of(const int64_t* off, int P, int64_t e) {
     return lo;
 }
 
-// owner_of for a whole block (block-uniform call): the largest p < P with
-// off[p] <= e, found by counting instead of a serial binary search -- the
-// owner is (number of p with off[p] <= e) - 1 because off is non-decreasing.
-// Ranges wider than 4 x blockDim are first narrowed by one sampled round.
-__device__ __forceinline__ int block_owner_of(const int64_t* off, int P, int64_t e) {
-    int lo = 0, hi = P;  // invariant: off[lo] <= e and (hi == P or off[hi] > e)
-    const int bd = (int)blockDim.x, tid = (int)threadIdx.x;
-    while (hi - lo > 1) {
-        const int len = hi - lo;
-        if (len <= 4 * bd) {
-            bool f[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int p = lo + tid + k * bd;
-                f[k] = p < hi && off[p] <= e;
-            }
-            int n = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) n += __syncthreads_count(f[k]);
-            return lo + n - 1;
-        }
-        const int p = lo + (int)(((int64_t)tid * len) / bd);
-        const int n = __syncthreads_count(off[p] <= e);  // >= 1: sample 0 is lo
-        const int i = n - 1;
-        const int nlo = lo + (int)(((int64_t)i * len) / bd);
-        const int nhi = i + 1 < bd ? lo + (int)(((int64_t)(i + 1) * len) / bd) : hi;
-        lo = nlo;
-        hi = nhi;
-    }
-    return lo;
-}
-
 struct EntryCell {
     int p;
     int32_t ix, iy, iz;
@@ -370,6 +338,41 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*s)[NV]) {
 
 constexpr int LOAD_THREADS = 256;
 
+// Descriptor of one load-reduction chunk, computed by k_chunk_desc (one
+// thread per chunk, so the lookups of many chunks overlap) into the chunk's
+// own partial row (6 doubles); the chunk's block reads it before it
+// overwrites the row with its sums.
+struct ChunkDesc {
+    int64_t e0, e1;       // entry range
+    int32_t p;            // particle
+    int32_t local0;       // e0 - ent_off[p]
+    int32_t x0, y0, z0;   // clipped box origin
+    int32_t ey, ez;       // box extents in y and z
+    int32_t pad;
+};
+static_assert(sizeof(ChunkDesc) == 6 * sizeof(double), "a chunk descriptor fills one partial row");
+
+__global__ void __launch_bounds__(256) k_chunk_desc(psc_geometry g, double* part) {
+    const int64_t C = g.totals[1];
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C; c += (int64_t)gridDim.x * blockDim.x) {
+        const int p = owner_of(g.chunk_off, g.nparticles, c);
+        const int64_t eb = g.ent_off[p];
+        ChunkDesc d;
+        d.e0 = eb + (c - g.chunk_off[p]) * g.chunk_entries;
+        d.e1 = min(d.e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
+        d.p = p;
+        d.local0 = (int32_t)(d.e0 - eb);
+        const int32_t* bb = g.bbox + (size_t)p * 6;
+        d.x0 = bb[0];
+        d.y0 = bb[1];
+        d.z0 = bb[2];
+        d.ey = bb[4];
+        d.ez = bb[5];
+        d.pad = 0;
+        *reinterpret_cast<ChunkDesc*>(part + c * 6) = d;
+    }
+}
+
 // The block's table of inside / S^3 for every sample count (S <= 16) holds
 // the exact IEEE quotients of psc3d.py:88, computed once per block.
 constexpr int LOAD_UNROLL = 4;
@@ -395,17 +398,16 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
     for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
     __syncthreads();
     for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
-        const int p = block_owner_of(g.chunk_off, g.nparticles, chunk);
-        const int64_t eb = g.ent_off[p];
-        const int64_t e0 = eb + (chunk - g.chunk_off[p]) * g.chunk_entries;
-        const int64_t e1 = min(e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
-        const double* q = g.particles + (size_t)p * PF;
-        const int32_t* bb = g.bbox + (size_t)p * 6;
-        const uint32_t ey = (uint32_t)bb[4], ez = (uint32_t)bb[5];
+        // every thread reads the chunk's descriptor; the block sum below (its barriers) comes before
+        // thread 0 overwrites the row with the chunk's sums
+        const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
+        const int64_t e0 = dsc.e0, e1 = dsc.e1;
+        const double* q = g.particles + (size_t)dsc.p * PF;
+        const uint32_t ey = (uint32_t)dsc.ey, ez = (uint32_t)dsc.ez;
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         if (e0 + threadIdx.x < e1) {
             // bbox-local coordinates of this thread's first entry, and the stride
-            const uint32_t local = (uint32_t)(e0 - eb) + threadIdx.x;
+            const uint32_t local = (uint32_t)dsc.local0 + threadIdx.x;
             const uint32_t eyz = ey * ez;
             uint32_t a = local / eyz;
             const uint32_t rem = local - a * eyz;
@@ -418,7 +420,7 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
             const double qx = q[0], qy = q[1], qz = q[2];
             // LOAD_UNROLL entries per pass: all their loads are issued together,
             // then accumulated in entry order (the order of a one-entry loop)
-            const uint32_t bx = (uint32_t)bb[0], by = (uint32_t)bb[1], bz = (uint32_t)bb[2];
+            const uint32_t bx = (uint32_t)dsc.x0, by = (uint32_t)dsc.y0, bz = (uint32_t)dsc.z0;
             for (int64_t e = e0 + threadIdx.x; e < e1; e += (int64_t)LOAD_UNROLL * blockDim.x) {
                 uint16_t cnt[LOAD_UNROLL];
                 uint32_t cx[LOAD_UNROLL], cy[LOAD_UNROLL], cz[LOAD_UNROLL];
@@ -671,6 +673,8 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
         const int64_t cap = (int64_t)sm_count() * 16;
         const unsigned grid = (unsigned)(g.capacity_chunks < cap ? g.capacity_chunks : cap);
         const size_t lut = (size_t)(g.subsamples * g.subsamples * g.subsamples + 1) * sizeof(double);
+        const int64_t cg = (g.capacity_chunks + 255) / 256;
+        k_chunk_desc<<<(unsigned)(cg < cap ? cg : cap), 256, 0, stream>>>(g, chunk_partials);
         if (imb_type == 0)
             k_loads_chunks<double><<<grid, LOAD_THREADS, lut, stream>>>(g, reinterpret_cast<const double*>(imb),
                                                                         chunk_partials);

@@ -358,9 +358,27 @@ int window_ensure_moments(Window& w, cudaStream_t s) {
 int window_set_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who) {
     if (P < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
     if (P > 0 && !hp) return fail(PSC_E_INVALID, std::string(who) + ": null particle array");
-    for (int64_t i = 0; i < (int64_t)P * 10; ++i)
-        if (!std::isfinite(hp[i])) return fail(PSC_E_INVALID, std::string(who) + ": particle state contains NaN or Inf");
-    const bool changed = P != w.P || (P > 0 && std::memcmp(w.hp.data(), hp, (size_t)P * 10 * sizeof(double)) != 0);
+    // one read pass: finiteness (the reference fails on NaN / Inf), change against the previous
+    // upload (bitwise, like memcmp) and whether any particle moves
+    const size_t n10 = (size_t)P * 10;
+    const bool same_size = P == w.P && w.hp.size() == n10;
+    bool finite = true, differs = !same_size, mv = false;
+    for (int p = 0; p < P; ++p) {
+        const double* q = hp + (size_t)p * 10;
+        for (int k = 0; k < 10; ++k) {
+            const double v = q[k];
+            finite = finite && std::isfinite(v);
+            if (k >= 4) mv = mv || v != 0.0;
+            if (same_size && !differs) {
+                uint64_t a, b;
+                std::memcpy(&a, &v, 8);
+                std::memcpy(&b, &w.hp[(size_t)p * 10 + k], 8);
+                differs = a != b;
+            }
+        }
+    }
+    if (!finite) return fail(PSC_E_INVALID, std::string(who) + ": particle state contains NaN or Inf");
+    const bool changed = differs;
     if (P != w.P || !w.particles.p) {
         PSC_CUDA(cudaEventSynchronize(w.upload_done), who);  // the old staging buffer may still be read
         PSC_CUDA(w.particles.ensure((int64_t)P * 10, true, s), who);
@@ -388,13 +406,6 @@ int window_set_particles(Window& w, const double* hp, int P, cudaStream_t s, con
         PSC_CUDA(cudaEventRecord(w.upload_done, s), who);
     }
     if (changed) ++w.pversion;
-    bool mv = false;
-    for (int p = 0; p < P && !mv; ++p)
-        for (int k = 4; k < 10; ++k)
-            if (hp[(size_t)p * 10 + k] != 0.0) {
-                mv = true;
-                break;
-            }
     if (mv != w.moving) {
         w.moving = mv;
         w.touch();
