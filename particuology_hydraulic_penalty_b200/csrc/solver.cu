@@ -220,6 +220,7 @@ struct Window {
     HArray<double> pinned;
     cudaEvent_t upload_done = nullptr;
     DArray<double> particles;
+    const double* ext_particles = nullptr;  // a batch's shared upload buffer (psc_batch_set_particles_all)
     DArray<int32_t> bbox;
     DArray<int64_t> ent_off, chunk_off, totals;
     DArray<uint16_t> ent_cnt, cl_cnt;
@@ -259,7 +260,7 @@ struct Window {
         g.chunk_entries = kChunkEntries;
         g.capacity_entries = cap_entries;
         g.capacity_chunks = cap_chunks;
-        g.particles = P ? particles.p : nullptr;
+        g.particles = P ? (ext_particles ? ext_particles : particles.p) : nullptr;
         g.bbox = bbox.p;
         g.ent_off = ent_off.p;
         g.chunk_off = chunk_off.p;
@@ -355,7 +356,9 @@ int window_ensure_moments(Window& w, cudaStream_t s) {
     return PSC_OK;
 }
 
-int window_set_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who) {
+// Validation and bookkeeping of a new particle state (no upload): per-P
+// buffers, the host copy, the change version and the moving flag.
+int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who) {
     if (P < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
     if (P > 0 && !hp) return fail(PSC_E_INVALID, std::string(who) + ": null particle array");
     // one read pass: finiteness (the reference fails on NaN / Inf), change against the previous
@@ -396,6 +399,17 @@ int window_set_particles(Window& w, const double* hp, int P, cudaStream_t s, con
         w.P = P;
     }
     w.hp.assign(hp, hp + (size_t)P * 10);
+    if (changed) ++w.pversion;
+    if (mv != w.moving) {
+        w.moving = mv;
+        w.touch();
+    }
+    return PSC_OK;
+}
+
+int window_set_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who) {
+    PSC_TRY(window_accept_particles(w, hp, P, s, who));
+    w.ext_particles = nullptr;
     if (P > 0) {
         // every step reads the caller's current state (psc3d.py re-reads the
         // Particle3D objects each call); staged through page-locked memory
@@ -404,11 +418,6 @@ int window_set_particles(Window& w, const double* hp, int P, cudaStream_t s, con
         PSC_CUDA(cudaMemcpyAsync(w.particles.p, w.pinned.p, (size_t)P * 10 * sizeof(double), cudaMemcpyHostToDevice, s),
                  who);
         PSC_CUDA(cudaEventRecord(w.upload_done, s), who);
-    }
-    if (changed) ++w.pversion;
-    if (mv != w.moving) {
-        w.moving = mv;
-        w.touch();
     }
     return PSC_OK;
 }
@@ -977,10 +986,14 @@ struct psc_batch {
     std::vector<uint64_t> built_desc;  // descriptor versions the tables were built from
     bool moving_any = false;
     Lanes lanes;  // particle loads of the windows beside the post-stream reduction pass
+    HArray<double> up_host;    // every window's particles, staged for one upload
+    DArray<double> up_dev;
+    cudaEvent_t up_done = nullptr;
 
     ~psc_batch() {
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
+        if (up_done) cudaEventDestroy(up_done);
     }
 };
 
@@ -1206,6 +1219,7 @@ int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_lau
         if (e == cudaSuccess) e = b->diag.ensure((int64_t)nwin * PSC_NDIAG, true, b->stream);
         if (e == cudaSuccess) e = b->host.ensure((int64_t)nwin * kOutLen);
         if (e == cudaSuccess) e = b->lanes.init(Lanes::kMax);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->up_done, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) st = cuda_fail(e, "psc_batch_create");
     }
@@ -1237,8 +1251,34 @@ int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, in
 int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, const int* h_nparticles) {
     if (!b || !h_particles || !h_nparticles) return fail(PSC_E_INVALID, "psc_batch_set_particles_all: null argument");
     DeviceScope ds(b->device);
-    for (size_t k = 0; k < b->w.size(); ++k)
-        PSC_TRY(window_set_particles(*b->w[k], h_particles[k], h_nparticles[k], b->stream, "psc_batch_set_particles_all"));
+    const char* who = "psc_batch_set_particles_all";
+    const size_t nwin = b->w.size();
+    int64_t total = 0;
+    for (size_t k = 0; k < nwin; ++k) {
+        if (h_nparticles[k] < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
+        total += (int64_t)h_nparticles[k] * 10;
+    }
+    // one staging buffer and one host-to-device copy for all windows
+    PSC_CUDA(cudaEventSynchronize(b->up_done), who);  // the previous upload has left the staging buffer
+    if (b->up_dev.n < total) {
+        PSC_CUDA(cudaStreamSynchronize(b->stream), who);  // kernels may still read the old buffer
+        PSC_CUDA(b->up_dev.ensure(total + total / 4 + 64, false, b->stream), who);
+    }
+    PSC_CUDA(b->up_host.ensure(b->up_dev.n), who);
+    int64_t off = 0;
+    for (size_t k = 0; k < nwin; ++k) {
+        Window& w = *b->w[k];
+        const int P = h_nparticles[k];
+        PSC_TRY(window_accept_particles(w, h_particles[k], P, b->stream, who));
+        if (P > 0) std::memcpy(b->up_host.p + off, h_particles[k], (size_t)P * 10 * sizeof(double));
+        w.ext_particles = b->up_dev.p + off;
+        off += (int64_t)P * 10;
+    }
+    if (total > 0)
+        PSC_CUDA(cudaMemcpyAsync(b->up_dev.p, b->up_host.p, (size_t)total * sizeof(double), cudaMemcpyHostToDevice,
+                                 b->stream),
+                 who);
+    PSC_CUDA(cudaEventRecord(b->up_done, b->stream), who);
     return PSC_OK;
 }
 
