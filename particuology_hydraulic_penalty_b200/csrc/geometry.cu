@@ -375,11 +375,19 @@ __global__ void __launch_bounds__(256) k_chunk_desc(psc_geometry g, double* part
 
 // The block's table of inside / S^3 for every sample count (S <= 16) holds
 // the exact IEEE quotients of psc3d.py:88, computed once per block.
-constexpr int LOAD_UNROLL = 4;
+// Entries whose loads one thread issues together per pass.  The kernel is
+// latency-bound, and resident warps help more than loads per thread: on the
+// 160^3 window (6.9 M entries) one entry per pass at four blocks per SM took
+// 71.5 us, two at four 82 us, four at three 91 us, eight at two 107 us; fewer
+// than 64 registers spill and lose again (78-98 us).
+#ifndef PSC_LOADS_UNROLL
+#define PSC_LOADS_UNROLL 1
+#endif
+constexpr int LOAD_UNROLL = PSC_LOADS_UNROLL;
 // Resident blocks per SM the register allocation of k_loads_chunks aims for
 // (the kernel is latency-bound: more resident warps, more loads in flight).
 #ifndef PSC_LOADS_MIN_BLOCKS
-#define PSC_LOADS_MIN_BLOCKS 3
+#define PSC_LOADS_MIN_BLOCKS 4
 #endif
 
 // One block per chunk of one particle's bbox entries.  A thread visits the

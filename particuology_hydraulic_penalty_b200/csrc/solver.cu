@@ -361,26 +361,21 @@ int window_ensure_moments(Window& w, cudaStream_t s) {
 int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who) {
     if (P < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
     if (P > 0 && !hp) return fail(PSC_E_INVALID, std::string(who) + ": null particle array");
-    // one read pass: finiteness (the reference fails on NaN / Inf), change against the previous
-    // upload (bitwise, like memcmp) and whether any particle moves
+    // unchanged (bitwise) since the last upload: nothing to validate or record again
     const size_t n10 = (size_t)P * 10;
     const bool same_size = P == w.P && w.hp.size() == n10;
-    bool finite = true, differs = !same_size, mv = false;
-    for (int p = 0; p < P; ++p) {
-        const double* q = hp + (size_t)p * 10;
-        for (int k = 0; k < 10; ++k) {
-            const double v = q[k];
-            finite = finite && std::isfinite(v);
-            if (k >= 4) mv = mv || v != 0.0;
-            if (same_size && !differs) {
-                uint64_t a, b;
-                std::memcpy(&a, &v, 8);
-                std::memcpy(&b, &w.hp[(size_t)p * 10 + k], 8);
-                differs = a != b;
-            }
-        }
+    const bool differs = !same_size || (n10 && std::memcmp(w.hp.data(), hp, n10 * sizeof(double)) != 0);
+    bool mv = w.moving;
+    if (differs) {
+        // finiteness (the reference fails on NaN / Inf) as one sum: v * 0 is NaN exactly for
+        // non-finite v; and whether any particle moves
+        double probe = 0.0;
+        mv = false;
+        for (size_t i = 0; i < n10; ++i) probe += hp[i] * 0.0;
+        for (int p = 0; p < P && !mv; ++p)
+            for (int k = 4; k < 10; ++k) mv = mv || hp[(size_t)p * 10 + k] != 0.0;
+        if (!(probe == 0.0)) return fail(PSC_E_INVALID, std::string(who) + ": particle state contains NaN or Inf");
     }
-    if (!finite) return fail(PSC_E_INVALID, std::string(who) + ": particle state contains NaN or Inf");
     const bool changed = differs;
     if (P != w.P || !w.particles.p) {
         PSC_CUDA(cudaEventSynchronize(w.upload_done), who);  // the old staging buffer may still be read
@@ -398,8 +393,10 @@ int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, 
         }
         w.P = P;
     }
-    w.hp.assign(hp, hp + (size_t)P * 10);
-    if (changed) ++w.pversion;
+    if (changed) {
+        w.hp.assign(hp, hp + (size_t)P * 10);
+        ++w.pversion;
+    }
     if (mv != w.moving) {
         w.moving = mv;
         w.touch();
