@@ -16,8 +16,13 @@ from . import _native as nat
 _VP = ctypes.c_void_p
 
 
+def _addr(a: np.ndarray) -> int:
+    # the array interface is much cheaper per call than ndarray.ctypes (which builds a helper object)
+    return a.__array_interface__["data"][0]
+
+
 def _ptr(a: np.ndarray):
-    return a.ctypes.data_as(_VP)
+    return _VP(_addr(a))
 
 
 def _diag_dict(d: nat.PscDiag) -> dict:
@@ -179,7 +184,7 @@ class BatchHandle:
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrays]
         if len(arrs) != self.nwin:
             raise ValueError(f"expected {self.nwin} particle arrays")
-        ptrs = (_VP * self.nwin)(*[a.ctypes.data if a.size else None for a in arrs])
+        ptrs = (_VP * self.nwin)(*[_addr(a) if a.size else None for a in arrs])
         counts = (ctypes.c_int * self.nwin)(*[int(a.shape[0]) for a in arrs])
         nat.check(self._lib.psc_batch_set_particles_all(self._h, ptrs, counts), "psc_batch_set_particles_all")
         self.P = [int(a.shape[0]) for a in arrs]
