@@ -471,6 +471,26 @@ int psc_get_diag(psc_solver* h, psc_diag* h_diag);
 int psc_get_sparse_alpha(psc_solver* h, int64_t* h_offsets, int64_t* h_ids, double* h_vals, int64_t capacity);
 /* Particle count and lattice cells of the handle. */
 int psc_solver_info(psc_solver* h, int* h_nparticles, int64_t* h_cells);
+/* ---- adjoint handle: K and dK/d(x, y, z, r) of every particle (no counterpart
+ * in the reference) ---------------------------------------------------------
+ * One static periodic BGK window in PSC_STORE_F32 or F64 deviation storage,
+ * run from rest for `steps` steps with the smooth solid fraction (each
+ * sub-sample contributes sigma((r - d) / smooth_eps)); checkpoints every
+ * `checkpoint_every` steps; the backward pass recomputes each segment from its
+ * checkpoint and runs the reverse steps (psc_adjoint_seed / psc_adjoint_step)
+ * and the geometry gradient (psc_adjoint_geometry_grad).  K = nu (sum
+ * (1 - solid) u . d) / N / |F|, d = F / |F|.  Device memory: the two
+ * population buffers, ceil(steps / checkpoint_every) checkpoints and
+ * checkpoint_every recomputed states. */
+typedef struct psc_adjoint psc_adjoint;
+int psc_adjoint_create(const psc_config* h_cfg, double smooth_eps, int steps, int checkpoint_every,
+                       psc_adjoint** out);
+int psc_adjoint_destroy(psc_adjoint* a);
+/* K after the forward run with h_particles [P][10] (velocities ignored: static particles). */
+int psc_adjoint_forward(psc_adjoint* a, const double* h_particles, int nparticles, double* h_K);
+/* h_grad [P][4] = dK/d(x, y, z, r) of every particle for the last forward run. */
+int psc_adjoint_backward(psc_adjoint* a, double* h_grad);
+
 /* sizeof of the handle-layer structs as compiled into the library. */
 size_t psc_config_size(void);
 size_t psc_diag_size(void);

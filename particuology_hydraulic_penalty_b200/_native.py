@@ -194,6 +194,10 @@ SIGNATURES = {
     "psc_accumulate_particle_loads": (c_int, [c_void_p]),
     "psc_get_sparse_alpha": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64]),
     "psc_solver_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int64)]),
+    "psc_adjoint_create": (c_int, [POINTER(PscConfig), c_double, c_int, c_int, POINTER(c_void_p)]),
+    "psc_adjoint_destroy": (c_int, [c_void_p]),
+    "psc_adjoint_forward": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_double)]),
+    "psc_adjoint_backward": (c_int, [c_void_p, c_void_p]),
     "psc_config_size": (c_size_t, []),
     "psc_diag_size": (c_size_t, []),
     "psc_status_size": (c_size_t, []),

@@ -229,6 +229,9 @@ struct Window {
     DArray<uint8_t> level;
     DArray<unsigned char> scan_tmp;
     DArray<double> chunk_partials;
+    double smooth_eps = 0.0;  // > 0: smooth solid fraction (the adjoint's differentiable surrogate)
+    DArray<double> ent_alpha;
+    DArray<int32_t> cl_ent;
     int64_t cap_entries = 0, cap_chunks = 0, n_entries = 0, n_chunks = 0;
     DArray<double> forces, torques;
     uint64_t pversion = 1, built_version = 0, us_version = 0;
@@ -274,9 +277,9 @@ struct Window {
         g.solid = solid.p;
         g.level = want_level ? level.p : nullptr;
         g.scan_tmp = scan_tmp.p;
-        g.smooth_eps = 0.0;
-        g.ent_alpha = nullptr;
-        g.cl_ent = nullptr;
+        g.smooth_eps = smooth_eps;
+        g.ent_alpha = smooth_eps > 0.0 && cap_entries ? ent_alpha.p : nullptr;
+        g.cl_ent = smooth_eps > 0.0 && cap_entries ? cl_ent.p : nullptr;
         return g;
     }
 
@@ -317,7 +320,7 @@ int window_init(Window& w, const psc_config& c, cudaStream_t s, const char* who)
     w.elem = store_elem_bytes(c.store);
     w.fdouble = c.store == PSC_STORE_F64_EXACT || c.store == PSC_STORE_F64;
     w.scale = c.store_scale > 0.0 ? c.store_scale : default_store_scale(c.store);
-    w.want_level = c.store != PSC_STORE_F64_EXACT;
+    w.want_level = c.store != PSC_STORE_F64_EXACT && !(w.smooth_eps > 0.0);
     const int64_t N = w.N;
     PSC_CUDA(w.f[0].ensure(kQ * N * w.elem, false, s), who);
     PSC_CUDA(w.f[1].ensure(kQ * N * w.elem, false, s), who);
@@ -434,6 +437,10 @@ int window_rebuild(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* 
         PSC_CUDA(w.ent_cnt.ensure(cap, false, s), who);
         PSC_CUDA(w.cl_pid.ensure(cap, false, s), who);
         PSC_CUDA(w.cl_cnt.ensure(cap, false, s), who);
+        if (w.smooth_eps > 0.0) {
+            PSC_CUDA(w.ent_alpha.ensure(cap, false, s), who);
+            PSC_CUDA(w.cl_ent.ensure(cap, false, s), who);
+        }
         w.cap_entries = cap;
     }
     if (w.n_chunks > w.cap_chunks) {
@@ -1438,6 +1445,230 @@ int psc_batch_get_fields(psc_batch* b, int win, int which, double* h_dst) {
     Window& w = *b->w[(size_t)win];
     batch_sync_cur(*b);
     return window_get_field(w, which, h_dst, b->stream, b->tot, "psc_batch_get_fields");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// adjoint of the permeability (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+struct psc_adjoint {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Window w;  // smooth geometry, PSC_STORE_F32 / F64 deviation storage
+    HArray<int64_t> tot;
+    HArray<double> host;
+    int steps = 0, every = 0;
+    std::vector<std::unique_ptr<DArray<unsigned char>>> ckpt;  // S_t at t = 0, every, 2 every, ...
+    DArray<unsigned char> states;                              // one segment's recomputed states
+    DArray<psc_window> seg_tab;                                // their step descriptors
+    DArray<unsigned char> lam[2];
+    DArray<double> dKdB, dKds, red, gpart, grad;
+    bool forward_done = false;
+    double K = 0.0;
+};
+
+namespace psc {
+namespace {
+
+size_t adj_state_bytes(const psc_adjoint& a) { return (size_t)19 * a.w.N * a.w.elem; }
+
+psc_adjoint_args adj_args(const psc_adjoint& a) {
+    const Window& w = a.w;
+    const double* F = w.cfg.force;
+    const double fmag = std::sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]);
+    psc_adjoint_args r{};
+    r.nx = w.cfg.nx;
+    r.ny = w.cfg.ny;
+    r.nz = w.cfg.nz;
+    r.store = w.cfg.store;
+    r.tau = w.cfg.tau;
+    r.force[0] = F[0];
+    r.force[1] = F[1];
+    r.force[2] = F[2];
+    r.kappa = (w.cfg.tau - 0.5) / 3.0 / (fmag * (double)w.N);
+    r.dir[0] = F[0] / fmag;
+    r.dir[1] = F[1] / fmag;
+    r.dir[2] = F[2] / fmag;
+    r.solid = w.solid.p;
+    r.dKdB = a.dKdB.p;
+    r.dKdsolid = a.dKds.p;
+    return r;
+}
+
+// States S_t0 .. S_{t1-1} of one segment, recomputed from its checkpoint.
+int adj_segment(psc_adjoint& a, int t0, int t1) {
+    Window& w = a.w;
+    cudaStream_t s = a.stream;
+    const size_t sb = adj_state_bytes(a);
+    const int L = t1 - t0;
+    PSC_CUDA(cudaMemcpyAsync(a.states.p, a.ckpt[(size_t)(t0 / a.every)]->p, sb, cudaMemcpyDeviceToDevice, s),
+             "psc_adjoint_backward");
+    if (L < 2) return PSC_OK;
+    std::vector<psc_window> tab((size_t)(L - 1));
+    for (int k = 0; k < L - 1; ++k) {
+        psc_window d = w.descriptor(0);
+        d.f_src = a.states.p + (size_t)k * sb;
+        d.f_dst = a.states.p + (size_t)(k + 1) * sb;
+        d.imb = nullptr;
+        d.moments = nullptr;
+        d.flags &= ~PSC_WIN_MOVING;
+        int64_t total = 0;
+        PSC_TRY(psc_plan_tiles(&d, 1, 0, &total));
+        tab[(size_t)k] = d;
+    }
+    PSC_CUDA(a.seg_tab.ensure(L - 1, false, s), "psc_adjoint_backward");
+    PSC_CUDA(cudaMemcpyAsync(a.seg_tab.p, tab.data(), (size_t)(L - 1) * sizeof(psc_window), cudaMemcpyHostToDevice, s),
+             "psc_adjoint_backward");
+    psc_launch c = {0, 1, PSC_KERNEL_AUTO, 0, 0};
+    for (int k = 0; k < L - 1; ++k)
+        PSC_TRY(psc_step_windows_ex(w.cfg.store, a.seg_tab.p + k, 1, tab[(size_t)k].tile_count, PSC_STEP_COLLIDE, &c, s));
+    PSC_CUDA(cudaStreamSynchronize(s), "psc_adjoint_backward");  // tab lives on this frame
+    return PSC_OK;
+}
+
+}  // namespace
+}  // namespace psc
+
+extern "C" {
+
+int psc_adjoint_create(const psc_config* h_cfg, double smooth_eps, int steps, int checkpoint_every,
+                       psc_adjoint** out) {
+    if (!h_cfg || !out) return fail(PSC_E_INVALID, "psc_adjoint_create: null argument");
+    *out = nullptr;
+    PSC_TRY(check_config(*h_cfg, "psc_adjoint_create"));
+    if (h_cfg->store != PSC_STORE_F32 && h_cfg->store != PSC_STORE_F64)
+        return fail(PSC_E_UNSUPPORTED, "psc_adjoint_create: the adjoint runs in PSC_STORE_F32 or PSC_STORE_F64");
+    if (!(smooth_eps > 0.0) || !std::isfinite(smooth_eps))
+        return fail(PSC_E_INVALID, "psc_adjoint_create: smooth_eps must be > 0");
+    if (steps < 1 || checkpoint_every < 1) return fail(PSC_E_INVALID, "psc_adjoint_create: steps and checkpoint_every must be >= 1");
+    if (!(h_cfg->tau > 0.5)) return fail(PSC_E_INVALID, "psc_adjoint_create: tau must exceed 0.5");
+    if (h_cfg->tau_minus > 0.0 || h_cfg->open_x)
+        return fail(PSC_E_UNSUPPORTED, "psc_adjoint_create: the adjoint runs BGK on periodic windows");
+    const double* F = h_cfg->force;
+    if (!(F[0] * F[0] + F[1] * F[1] + F[2] * F[2] > 0.0))
+        return fail(PSC_E_INVALID, "psc_adjoint_create: the permeability needs a non-zero body force");
+    DeviceScope ds(h_cfg->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_adjoint_create: cudaSetDevice");
+    std::unique_ptr<psc_adjoint> a(new (std::nothrow) psc_adjoint());
+    if (!a) return fail(PSC_E_CAPACITY, "psc_adjoint_create: out of host memory");
+    a->device = h_cfg->device;
+    a->steps = steps;
+    a->every = checkpoint_every;
+    if (h_cfg->stream) {
+        a->stream = as_stream(h_cfg->stream);
+    } else {
+        PSC_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking), "psc_adjoint_create");
+        a->own_stream = true;
+    }
+    psc_config c = *h_cfg;
+    c.static_geometry = 1;
+    a->w.smooth_eps = smooth_eps;
+    int st = window_init(a->w, c, a->stream, "psc_adjoint_create");
+    if (st == PSC_OK) st = window_set_particles(a->w, nullptr, 0, a->stream, "psc_adjoint_create");
+    if (st != PSC_OK) {
+        psc_adjoint_destroy(a.release());
+        return st;
+    }
+    *out = a.release();
+    return PSC_OK;
+}
+
+int psc_adjoint_destroy(psc_adjoint* a) {
+    if (!a) return PSC_OK;
+    DeviceScope ds(a->device);
+    cudaStreamSynchronize(a->stream);
+    cudaStream_t s = a->stream;
+    bool own = a->own_stream;
+    delete a;
+    if (own) cudaStreamDestroy(s);
+    return PSC_OK;
+}
+
+int psc_adjoint_forward(psc_adjoint* a, const double* h_particles, int nparticles, double* h_K) {
+    if (!a || !h_K) return fail(PSC_E_INVALID, "psc_adjoint_forward: null argument");
+    DeviceScope ds(a->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_adjoint_forward: cudaSetDevice");
+    Window& w = a->w;
+    cudaStream_t s = a->stream;
+    const char* who = "psc_adjoint_forward";
+    // the particles are static for the run: their velocities do not enter
+    PSC_TRY(window_set_particles(w, h_particles, nparticles, s, who));
+    PSC_TRY(window_rebuild(w, s, a->tot, who));
+    if (w.moving) {
+        w.moving = false;
+        w.touch();
+    }
+    PSC_TRY(psc_init_equilibrium(w.cfg.store, w.scale, w.f[0].p, w.N, s));
+    w.cur = 0;
+    const size_t sb = adj_state_bytes(*a);
+    const int nck = (a->steps + a->every - 1) / a->every;
+    while ((int)a->ckpt.size() < nck) a->ckpt.emplace_back(new DArray<unsigned char>());
+    for (int t = 0; t < a->steps; ++t) {
+        if (t % a->every == 0) {
+            DArray<unsigned char>& ck = *a->ckpt[(size_t)(t / a->every)];
+            PSC_CUDA(ck.ensure((int64_t)sb, false, s), who);
+            PSC_CUDA(cudaMemcpyAsync(ck.p, w.f[w.cur].p, sb, cudaMemcpyDeviceToDevice, s), who);
+        }
+        PSC_TRY(launch_solo(w, PSC_STEP_COLLIDE, s));
+        w.cur ^= 1;
+    }
+    PSC_TRY(launch_solo(w, PSC_STEP_REDUCE, s));
+    PSC_CUDA(a->red.ensure(PSC_NRED, true, s), who);
+    PSC_TRY(psc_reduce_windows(w.solo[w.cur].p, 1, a->red.p, s));
+    PSC_CUDA(a->host.ensure(PSC_NRED), who);
+    PSC_CUDA(cudaMemcpyAsync(a->host.p, a->red.p, PSC_NRED * sizeof(double), cudaMemcpyDeviceToHost, s), who);
+    PSC_CUDA(cudaStreamSynchronize(s), who);
+    a->K = row_permeability(w, a->host.p);
+    a->forward_done = true;
+    *h_K = a->K;
+    return PSC_OK;
+}
+
+int psc_adjoint_backward(psc_adjoint* a, double* h_grad) {
+    if (!a) return fail(PSC_E_INVALID, "psc_adjoint_backward: null handle");
+    if (!a->forward_done) return fail(PSC_E_INVALID, "psc_adjoint_backward: call psc_adjoint_forward first");
+    Window& w = a->w;
+    if (w.P > 0 && !h_grad) return fail(PSC_E_INVALID, "psc_adjoint_backward: null output");
+    DeviceScope ds(a->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_adjoint_backward: cudaSetDevice");
+    cudaStream_t s = a->stream;
+    const char* who = "psc_adjoint_backward";
+    const size_t sb = adj_state_bytes(*a);
+    PSC_CUDA(a->lam[0].ensure((int64_t)sb, false, s), who);
+    PSC_CUDA(a->lam[1].ensure((int64_t)sb, false, s), who);
+    PSC_CUDA(a->dKdB.ensure(w.N, false, s), who);
+    PSC_CUDA(a->dKds.ensure(w.N, false, s), who);
+    PSC_CUDA(cudaMemsetAsync(a->dKdB.p, 0, (size_t)w.N * 8, s), who);
+    PSC_CUDA(cudaMemsetAsync(a->dKds.p, 0, (size_t)w.N * 8, s), who);
+    PSC_CUDA(a->states.ensure((int64_t)sb * std::min(a->every, a->steps), false, s), who);
+    psc_adjoint_args args = adj_args(*a);
+    args.state = w.f[w.cur].p;
+    args.lam_out = a->lam[0].p;
+    PSC_TRY(psc_adjoint_seed(&args, s));
+    int cur = 0;
+    const int nseg = (a->steps + a->every - 1) / a->every;
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        const int t0 = seg * a->every;
+        const int t1 = std::min(t0 + a->every, a->steps);
+        PSC_TRY(adj_segment(*a, t0, t1));
+        for (int t = t1 - 1; t >= t0; --t) {
+            args.state = a->states.p + (size_t)(t - t0) * sb;
+            args.lam_in = a->lam[cur].p;
+            args.lam_out = a->lam[1 - cur].p;
+            PSC_TRY(psc_adjoint_step(&args, s));
+            cur = 1 - cur;
+        }
+    }
+    psc_geometry g = w.geometry();
+    PSC_CUDA(a->gpart.ensure(std::max<int64_t>(w.cap_chunks, 1) * 4, false, s), who);
+    PSC_CUDA(a->grad.ensure((int64_t)std::max(w.P, 1) * 4, true, s), who);
+    PSC_TRY(psc_adjoint_geometry_grad(&g, &args, a->gpart.p, a->grad.p, s));
+    if (w.P > 0)
+        PSC_CUDA(cudaMemcpyAsync(h_grad, a->grad.p, (size_t)w.P * 4 * sizeof(double), cudaMemcpyDeviceToHost, s), who);
+    PSC_CUDA(cudaStreamSynchronize(s), who);
+    return PSC_OK;
 }
 
 }  // extern "C"

@@ -217,4 +217,39 @@ class BatchHandle:
         return out
 
 
+class AdjointHandle:
+    """One ``psc_adjoint``: K of a static window and dK/d(x, y, z, r) of every particle (native runtime)."""
+
+    def __init__(self, cfg: nat.PscConfig, smooth_eps: float = 0.05, steps: int = 2000, checkpoint_every: int = 100):
+        self._lib = nat.load()
+        self._h = _VP()
+        nat.call("psc_adjoint_create", ctypes.byref(cfg), float(smooth_eps), int(steps), int(checkpoint_every),
+                 ctypes.byref(self._h))
+        self.P = 0
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            self._lib.psc_adjoint_destroy(self._h)
+        self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, particles: np.ndarray) -> float:
+        arr = np.ascontiguousarray(particles, dtype=np.float64)
+        K = ctypes.c_double(0.0)
+        nat.check(self._lib.psc_adjoint_forward(self._h, _ptr(arr), int(arr.shape[0]), ctypes.byref(K)),
+                  "psc_adjoint_forward")
+        self.P = int(arr.shape[0])
+        return float(K.value)
+
+    def backward(self) -> np.ndarray:
+        g = np.zeros((self.P, 4))
+        nat.check(self._lib.psc_adjoint_backward(self._h, _ptr(g) if self.P else None), "psc_adjoint_backward")
+        return g
+
+
 diag_dict = _diag_dict
