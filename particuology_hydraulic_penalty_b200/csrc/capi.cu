@@ -278,6 +278,11 @@ int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb,
         return fail(PSC_E_INVALID, "psc_particle_loads: null array");
     if (h_geo->nparticles > 0 && h_geo->capacity_chunks > 0 && !chunk_partials)
         return fail(PSC_E_INVALID, "psc_particle_loads: null chunk partials");
+    // the entry gathers are asynchronous copies of whole elements (counts as aligned pairs)
+    if (h_geo->nparticles > 0 &&
+        ((uintptr_t)h_geo->ent_cnt % 4 || (uintptr_t)h_geo->alpha_sum % 8 || (uintptr_t)imb % (imb_type == 0 ? 8 : 4)))
+        return fail(PSC_E_INVALID,
+                    "psc_particle_loads: ent_cnt must be 4-byte aligned, alpha_sum and the IMB field element-aligned");
     cudaError_t e = launch_particle_loads(*h_geo, imb_type, imb, chunk_partials, imb_sums, forces, torques, diag,
                                           as_stream(stream));
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_particle_loads");

@@ -352,55 +352,182 @@ struct ChunkDesc {
 };
 static_assert(sizeof(ChunkDesc) == 6 * sizeof(double), "a chunk descriptor fills one partial row");
 
+__device__ __forceinline__ ChunkDesc make_chunk_desc(const psc_geometry& g, int64_t c) {
+    const int p = owner_of(g.chunk_off, g.nparticles, c);
+    const int64_t eb = g.ent_off[p];
+    ChunkDesc d;
+    d.e0 = eb + (c - g.chunk_off[p]) * g.chunk_entries;
+    d.e1 = min(d.e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
+    d.p = p;
+    d.local0 = (int32_t)(d.e0 - eb);
+    const int32_t* bb = g.bbox + (size_t)p * 6;
+    d.x0 = bb[0];
+    d.y0 = bb[1];
+    d.z0 = bb[2];
+    d.ey = bb[4];
+    d.ez = bb[5];
+    d.pad = 0;
+    return d;
+}
+
 __global__ void __launch_bounds__(256) k_chunk_desc(psc_geometry g, double* part) {
     const int64_t C = g.totals[1];
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C; c += (int64_t)gridDim.x * blockDim.x) {
-        const int p = owner_of(g.chunk_off, g.nparticles, c);
-        const int64_t eb = g.ent_off[p];
-        ChunkDesc d;
-        d.e0 = eb + (c - g.chunk_off[p]) * g.chunk_entries;
-        d.e1 = min(d.e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
-        d.p = p;
-        d.local0 = (int32_t)(d.e0 - eb);
-        const int32_t* bb = g.bbox + (size_t)p * 6;
-        d.x0 = bb[0];
-        d.y0 = bb[1];
-        d.z0 = bb[2];
-        d.ey = bb[4];
-        d.ez = bb[5];
-        d.pad = 0;
-        *reinterpret_cast<ChunkDesc*>(part + c * 6) = d;
-    }
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C; c += (int64_t)gridDim.x * blockDim.x)
+        *reinterpret_cast<ChunkDesc*>(part + c * 6) = make_chunk_desc(g, c);
 }
 
 // The block's table of inside / S^3 for every sample count (S <= 16) holds
 // the exact IEEE quotients of psc3d.py:88, computed once per block.
-// Entries whose loads one thread issues together per pass.  The kernel is
-// latency-bound, and resident warps help more than loads per thread: on the
-// 160^3 window (6.9 M entries) one entry per pass at four blocks per SM took
-// 71.5 us, two at four 82 us, four at three 91 us, eight at two 107 us; fewer
-// than 64 registers spill and lose again (78-98 us).
-#ifndef PSC_LOADS_UNROLL
-#define PSC_LOADS_UNROLL 1
+//
+// The gathers are latency-bound: an entry's five loads (count, alpha sum,
+// three IMB components) go to cells spread over its bounding box, and with
+// the loads of one pass per thread in flight the kernel kept DRAM at 13 % of
+// its bandwidth (ncu: 55 % of stalls on long scoreboard).  So each thread
+// copies the data of its entries LOAD_STAGES - 1 passes ahead into its own
+// shared-memory slots (cp.async, no registers held) and computes from there;
+// the arithmetic and its order per thread are those of a one-entry loop.
+// On the 24-window batch (57.5 M entries) the all-windows chunk kernel took
+// 504 us with four stages against 581 us with the loads in registers; three
+// stages ran as fast as four, two slower than none.  What is left is issue-
+// and conversion-bound (FP64 division and conversions per entry): exact
+// integer-path conversions cut the conversion-unit load but added more
+// instructions than they saved.
+#ifndef PSC_LOADS_STAGES
+#define PSC_LOADS_STAGES 4
 #endif
-constexpr int LOAD_UNROLL = PSC_LOADS_UNROLL;
-// Resident blocks per SM the register allocation of k_loads_chunks aims for
-// (the kernel is latency-bound: more resident warps, more loads in flight).
+constexpr int LOAD_STAGES = PSC_LOADS_STAGES;
+static_assert(LOAD_STAGES >= 2, "the staging ring needs two slots");
+// Resident blocks per SM the register allocation of the chunk kernels aims for.
 #ifndef PSC_LOADS_MIN_BLOCKS
-#define PSC_LOADS_MIN_BLOCKS 4
+#define PSC_LOADS_MIN_BLOCKS 3
 #endif
 
-// One block per chunk of one particle's bbox entries.  A thread visits the
+// One block's staging ring, structure of arrays over the threads (thread t
+// owns column t of every row: no bank conflicts, no barriers).
+template <typename I>
+struct LoadRing {
+    double alpha[LOAD_STAGES][LOAD_THREADS];
+    I imb[LOAD_STAGES][3][LOAD_THREADS];
+    uint32_t cnt[LOAD_STAGES][LOAD_THREADS];  // the aligned pair of uint16 counts holding the entry's
+};
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
+// This thread's share of one chunk's sums (force, torque).  A thread visits the
 // entries e0 + tid, e0 + tid + 256, ...; their bbox coordinates advance by a
 // fixed mixed-radix stride with carries (one 32-bit division per chunk).
+// s_al holds count / S^3 for every count; cap_entries is the length of
+// ent_cnt (the count pairs are read as aligned 32-bit words inside it).
+template <typename I>
+__device__ __forceinline__ void chunk_thread_sums(const ChunkDesc& dsc, const double* particles,
+                                                  const uint16_t* ent_cnt, int64_t cap_entries,
+                                                  const double* alpha_sum, const I* imb, uint32_t N, uint32_t ny,
+                                                  uint32_t nz, const double* s_al, LoadRing<I>& ring,
+                                                  double (&acc)[6]) {
+    const int64_t e0 = dsc.e0, e1 = dsc.e1;
+    const int tid = threadIdx.x;
+    if (e0 + tid >= e1) return;
+    const double* q = particles + (size_t)dsc.p * PF;
+    const uint32_t ey = (uint32_t)dsc.ey, ez = (uint32_t)dsc.ez;
+    // bbox-local coordinates of this thread's first entry, and the stride
+    const uint32_t local = (uint32_t)dsc.local0 + tid;
+    const uint32_t eyz = ey * ez;
+    uint32_t a = local / eyz;
+    const uint32_t rem = local - a * eyz;
+    uint32_t b = rem / ez;
+    uint32_t k = rem - b * ez;
+    const uint32_t step_k = blockDim.x % ez;
+    const uint32_t step_q = blockDim.x / ez;
+    const uint32_t step_b = step_q % ey;
+    const uint32_t step_a = step_q / ey;
+    const uint32_t bx = (uint32_t)dsc.x0, by = (uint32_t)dsc.y0, bz = (uint32_t)dsc.z0;
+    // prefetch cursor: entry ep at bbox-local (pa, pb, pk)
+    int64_t ep = e0 + tid;
+    uint32_t pa = a, pb = b, pk = k;
+    auto prefetch = [&](int slot) {
+        if (ep < e1) {  // the cell lies in the clipped box, so it exists even where the count is 0
+            const uint32_t cell = ((bx + pa) * ny + (by + pb)) * nz + (bz + pk);
+            cp_async<8>(&ring.alpha[slot][tid], alpha_sum + cell);
+            cp_async<sizeof(I)>(&ring.imb[slot][0][tid], imb + cell);
+            cp_async<sizeof(I)>(&ring.imb[slot][1][tid], imb + (size_t)N + cell);
+            cp_async<sizeof(I)>(&ring.imb[slot][2][tid], imb + 2 * (size_t)N + cell);
+            const int64_t even = ep & ~(int64_t)1;
+            if (even + 1 < cap_entries) cp_async<4>(&ring.cnt[slot][tid], ent_cnt + even);
+            else ring.cnt[slot][tid] = ent_cnt[ep];  // last entry of the array at an even index
+        }
+        cp_async_commit();  // one group per pass, empty past the end
+        ep += blockDim.x;
+        pk += step_k;
+        const uint32_t ck = pk >= ez;
+        pk -= ck ? ez : 0u;
+        pb += step_b + ck;
+        const uint32_t cb = pb >= ey;
+        pb -= cb ? ey : 0u;
+        pa += step_a + cb;
+    };
+#pragma unroll
+    for (int s = 0; s < LOAD_STAGES - 1; ++s) prefetch(s);
+    const double qx = q[0], qy = q[1], qz = q[2];
+    int slot = 0;
+    for (int64_t e = e0 + tid; e < e1; e += blockDim.x) {
+        cp_async_wait<LOAD_STAGES - 2>();  // the group of this pass has landed
+        const uint32_t pair = ring.cnt[slot][tid];
+        const uint32_t cnt = (e & 1) ? pair >> 16 : pair & 0xffffu;
+        if (cnt != 0) {
+            const double as = ring.alpha[slot][tid];
+            const double mx = (double)ring.imb[slot][0][tid];
+            const double my = (double)ring.imb[slot][1][tid];
+            const double mz = (double)ring.imb[slot][2][tid];
+            // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
+            const double al = s_al[cnt];
+            const double ow = xdiv(al, as > 1.0e-14 ? as : 1.0e-14);
+            const double nfx = -xmul(ow, mx);
+            const double nfy = -xmul(ow, my);
+            const double nfz = -xmul(ow, mz);
+            // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
+            const double rx = xsub(xadd((double)(bx + a), 0.5), qx);
+            const double ry = xsub(xadd((double)(by + b), 0.5), qy);
+            const double rz = xsub(xadd((double)(bz + k), 0.5), qz);
+            acc[0] += nfx;
+            acc[1] += nfy;
+            acc[2] += nfz;
+            acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
+            acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
+            acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
+        }
+        // refill the slot consumed in the previous pass (its values are used above)
+        prefetch(slot == 0 ? LOAD_STAGES - 1 : slot - 1);
+        slot = slot == LOAD_STAGES - 1 ? 0 : slot + 1;
+        // next entry of this thread: (a, b, k) += (step_a, step_b, step_k) with carries
+        k += step_k;
+        const uint32_t ck = k >= ez;
+        k -= ck ? ez : 0u;
+        b += step_b + ck;
+        const uint32_t cb = b >= ey;
+        b -= cb ? ey : 0u;
+        a += step_a + cb;
+    }
+    cp_async_wait<0>();  // nothing in flight into the ring when the next chunk starts
+}
+
+// One block per chunk of one particle's bbox entries.
 template <typename I>
 __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_chunks(psc_geometry g, const I* imb,
                                                                                  double* part) {
     __shared__ double s[LOAD_THREADS / 32][6];
+    __shared__ LoadRing<I> ring;
     extern __shared__ double s_al[];  // S^3 + 1 entries (dynamic)
     const int64_t C = g.totals[1];
     const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
-    const uint32_t ny = (uint32_t)g.ny, nz = (uint32_t)g.nz;
     const int S3 = g.subsamples * g.subsamples * g.subsamples;
     const double S3d = (double)S3;
     for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
@@ -409,79 +536,9 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
         // every thread reads the chunk's descriptor; the block sum below (its barriers) comes before
         // thread 0 overwrites the row with the chunk's sums
         const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
-        const int64_t e0 = dsc.e0, e1 = dsc.e1;
-        const double* q = g.particles + (size_t)dsc.p * PF;
-        const uint32_t ey = (uint32_t)dsc.ey, ez = (uint32_t)dsc.ez;
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (e0 + threadIdx.x < e1) {
-            // bbox-local coordinates of this thread's first entry, and the stride
-            const uint32_t local = (uint32_t)dsc.local0 + threadIdx.x;
-            const uint32_t eyz = ey * ez;
-            uint32_t a = local / eyz;
-            const uint32_t rem = local - a * eyz;
-            uint32_t b = rem / ez;
-            uint32_t k = rem - b * ez;
-            const uint32_t step_k = blockDim.x % ez;
-            const uint32_t step_q = blockDim.x / ez;
-            const uint32_t step_b = step_q % ey;
-            const uint32_t step_a = step_q / ey;
-            const double qx = q[0], qy = q[1], qz = q[2];
-            // LOAD_UNROLL entries per pass: all their loads are issued together,
-            // then accumulated in entry order (the order of a one-entry loop)
-            const uint32_t bx = (uint32_t)dsc.x0, by = (uint32_t)dsc.y0, bz = (uint32_t)dsc.z0;
-            for (int64_t e = e0 + threadIdx.x; e < e1; e += (int64_t)LOAD_UNROLL * blockDim.x) {
-                uint16_t cnt[LOAD_UNROLL];
-                uint32_t cx[LOAD_UNROLL], cy[LOAD_UNROLL], cz[LOAD_UNROLL];
-                double as[LOAD_UNROLL];
-                I mx[LOAD_UNROLL], my[LOAD_UNROLL], mz[LOAD_UNROLL];  // the field's own type until used
-#pragma unroll
-                for (int u = 0; u < LOAD_UNROLL; ++u) {
-                    const int64_t eu = e + (int64_t)u * blockDim.x;
-                    cnt[u] = 0;
-                    if (eu < e1) {
-                        // every load of the entry at once (the cell lies in the clipped box, so
-                        // it exists even where the count is 0): one memory round trip per pass
-                        const uint32_t cell = ((bx + a) * ny + (by + b)) * nz + (bz + k);
-                        cnt[u] = g.ent_cnt[eu];
-                        as[u] = g.alpha_sum[cell];
-                        mx[u] = imb[cell];
-                        my[u] = imb[(size_t)N + cell];
-                        mz[u] = imb[2 * (size_t)N + cell];
-                    }
-                    cx[u] = bx + a;
-                    cy[u] = by + b;
-                    cz[u] = bz + k;
-                    // next entry of this thread: (a, b, k) += (step_a, step_b, step_k) with carries
-                    k += step_k;
-                    const uint32_t ck = k >= ez;
-                    k -= ck ? ez : 0u;
-                    b += step_b + ck;
-                    const uint32_t cb = b >= ey;
-                    b -= cb ? ey : 0u;
-                    a += step_a + cb;
-                }
-#pragma unroll
-                for (int u = 0; u < LOAD_UNROLL; ++u) {
-                    if (cnt[u] == 0) continue;
-                    // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
-                    const double al = s_al[cnt[u]];
-                    const double ow = xdiv(al, as[u] > 1.0e-14 ? as[u] : 1.0e-14);
-                    const double nfx = -xmul(ow, (double)mx[u]);
-                    const double nfy = -xmul(ow, (double)my[u]);
-                    const double nfz = -xmul(ow, (double)mz[u]);
-                    // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
-                    const double rx = xsub(xadd((double)cx[u], 0.5), qx);
-                    const double ry = xsub(xadd((double)cy[u], 0.5), qy);
-                    const double rz = xsub(xadd((double)cz[u], 0.5), qz);
-                    acc[0] += nfx;
-                    acc[1] += nfy;
-                    acc[2] += nfz;
-                    acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
-                    acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
-                    acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
-                }
-            }
-        }
+        chunk_thread_sums<I>(dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum, imb, N, (uint32_t)g.ny,
+                             (uint32_t)g.nz, s_al, ring, acc);
         block_sum<6>(acc, s);
         if (threadIdx.x == 0) {
 #pragma unroll
@@ -490,16 +547,13 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
     }
 }
 
-// Per-particle sums of the chunk partials: one warp per particle, lane l
-// sums chunks l, l + 32, ... in order, then a fixed shuffle tree.
-__global__ void __launch_bounds__(256) k_loads_particles(psc_geometry g, const double* part, double* forces,
-                                                         double* torques) {
+// Per-particle sums of the chunk partials c0 .. c1-1: one warp per particle,
+// lane l sums chunks c0 + l, c0 + l + 32, ... in order, then a fixed shuffle tree.
+__device__ __forceinline__ void particle_sums(const double* part, int64_t c0, int64_t c1, double* force,
+                                              double* torque) {
     const int lane = threadIdx.x & 31;
-    const int p = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
-    if (p >= g.nparticles) return;  // warp-uniform
     double F[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    const int64_t c1 = g.chunk_off[p + 1];
-    for (int64_t c = g.chunk_off[p] + lane; c < c1; c += 32) {
+    for (int64_t c = c0 + lane; c < c1; c += 32) {
 #pragma unroll
         for (int k = 0; k < 6; ++k) F[k] += part[c * 6 + k];
     }
@@ -509,17 +563,23 @@ __global__ void __launch_bounds__(256) k_loads_particles(psc_geometry g, const d
         for (int o = 16; o > 0; o >>= 1) F[k] += __shfl_xor_sync(0xffffffffu, F[k], o);
     }
     if (lane < 3) {
-        forces[(size_t)p * 3 + lane] = F[lane];
-        torques[(size_t)p * 3 + lane] = F[3 + lane];
+        force[lane] = F[lane];
+        torque[lane] = F[3 + lane];
     }
+}
+
+__global__ void __launch_bounds__(256) k_loads_particles(psc_geometry g, const double* part, double* forces,
+                                                         double* torques) {
+    const int p = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
+    if (p >= g.nparticles) return;  // warp-uniform
+    particle_sums(part, g.chunk_off[p], g.chunk_off[p + 1], forces + (size_t)p * 3, torques + (size_t)p * 3);
 }
 
 // One block: the closure residual |sum_p F_p + sum_x imb| and the max force /
 // torque norms (psc3d.py:247-253, :280-281) from the per-particle loads.
-__global__ void __launch_bounds__(1024) k_loads_diag(psc_geometry g, const double* imb_sums, const double* forces,
-                                                     const double* torques, double* diag) {
+__device__ __forceinline__ void loads_diag_block(int P, const double* imb_sums, const double* forces,
+                                                 const double* torques, double* diag) {
     __shared__ double s[32][5];
-    const int P = g.nparticles;
     double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // sum Fx, Fy, Fz, max |F|^2, max |T|^2
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
         const double* F = forces + (size_t)p * 3;
@@ -556,6 +616,80 @@ __global__ void __launch_bounds__(1024) k_loads_diag(psc_geometry g, const doubl
         diag[PSC_DIAG_FORCE_SUM_Y] = r[1];
         diag[PSC_DIAG_FORCE_SUM_Z] = r[2];
     }
+}
+
+__global__ void __launch_bounds__(1024) k_loads_diag(psc_geometry g, const double* imb_sums, const double* forces,
+                                                     const double* torques, double* diag) {
+    loads_diag_block(g.nparticles, imb_sums, forces, torques, diag);
+}
+
+// ---------------------------------------------------------------------------
+// particle loads of many windows in one launch sequence
+// ---------------------------------------------------------------------------
+// The chunks of all jobs form one index space (job k owns chunks
+// chunk_base[k] .. chunk_base[k+1]-1, its particles particle_base[k] ..),
+// so the small windows of a batch fill the GPU together instead of one
+// launch each.  Every per-chunk, per-particle and per-window sum runs the
+// single-window arithmetic in the same order: the results are bitwise those
+// of one launch_particle_loads per window.
+
+__global__ void __launch_bounds__(256) k_chunk_desc_multi(const LoadsJob* jobs, const int64_t* chunk_base, int njobs,
+                                                          double* part) {
+    const int64_t C = chunk_base[njobs];
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C; c += (int64_t)gridDim.x * blockDim.x) {
+        const int k = owner_of(chunk_base, njobs, c);
+        ChunkDesc d = make_chunk_desc(jobs[k].g, c - chunk_base[k]);
+        d.pad = k;  // the chunk's job
+        *reinterpret_cast<ChunkDesc*>(part + c * 6) = d;
+    }
+}
+
+template <typename I>
+__global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS)
+    k_loads_chunks_multi(const LoadsJob* jobs, const int64_t* chunk_base, int njobs, double* part) {
+    __shared__ double s[LOAD_THREADS / 32][6];
+    __shared__ LoadRing<I> ring;
+    extern __shared__ double s_al[];  // S^3 + 1 entries for the largest S of the jobs (dynamic)
+    const int64_t C = chunk_base[njobs];
+    int cur_S = 0;  // S of the table in s_al (block-uniform)
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
+        const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
+        const psc_geometry& g = jobs[dsc.pad].g;
+        const int S = g.subsamples;
+        if (S != cur_S) {  // block-uniform; the previous chunk's reads of s_al ended before its block sum
+            const int S3 = S * S * S;
+            const double S3d = (double)S3;
+            for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
+            __syncthreads();
+            cur_S = S;
+        }
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        chunk_thread_sums<I>(dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum,
+                             reinterpret_cast<const I*>(jobs[dsc.pad].imb), (uint32_t)g.nx * g.ny * g.nz,
+                             (uint32_t)g.ny, (uint32_t)g.nz, s_al, ring, acc);
+        block_sum<6>(acc, s);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_loads_particles_multi(const LoadsJob* jobs, const int64_t* chunk_base,
+                                                               const int64_t* particle_base, int njobs,
+                                                               const double* part) {
+    const int64_t gp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (gp >= particle_base[njobs]) return;  // warp-uniform
+    const int k = owner_of(particle_base, njobs, gp);
+    const LoadsJob& J = jobs[k];
+    const int p = (int)(gp - particle_base[k]);
+    particle_sums(part + chunk_base[k] * 6, J.g.chunk_off[p], J.g.chunk_off[p + 1], J.forces + (size_t)p * 3,
+                  J.torques + (size_t)p * 3);
+}
+
+__global__ void __launch_bounds__(1024) k_loads_diag_multi(const LoadsJob* jobs) {
+    const LoadsJob& J = jobs[blockIdx.x];
+    loads_diag_block(J.g.nparticles, J.imb_sums, J.forces, J.torques, J.diag);
 }
 
 // ---------------------------------------------------------------------------
@@ -674,6 +808,25 @@ cudaError_t launch_solid_velocity(const psc_geometry& g, int us_type, void* us, 
     return cudaGetLastError();
 }
 
+// The chunk kernels hold a static staging ring and a dynamic count table of
+// up to 16^3 + 1 doubles; for FP64 fields the sum can pass the default 48 KB
+// of shared memory per block, so every device gets the opt-in once.
+static cudaError_t loads_smem_optin() {
+    constexpr int kMaxDev = 64;
+    static int done[kMaxDev];  // benign race: setting the attribute twice is harmless
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDev || done[dev]) return e;
+    const int lut = (16 * 16 * 16 + 1) * (int)sizeof(double);
+    if ((e = cudaFuncSetAttribute(k_loads_chunks<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)) ||
+        (e = cudaFuncSetAttribute(k_loads_chunks<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)) ||
+        (e = cudaFuncSetAttribute(k_loads_chunks_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)) ||
+        (e = cudaFuncSetAttribute(k_loads_chunks_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)))
+        return e;
+    done[dev] = 1;
+    return cudaSuccess;
+}
+
 cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const void* imb, double* chunk_partials,
                                   const double* imb_sums, double* forces, double* torques, double* diag,
                                   cudaStream_t stream) {
@@ -682,6 +835,8 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
         const unsigned grid = (unsigned)(g.capacity_chunks < cap ? g.capacity_chunks : cap);
         const size_t lut = (size_t)(g.subsamples * g.subsamples * g.subsamples + 1) * sizeof(double);
         const int64_t cg = (g.capacity_chunks + 255) / 256;
+        cudaError_t e0 = loads_smem_optin();
+        if (e0 != cudaSuccess) return e0;
         k_chunk_desc<<<(unsigned)(cg < cap ? cg : cap), 256, 0, stream>>>(g, chunk_partials);
         if (imb_type == 0)
             k_loads_chunks<double><<<grid, LOAD_THREADS, lut, stream>>>(g, reinterpret_cast<const double*>(imb),
@@ -698,6 +853,36 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
         if (e != cudaSuccess) return e;
     }
     k_loads_diag<<<1, 1024, 0, stream>>>(g, imb_sums, forces, torques, diag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_particle_loads_multi(const LoadsJob* d_jobs, const int64_t* d_chunk_base,
+                                        const int64_t* d_particle_base, int njobs, int64_t total_chunks,
+                                        int64_t total_particles, int imb_type, int max_subsamples, double* part,
+                                        cudaStream_t stream) {
+    if (njobs <= 0) return cudaSuccess;
+    const int64_t cap = (int64_t)sm_count() * 16;
+    if (total_chunks > 0) {
+        const int64_t cg = (total_chunks + 255) / 256;
+        cudaError_t e0 = loads_smem_optin();
+        if (e0 != cudaSuccess) return e0;
+        k_chunk_desc_multi<<<(unsigned)(cg < cap ? cg : cap), 256, 0, stream>>>(d_jobs, d_chunk_base, njobs, part);
+        const unsigned grid = (unsigned)(total_chunks < cap ? total_chunks : cap);
+        const size_t lut = (size_t)(max_subsamples * max_subsamples * max_subsamples + 1) * sizeof(double);
+        if (imb_type == 0)
+            k_loads_chunks_multi<double><<<grid, LOAD_THREADS, lut, stream>>>(d_jobs, d_chunk_base, njobs, part);
+        else
+            k_loads_chunks_multi<float><<<grid, LOAD_THREADS, lut, stream>>>(d_jobs, d_chunk_base, njobs, part);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (total_particles > 0) {
+        k_loads_particles_multi<<<(unsigned)((total_particles + 7) / 8), 256, 0, stream>>>(
+            d_jobs, d_chunk_base, d_particle_base, njobs, part);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    k_loads_diag_multi<<<(unsigned)njobs, 1024, 0, stream>>>(d_jobs);
     return cudaGetLastError();
 }
 

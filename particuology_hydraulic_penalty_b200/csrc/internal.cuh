@@ -50,6 +50,24 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
                                   const double* imb_sums, double* forces, double* torques, double* diag,
                                   cudaStream_t stream);
 
+// One window of a many-window particle-loads launch (a device table).
+struct LoadsJob {
+    psc_geometry g;
+    const void* imb;          // IMB field [3][N] of the window (one imb_type for all jobs)
+    const double* imb_sums;   // sum of the IMB field (3)
+    double* forces;           // [P][3]
+    double* torques;          // [P][3]
+    double* diag;             // [PSC_NDIAG]
+};
+// Particle loads and load diagnostics of njobs windows in four launches.
+// d_chunk_base / d_particle_base: [njobs + 1] exclusive prefix sums of the
+// jobs' chunk and particle counts (the totals are their last entries, also
+// passed by value); part: total_chunks rows of 6 doubles.
+cudaError_t launch_particle_loads_multi(const LoadsJob* d_jobs, const int64_t* d_chunk_base,
+                                        const int64_t* d_particle_base, int njobs, int64_t total_chunks,
+                                        int64_t total_particles, int imb_type, int max_subsamples, double* part,
+                                        cudaStream_t stream);
+
 cudaError_t launch_adjoint_seed(const psc_adjoint_args& a, cudaStream_t stream);
 cudaError_t launch_adjoint_step(const psc_adjoint_args& a, cudaStream_t stream);
 cudaError_t launch_adjoint_geometry_grad(const psc_geometry& g, const psc_adjoint_args& a, double* part,

@@ -993,6 +993,14 @@ struct psc_batch {
     HArray<double> up_host;    // every window's particles, staged for one upload
     DArray<double> up_dev;
     cudaEvent_t up_done = nullptr;
+    // particle loads of all active windows in one launch sequence: job table
+    // [LoadsJob x n][chunk bases n+1][particle bases n+1], as last uploaded
+    std::vector<unsigned char> jobs_last;
+    HArray<unsigned char> jobs_host;
+    DArray<unsigned char> jobs_dev;
+    DArray<double> loads_part;  // chunk partials of all jobs
+    int jobs_n = 0, jobs_max_s = 1;
+    int64_t jobs_chunks = 0, jobs_particles = 0;
 
     ~psc_batch() {
         for (auto& g : graph)
@@ -1003,6 +1011,60 @@ struct psc_batch {
 
 namespace psc {
 namespace {
+
+// Job table of the particle loads of every active window (one
+// launch_particle_loads_multi per reporting step).  Built on the host each
+// time and uploaded only when it changed (new geometry, buffers, frozen set).
+int batch_loads_table(psc_batch& b, const char* who) {
+    const int nwin = (int)b.w.size();
+    std::vector<LoadsJob> jobs;
+    std::vector<int64_t> cb(1, 0), pb(1, 0);
+    int max_s = 1;
+    for (int k = 0; k < nwin; ++k) {
+        if (b.frozen[(size_t)k] >= 0) continue;
+        const Window& w = *b.w[(size_t)k];
+        LoadsJob j;
+        std::memset(&j, 0, sizeof(j));  // padding too: the table is compared bytewise
+        j.g = w.geometry();
+        j.imb = w.imb.p;
+        j.imb_sums = b.red_pre.p + (size_t)k * PSC_NRED + PSC_RED_IMBX;
+        j.forces = w.forces.p;
+        j.torques = w.torques.p;
+        j.diag = b.diag.p + (size_t)k * PSC_NDIAG;
+        jobs.push_back(j);
+        cb.push_back(cb.back() + (w.P > 0 ? w.n_chunks : 0));
+        pb.push_back(pb.back() + w.P);
+        max_s = std::max(max_s, w.cfg.subsamples);
+    }
+    const size_t n = jobs.size();
+    const size_t jb = n * sizeof(LoadsJob), bb = (n + 1) * sizeof(int64_t);
+    std::vector<unsigned char> bytes(jb + 2 * bb);
+    if (jb) std::memcpy(bytes.data(), jobs.data(), jb);
+    std::memcpy(bytes.data() + jb, cb.data(), bb);
+    std::memcpy(bytes.data() + jb + bb, pb.data(), bb);
+    b.jobs_n = (int)n;
+    b.jobs_max_s = max_s;
+    b.jobs_chunks = cb.back();
+    b.jobs_particles = pb.back();
+    if (bytes == b.jobs_last) return PSC_OK;
+    // kernels of earlier steps may still read the old table or partials, the copy the pinned buffer
+    PSC_CUDA(cudaStreamSynchronize(b.stream), who);
+    PSC_CUDA(b.loads_part.ensure(std::max<int64_t>(b.jobs_chunks, 1) * 6, false, b.stream), who);
+    PSC_CUDA(b.jobs_dev.ensure((int64_t)bytes.size(), false, b.stream), who);
+    PSC_CUDA(b.jobs_host.ensure((int64_t)bytes.size()), who);
+    std::memcpy(b.jobs_host.p, bytes.data(), bytes.size());
+    PSC_CUDA(cudaMemcpyAsync(b.jobs_dev.p, b.jobs_host.p, bytes.size(), cudaMemcpyHostToDevice, b.stream), who);
+    b.jobs_last.swap(bytes);
+    return PSC_OK;
+}
+
+const int64_t* batch_chunk_base(const psc_batch& b) {
+    return reinterpret_cast<const int64_t*>(b.jobs_dev.p + (size_t)b.jobs_n * sizeof(LoadsJob));
+}
+
+const int64_t* batch_particle_base(const psc_batch& b) {
+    return batch_chunk_base(b) + b.jobs_n + 1;
+}
 
 void batch_drop_graphs(psc_batch& b) {
     for (auto& g : b.graph)
@@ -1222,7 +1284,7 @@ int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_lau
         if (e == cudaSuccess) e = b->red_post.ensure((int64_t)nwin * PSC_NRED, true, b->stream);
         if (e == cudaSuccess) e = b->diag.ensure((int64_t)nwin * PSC_NDIAG, true, b->stream);
         if (e == cudaSuccess) e = b->host.ensure((int64_t)nwin * kOutLen);
-        if (e == cudaSuccess) e = b->lanes.init(Lanes::kMax);
+        if (e == cudaSuccess) e = b->lanes.init(1);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->up_done, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) st = cuda_fail(e, "psc_batch_create");
@@ -1304,17 +1366,16 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
         b->parity ^= 1;
         batch_sync_cur(*b);
         PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_pre.p, b->stream));
-        // the loads read the IMB field and geometry only: on the lanes, beside the reduction pass
+        // the loads of every active window in one launch sequence; they read the IMB field and
+        // geometry only: on a lane, beside the reduction pass
+        PSC_TRY(batch_loads_table(*b, "psc_batch_step"));
         PSC_CUDA(b->lanes.begin(b->stream), "psc_batch_step");
-        for (int k = 0; k < nwin; ++k) {
-            Window& w = *b->w[(size_t)k];
-            if (b->frozen[(size_t)k] >= 0) continue;
-            psc_geometry g = w.geometry();
-            PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p,
-                                       b->red_pre.p + (size_t)k * PSC_NRED + PSC_RED_IMBX, w.forces.p, w.torques.p,
-                                       b->diag.p + (size_t)k * PSC_NDIAG, b->lanes.lane(k)));
-            w.loads_ready = true;
-        }
+        PSC_CUDA(launch_particle_loads_multi(reinterpret_cast<const LoadsJob*>(b->jobs_dev.p), batch_chunk_base(*b),
+                                             batch_particle_base(*b), b->jobs_n, b->jobs_chunks, b->jobs_particles,
+                                             b->w[0]->field_type(), b->jobs_max_s, b->loads_part.p, b->lanes.lane(0)),
+                 "psc_batch_step: particle loads");
+        for (int k = 0; k < nwin; ++k)
+            if (b->frozen[(size_t)k] < 0) b->w[(size_t)k]->loads_ready = true;
         PSC_TRY(batch_launch(*b, PSC_STEP_REDUCE | (fields ? PSC_STEP_MOMENTS : 0u)));
         PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_post.p, b->stream));
         PSC_CUDA(b->lanes.end(b->stream), "psc_batch_step");

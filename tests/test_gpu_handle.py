@@ -202,3 +202,42 @@ def test_batch_set_particles_all_equals_per_window():
     for k in range(len(wins)):
         assert np.array_equal(a.field(k, nat.FIELD_F), b.field(k, nat.FIELD_F))
         assert np.array_equal(a.loads(k)[0], b.loads(k)[0])
+
+
+def test_batch_loads_one_launch_match_solo_windows():
+    """The batch computes the loads of all its windows in one launch sequence (one chunk space over
+    every window).  Windows with different sub-sample counts (the per-block count / S^3 table is
+    rebuilt when S changes), one without particles, and uneven sizes: forces, torques and the
+    load diagnostics equal those of each window solved alone."""
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.handle import BatchHandle, SolverHandle, make_config
+
+    wins = [_window(24, "skeleton", 1), _window(32, "passive", 2), None, _window(40, "preloaded", 3),
+            _window(24, "passive", 4)]
+    sizes = [24, 32, 16, 40, 24]
+    subs = [4, 3, 2, 4, 2]
+    parts = [w.particles if w is not None else np.zeros((0, 10)) for w in wins]
+    cfgs = [make_config((n,) * 3, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=s, store=nat.STORE_F32)
+            for n, s in zip(sizes, subs)]
+    b = BatchHandle(cfgs, graph_steps=4)
+    b.set_particles_all(parts)
+    b.step(7, nat.RUN_DIAG)
+    for rep in range(2):  # a second reporting step reuses the uploaded job table
+        for k in range(len(cfgs)):
+            h = SolverHandle(make_config((sizes[k],) * 3, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=subs[k],
+                                         store=nat.STORE_F32))
+            h.set_particles(parts[k])
+            h.step(7 + rep, nat.RUN_DIAG)
+            F, T = h.loads()
+            Fb, Tb = b.loads(k)
+            assert np.array_equal(F, Fb) and np.array_equal(T, Tb)
+            assert F.shape == (len(parts[k]), 3)
+            d, db = h.diag(), b.diag(k)
+            assert d.max_force == db.max_force and d.max_torque == db.max_torque
+            assert tuple(d.force_sum) == tuple(db.force_sum)
+            # the IMB sums come from the window reductions, grouped differently in a batch
+            scale = max(np.abs(F).sum(), 1e-300)
+            assert abs(d.momentum_residual - db.momentum_residual) <= 1e-12 * scale
+            h.close()
+        b.step(1, nat.RUN_DIAG)
+    b.close()
