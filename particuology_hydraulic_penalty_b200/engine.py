@@ -8,6 +8,7 @@ path: constructing anything here without a CUDA device raises.
 from __future__ import annotations
 
 import ctypes
+import operator
 from dataclasses import dataclass
 
 import numpy as np
@@ -48,6 +49,7 @@ DEFAULT_STORE_SCALE = {
 }
 Q = 19
 PARTICLE_FIELDS = ("x", "y", "z", "r", "vx", "vy", "vz", "wx", "wy", "wz")
+_particle_row = operator.attrgetter(*PARTICLE_FIELDS)
 
 
 def trt_tau_minus(tau: float, magic: float = 3.0 / 16.0) -> float:
@@ -113,10 +115,8 @@ def particles_array(particles) -> np.ndarray:
         if arr.ndim != 2 or arr.shape[1] != 10:
             raise ValueError("a particle array must have shape (P, 10)")
     else:
-        plist = list(particles)
-        arr = np.empty((len(plist), 10), dtype=np.float64)
-        for i, p in enumerate(plist):
-            arr[i] = [getattr(p, k) for k in PARTICLE_FIELDS]
+        # one attribute tuple per particle (callers mutate Particle3D fields in place between steps)
+        arr = np.array(list(map(_particle_row, particles)), dtype=np.float64).reshape(-1, 10)
     if not np.all(np.isfinite(arr)):
         raise ValueError("particle state contains NaN or Inf")
     return arr
