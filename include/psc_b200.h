@@ -448,7 +448,12 @@ int psc_set_particles(psc_solver* h, const double* h_particles, int nparticles);
 int psc_rebuild_geometry(psc_solver* h);
 /* nsteps calls of collide_stream_psc() (psc3d.py:208-253).  h_status may be
  * NULL.  Without PSC_RUN_DIAG the intermediate steps skip the reductions
- * (they change no state); the IMB field of the final step is always written. */
+ * (they change no state); the IMB field of the final step is always written.
+ * psc_step(h, 1, PSC_RUN_DIAG) (one drop-in call) replays its launches from a
+ * CUDA graph, one per population buffer, recorded on the second call whose
+ * launch arguments (buffers, sizes, kernel, descriptor version) match the
+ * previous call's; on a stream the caller is capturing it runs its launches
+ * directly, so they go into the caller's graph. */
 int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status);
 /* Field `which` (PSC_FIELD_*) as float64 into h_dst ([N], or [19][N] for PSC_FIELD_F). */
 int psc_get_fields(psc_solver* h, int which, double* h_dst);

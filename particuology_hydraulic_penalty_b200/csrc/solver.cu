@@ -724,6 +724,18 @@ struct psc_solver {
     Window w;
     HArray<int64_t> tot;
     HArray<double> host_out;
+    // The single reporting step (psc_step(h, 1, PSC_RUN_DIAG), one drop-in
+    // collide_stream_psc() call) as a CUDA graph per buffer parity, keyed by
+    // every pointer, size and version its launches capture: captured on the
+    // second call with an unchanged key, replayed while the key holds.
+    cudaGraphExec_t report_graph[2] = {nullptr, nullptr};
+    std::vector<unsigned char> report_key[2];   // key of report_graph[parity]
+    std::vector<unsigned char> report_seen[2];  // key of the last eager run of that parity
+
+    ~psc_solver() {
+        for (auto& g : report_graph)
+            if (g) cudaGraphExecDestroy(g);
+    }
 };
 
 namespace psc {
@@ -772,6 +784,121 @@ int solver_collide(psc_solver& h, bool imb) {
     w.loads_ready = false;
     w.diag_ready = false;
     if (imb) PSC_TRY(psc_reduce_windows(w.solo[w.cur].p, 1, red_pre(w), s));
+    return PSC_OK;
+}
+
+// Everything the launches of one reporting step from buffer parity `par`
+// capture: a graph recorded under one key replays correctly under the same key.
+std::vector<unsigned char> report_key(const psc_solver& h, int par) {
+    const Window& w = h.w;
+    struct Key {
+        psc_geometry g;
+        const void* desc[2];
+        const void* imb;
+        const void* out;
+        const void* host;
+        const void* chunks;
+        const void* forces;
+        const void* torques;
+        uint64_t desc_version;
+        int64_t tiles;
+        int32_t kernel, store, moving, par, field_type, pad;
+    } k;
+    std::memset(&k, 0, sizeof(k));  // padding too: keys compare bytewise
+    k.g = w.geometry();
+    k.desc[0] = w.solo[0].p;
+    k.desc[1] = w.solo[1].p;
+    k.imb = w.imb.p;
+    k.out = w.out.p;
+    k.host = h.host_out.p;
+    k.chunks = w.chunk_partials.p;
+    k.forces = w.forces.p;
+    k.torques = w.torques.p;
+    k.desc_version = w.desc_version;
+    k.tiles = w.solo_tiles;
+    k.kernel = w.solo_kernel;
+    k.store = w.cfg.store;
+    k.moving = w.moving ? 1 : 0;
+    k.par = par;
+    k.field_type = w.field_type();
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&k);
+    return std::vector<unsigned char>(b, b + sizeof(k));
+}
+
+// The GPU work of one reporting step from buffer parity `par` (the launches of
+// solver_collide(imb) + solver_report(loads, post) without their host-side
+// bookkeeping), ending with the read-back into host_out.
+int report_step_work(psc_solver& h, int par) {
+    Window& w = h.w;
+    cudaStream_t s = h.stream;
+    const unsigned mv = w.moving ? PSC_STEP_MOVING : 0u;
+    const psc_launch c = {0, 1, w.solo_kernel, 0, 0};
+    PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par].p, 1, w.solo_tiles,
+                                PSC_STEP_COLLIDE | PSC_STEP_IMB | PSC_STEP_REDUCE | mv, &c, s));
+    PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_pre(w), s));
+    PSC_CUDA(h.lanes.begin(s), "psc_step");
+    psc_geometry g = w.geometry();
+    PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
+                               w.forces.p, w.torques.p, diag_dev(w), h.lanes.lane(0)));
+    PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par ^ 1].p, 1, w.solo_tiles, PSC_STEP_REDUCE | mv, &c, s));
+    PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_post(w), s));
+    PSC_CUDA(h.lanes.end(s), "psc_step");
+    PSC_CUDA(cudaMemcpyAsync(h.host_out.p, w.out.p, kOutLen * sizeof(double), cudaMemcpyDeviceToHost, s), "psc_step");
+    return PSC_OK;
+}
+
+// One collide_stream_psc() step with its loads and diagnostics (the work of
+// solver_collide(imb) + solver_report(loads)), replayed from a CUDA graph
+// when nothing it captures has changed since the previous call.
+int solver_report_step(psc_solver& h) {
+    Window& w = h.w;
+    cudaStream_t s = h.stream;
+    // everything that may allocate, upload or synchronise happens here, outside any capture
+    PSC_TRY(window_ensure_imb(w, s));
+    PSC_TRY(window_upload_solo(w, s));
+    PSC_CUDA(h.host_out.ensure(kOutLen), "psc_step");
+    const int par = w.cur;
+    std::vector<unsigned char> key = report_key(h, par);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PSC_CUDA(cudaStreamIsCapturing(s, &cap), "psc_step");
+    if (cap != cudaStreamCaptureStatusNone) {
+        PSC_TRY(report_step_work(h, par));  // the caller records this step into its own graph
+    } else if (h.report_graph[par] && key == h.report_key[par]) {
+        PSC_CUDA(cudaGraphLaunch(h.report_graph[par], s), "psc_step");
+    } else if (key == h.report_seen[par]) {
+        // the same launches as the previous call of this parity: record them once, then replay
+        if (h.report_graph[par]) {
+            cudaGraphExecDestroy(h.report_graph[par]);
+            h.report_graph[par] = nullptr;
+            h.report_key[par].clear();
+        }
+        PSC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "psc_step");
+        const int st = report_step_work(h, par);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+        if (st != PSC_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (ec != cudaSuccess) return cuda_fail(ec, "psc_step: capturing the reporting step");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) return cuda_fail(ei, "psc_step: instantiating the reporting step");
+        h.report_graph[par] = exec;
+        h.report_key[par] = key;
+        PSC_CUDA(cudaGraphLaunch(exec, s), "psc_step");
+    } else {
+        PSC_TRY(report_step_work(h, par));
+        h.report_seen[par] = std::move(key);
+    }
+    w.cur ^= 1;
+    w.stepped = true;
+    w.moments_ready = false;
+    w.loads_ready = true;
+    PSC_CUDA(cudaStreamSynchronize(s), "psc_step");
+    fill_diag(w, h.host_out.p, w.last);
+    w.diag_ready = true;
     return PSC_OK;
 }
 
@@ -853,6 +980,13 @@ int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status) {
     psc_status st{};
     st.residual = INFINITY;
     if (nsteps > 0) PSC_TRY(window_prepare(w, h->stream, h->tot, "psc_step"));
+    if (nsteps == 1 && diag && !converge && !fields) {  // one collide_stream_psc() call
+        PSC_TRY(solver_report_step(*h));
+        st.steps_done = 1;
+        st.diag = w.last;
+        if (h_status) *h_status = st;
+        return PSC_OK;
+    }
     double previous = NAN;
     int k = 0;
     for (k = 1; k <= nsteps; ++k) {
