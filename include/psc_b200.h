@@ -48,7 +48,7 @@ extern "C" {
 #define PSC_OK 0
 #define PSC_E_INVALID -1     /* bad argument (null pointer, size, mode) */
 #define PSC_E_CUDA -2        /* a CUDA runtime call failed */
-#define PSC_E_UNSUPPORTED -3 /* valid but not supported by this build/device */
+#define PSC_E_UNSUPPORTED -3 /* valid but not supported by the library or the device */
 #define PSC_E_CAPACITY -4    /* a caller buffer is too small (see plan queries) */
 
 /* ---- storage / arithmetic modes of the populations ---------------------- */
@@ -513,7 +513,10 @@ int psc_batch_destroy(psc_batch* b);
 /* Particles of window `win`; a changed array re-voxelises that window before the next step. */
 int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, int nparticles);
 /* psc_batch_set_particles for every window in one call: h_particles[k] is window k's [P_k][10]
- * array (may be NULL when nparticles[k] is 0). */
+ * array (may be NULL when nparticles[k] is 0).  All windows are staged in one host buffer and
+ * uploaded with one copy.  If window k's state is rejected (NaN / Inf, null array), windows
+ * 0..k-1 keep their new states, window k and the later ones their previous ones, and the call
+ * returns the error. */
 int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, const int* h_nparticles);
 /* nsteps steps of every active window.  PSC_RUN_DIAG: diagnostics and loads
  * of every window at the final step into h_status[nwin] (may be NULL). */

@@ -361,13 +361,30 @@ int window_ensure_moments(Window& w, cudaStream_t s) {
 
 // Validation and bookkeeping of a new particle state (no upload): per-P
 // buffers, the host copy, the change version and the moving flag.
-int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who) {
+// Copies n doubles from src to dst and reports whether src equals ref bit for
+// bit: the staging copy and the unchanged-state test in one pass.
+bool copy_same(double* dst, const double* src, const double* ref, size_t n) {
+    uint64_t diff = 0;
+    for (size_t i = 0; i < n; ++i) {
+        uint64_t v, r;
+        std::memcpy(&v, src + i, sizeof(v));
+        std::memcpy(&r, ref + i, sizeof(r));
+        std::memcpy(dst + i, &v, sizeof(v));
+        diff |= v ^ r;
+    }
+    return diff == 0;
+}
+
+// known_same: 1 when the caller has established that hp equals the last
+// accepted state bit for bit (same count), 0 when not known.
+int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who, int known_same = 0) {
     if (P < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
     if (P > 0 && !hp) return fail(PSC_E_INVALID, std::string(who) + ": null particle array");
     // unchanged (bitwise) since the last upload: nothing to validate or record again
     const size_t n10 = (size_t)P * 10;
     const bool same_size = P == w.P && w.hp.size() == n10;
-    const bool differs = !same_size || (n10 && std::memcmp(w.hp.data(), hp, n10 * sizeof(double)) != 0);
+    const bool differs =
+        !same_size || (!known_same && n10 && std::memcmp(w.hp.data(), hp, n10 * sizeof(double)) != 0);
     bool mv = w.moving;
     if (differs) {
         // finiteness (the reference fails on NaN / Inf) as one sum: v * 0 is NaN exactly for
@@ -1466,20 +1483,33 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
     }
     PSC_CUDA(b->up_host.ensure(b->up_dev.n), who);
     int64_t off = 0;
-    for (size_t k = 0; k < nwin; ++k) {
+    int st = PSC_OK;
+    for (size_t k = 0; k < nwin && st == PSC_OK; ++k) {
         Window& w = *b->w[k];
         const int P = h_nparticles[k];
-        PSC_TRY(window_accept_particles(w, h_particles[k], P, b->stream, who));
-        if (P > 0) std::memcpy(b->up_host.p + off, h_particles[k], (size_t)P * 10 * sizeof(double));
+        if (P > 0 && !h_particles[k]) {
+            st = fail(PSC_E_INVALID, std::string(who) + ": null particle array");
+            break;
+        }
+        // stage the window's particles; an unchanged state is found in the same pass
+        const size_t n10 = (size_t)std::max(P, 0) * 10;
+        int same = 0;
+        if (P > 0 && P == w.P && w.hp.size() == n10)
+            same = copy_same(b->up_host.p + off, h_particles[k], w.hp.data(), n10) ? 1 : 0;
+        else if (P > 0)
+            std::memcpy(b->up_host.p + off, h_particles[k], n10 * sizeof(double));
+        st = window_accept_particles(w, h_particles[k], P, b->stream, who, same);
+        if (st != PSC_OK) break;  // (a rejected window keeps its previous state)
         w.ext_particles = b->up_dev.p + off;
         off += (int64_t)P * 10;
     }
-    if (total > 0)
-        PSC_CUDA(cudaMemcpyAsync(b->up_dev.p, b->up_host.p, (size_t)total * sizeof(double), cudaMemcpyHostToDevice,
+    // the windows accepted so far (all of them unless one was rejected) read their staged states
+    if (off > 0)
+        PSC_CUDA(cudaMemcpyAsync(b->up_dev.p, b->up_host.p, (size_t)off * sizeof(double), cudaMemcpyHostToDevice,
                                  b->stream),
                  who);
     PSC_CUDA(cudaEventRecord(b->up_done, b->stream), who);
-    return PSC_OK;
+    return st;
 }
 
 int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_status) {

@@ -278,3 +278,28 @@ def test_dropin_reporting_graph_follows_particle_updates():
 
     run(parts, 10, 0)
     run(parts[:-1], 5, 10)
+
+
+def test_batch_set_particles_all_rejects_a_window_and_keeps_the_rest_consistent():
+    """A non-finite particle state in one window: psc_batch_set_particles_all fails, the windows
+    before it take their new states (staged and uploaded), the rejected window and those after it
+    keep their previous ones.  Torques (arms from the uploaded centres) match a batch given
+    exactly those states."""
+    from particuology_hydraulic_penalty_b200 import _native as nat
+
+    wins = _three()
+    a = _batch(wins)
+    b = _batch(wins)
+    new = [w.particles.copy() for w in wins]
+    for m in new:
+        m[:, 0] += 0.25
+    bad = [new[0], new[1].copy(), new[2]]
+    bad[1][0, 2] = np.nan
+    with pytest.raises(nat.PscError):
+        b.set_particles_all(bad)
+    a.set_particles(0, new[0])
+    a.step(2, nat.RUN_DIAG)
+    b.step(2, nat.RUN_DIAG)
+    for k in range(len(wins)):
+        assert np.array_equal(a.loads(k)[1], b.loads(k)[1])
+        assert np.array_equal(a.field(k, nat.FIELD_F), b.field(k, nat.FIELD_F))
