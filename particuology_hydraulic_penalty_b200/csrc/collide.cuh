@@ -365,12 +365,16 @@ PSC_HD void collide_fast2(R* g, const WinConst<R>& c, R B, R kb, R usx, R usy, R
         //   g_i' = (1 - kb - B) g_i + B g_j + S + T,   g_j' = (1 - kb - B) g_j + B g_i + S - T,
         //   S = K cu + (kb - B) wrq + (kb w drho - 3 pref w uF) + B e_s,
         //   T = 3 (kb + B) w rho cu + B h_s + A,
-        // and the pair's IMB momentum B (os_i - os_j) = 2 B ((g_j - g_i) + h).  The per-weight
-        // factors are computed once per cell.
+        // and the pair's IMB momentum B (os_i - os_j) = 2 B ((g_j - g_i) + h).  With
+        // wrq = w rho (4.5 cu^2 - 1.5 u^2), S without e_s is the quadratic cu (q cu + K) + b,
+        // q = 4.5 (kb - B) w rho, b = kb w drho - 3 pref w uF - (kb - B) w rho 1.5 u^2: two FMAs per
+        // pair.  The per-weight factors are computed once per cell.
         const R omB = omk - B, kmB = kb - B, B2 = B + B;
         const R kbd = kb * drho;
         const R wr1 = R(W1) * rho, wr2 = R(W2) * rho;
-        const R base1 = R(W1) * kbd - c.pw3[1] * uF, base2 = R(W2) * kbd - c.pw3[2] * uF;
+        const R m1 = kmB * wr1, m2 = kmB * wr2;
+        const R q1 = R(4.5) * m1, q2 = R(4.5) * m2;
+        const R b1 = (R(W1) * kbd - c.pw3[1] * uF) - m1 * uu15, b2 = (R(W2) * kbd - c.pw3[2] * uF) - m2 * uu15;
         const R kp3 = R(3) * (kb + B);
         const R t1 = kp3 * wr1, t2 = kp3 * wr2;
         const R a1 = R(3) * wr1, a2 = R(3) * wr2;
@@ -380,8 +384,7 @@ PSC_HD void collide_fast2(R* g, const WinConst<R>& c, R B, R kb, R usx, R usy, R
             const bool axis = i < 7;
             const R wr = axis ? wr1 : wr2;
             const R cu = csel(cxv(i), uex) + csel(cyv(i), uey) + csel(czv(i), uez);
-            const R wrq = wr * (R(4.5) * cu * cu - uu15);
-            R S = c.K[k] * cu + (kmB * wrq + (axis ? base1 : base2));
+            R S = cu * ((axis ? q1 : q2) * cu + c.K[k]) + (axis ? b1 : b2);
             R T = (axis ? t1 : t2) * cu + c.A[k];
             R h = (axis ? a1 : a2) * cu;
             if (MOVING) {
