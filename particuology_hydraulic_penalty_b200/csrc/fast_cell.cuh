@@ -21,7 +21,8 @@ struct FastWin {
     int64_t tile_begin;
     int64_t tile_end;
     uint32_t nx, ny, nz, N;
-    uint32_t step_x, step_y, step_z;  // blockDim cells as a mixed-radix (x, y, z) increment
+    uint32_t step_x, step_y, step_z;     // blockDim cells as a mixed-radix (x, y, z) increment
+    uint32_t tstep_x, tstep_y, tstep_z;  // tile_cells cells (one tile on) likewise
     int32_t tile_cells;
     int32_t moving;
     int32_t inactive;
@@ -58,6 +59,11 @@ __device__ void load_fast_win(FastWin<T, R, O>& s, const psc_window& W, bool mov
         s.step_z = blockDim.x % (uint32_t)W.nz;
         s.step_y = q % (uint32_t)W.ny;
         s.step_x = q / (uint32_t)W.ny;
+        const uint32_t tc = W.tile_cells > 0 ? (uint32_t)W.tile_cells : 0u;
+        const uint32_t tq = tc / (uint32_t)W.nz;
+        s.tstep_z = tc % (uint32_t)W.nz;
+        s.tstep_y = tq % (uint32_t)W.ny;
+        s.tstep_x = tq / (uint32_t)W.ny;
         s.tile_cells = W.tile_cells;
         s.moving = (moving_launch && (W.flags & PSC_WIN_MOVING) && W.us != nullptr) ? 1 : 0;
         s.inactive = (W.flags & PSC_WIN_INACTIVE) ? 1 : 0;

@@ -82,6 +82,10 @@ __global__ void __launch_bounds__(STEP_THREADS, (PairOccupancy<STORE, MOVING, RE
     for (int q = 0; q < PSC_NRED; ++q) red[q] = 0.0;
     bool have = false;
     bool skip = false;  // block-uniform: the window in sw cannot run here
+    // this thread's first cell (ix, iy, iz) in the current tile: divided out when the CTA enters a
+    // window, then advanced tile by tile (consecutive tiles, tile_cells apart) by a carry-add
+    bool fresh = true;
+    uint32_t ix = 0, iy = 0, iz = 0;
     for (int64_t t = t0; t < t1; ++t) {
         if (t >= win_end) {  // block-uniform: entering a new window
             if (do_red && have)
@@ -94,15 +98,30 @@ __global__ void __launch_bounds__(STEP_THREADS, (PairOccupancy<STORE, MOVING, RE
             __syncthreads();
             win_end = sw.tile_end;
             skip = (sw.nz & 1u) != 0 || sw.tile_cells != PAIR_CELLS * (int32_t)blockDim.x;
+            fresh = true;
             if (skip && threadIdx.x == 0) atomicCAS(&g_pair_status, 0, (sw.nz & 1u) ? 0x201 : 0x202);
         }
         if (sw.inactive || skip) continue;  // block-uniform
         have = true;
         const uint32_t N = sw.N, nx = sw.nx, ny = sw.ny, nz = sw.nz;
         const uint32_t c0 = (uint32_t)((t - sw.tile_begin) * sw.tile_cells) + PAIR_CELLS * threadIdx.x;
-        if (c0 >= N) continue;  // N is even: c0 + 1 < N as well
+        if (fresh) {
+            iz = c0 % nz;
+            const uint32_t rr = c0 / nz;
+            iy = rr % ny;
+            ix = rr / ny;
+            fresh = false;
+        } else {  // one tile on: += the tile step, single carries (each step component < its extent)
+            iz += sw.tstep_z;
+            const uint32_t cz = iz >= nz;
+            iz -= cz ? nz : 0u;
+            iy += sw.tstep_y + cz;
+            const uint32_t cy = iy >= ny;
+            iy -= cy ? ny : 0u;
+            ix += sw.tstep_x + cy;
+        }
+        if (c0 >= N) continue;  // N is even: c0 + 1 < N as well (the window's last tile)
         const uint32_t c1 = c0 + 1;
-        const uint32_t iz = c0 % nz, rr = c0 / nz, iy = rr % ny, ix = rr / ny;
         const bool open_x = sw.open_x;
         const bool inlet = open_x && ix == 0;
         const int32_t nyz = (int32_t)(ny * nz);
