@@ -296,7 +296,7 @@ PSC_HD void make_win_const(WinConst<R>& c, double tau, double fx, double fy, dou
 // incoming state; imb the node IMB momentum when IMB.
 template <typename R, bool MOVING, bool IMB, bool TRT = false>
 PSC_HD void collide_fast2(R* g, const WinConst<R>& c, R B, R kb, R usx, R usy, R usz, R irho_hint, R* mom,
-                          R* imb) {
+                          R* imb, bool want_mom = true) {
     const R kbm = kb * c.trt_ratio;
     (void)kbm;
     const R drho = (((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7]))) +
@@ -307,10 +307,12 @@ PSC_HD void collide_fast2(R* g, const WinConst<R>& c, R B, R kb, R usx, R usy, R
     const R mx = ((g[1] - g[2]) + (g[7] - g[8])) + ((g[9] - g[10]) + (g[11] - g[12])) + (g[13] - g[14]);
     const R my = ((g[3] - g[4]) + (g[7] - g[8])) + ((g[10] - g[9]) + (g[15] - g[16])) + (g[17] - g[18]);
     const R mz = ((g[5] - g[6]) + (g[11] - g[12])) + ((g[14] - g[13]) + (g[15] - g[16])) + (g[18] - g[17]);
-    mom[0] = drho;
-    mom[1] = (mx + R(0.5) * c.fx) * irho;
-    mom[2] = (my + R(0.5) * c.fy) * irho;
-    mom[3] = (mz + R(0.5) * c.fz) * irho;
+    if (want_mom) {  // (plain steps of the throughput kernels store no moments)
+        mom[0] = drho;
+        mom[1] = (mx + R(0.5) * c.fx) * irho;
+        mom[2] = (my + R(0.5) * c.fy) * irho;
+        mom[3] = (mz + R(0.5) * c.fz) * irho;
+    }
     const R uex = (mx + c.fx) * irho, uey = (my + c.fy) * irho, uez = (mz + c.fz) * irho;
     const R uu15 = R(1.5) * (uex * uex + uey * uey + uez * uez);
     const R uF = uex * c.fx + uey * c.fy + uez * c.fz;

@@ -103,7 +103,7 @@ template <typename TR, bool MOVING, bool RED>
 __device__ __forceinline__ void fast_cell(const FastWin<typename TR::T, typename TR::R, typename TR::O>& sw,
                                           typename TR::R (&g)[Q], uint32_t c, uint32_t N, bool inlet, bool do_collide,
                                           bool do_imb, typename TR::R (&mom)[4], typename TR::R (&imb)[3],
-                                          double (&red)[PSC_NRED]) {
+                                          double (&red)[PSC_NRED], bool do_mom = true) {
     using R = typename TR::R;
     constexpr bool do_red = RED;
     if (TR::scaled) {
@@ -143,16 +143,17 @@ __device__ __forceinline__ void fast_cell(const FastWin<typename TR::T, typename
                    (((g[8] + g[9]) + (g[10] + g[11])) + ((g[12] + g[13]) + (g[14] + g[15]))) +
                    ((g[16] + g[17]) + g[18]);
     const R irho = fast_rcp<R>(R(1) + drho);
+    const bool want_mom = do_mom || RED;
     if (do_collide) {
         if (sw.trt) {
-            if (moving) collide_fast2<R, MOVING, true, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
-            else collide_fast2<R, false, true, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+            if (moving) collide_fast2<R, MOVING, true, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb, want_mom);
+            else collide_fast2<R, false, true, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb, want_mom);
         } else if (do_imb || do_red) {
-            if (moving) collide_fast2<R, MOVING, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
-            else collide_fast2<R, false, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+            if (moving) collide_fast2<R, MOVING, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb, want_mom);
+            else collide_fast2<R, false, true>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb, want_mom);
         } else {
-            if (moving) collide_fast2<R, MOVING, false>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
-            else collide_fast2<R, false, false>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb);
+            if (moving) collide_fast2<R, MOVING, false>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb, want_mom);
+            else collide_fast2<R, false, false>(g, sw.c, B, kb, usx, usy, usz, irho, mom, imb, want_mom);
         }
     } else {
         const R mx = ((g[1] - g[2]) + (g[7] - g[8])) + ((g[9] - g[10]) + (g[11] - g[12])) + (g[13] - g[14]);

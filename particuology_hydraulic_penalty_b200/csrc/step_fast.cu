@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(STEP_THREADS, (StepOccupancy<STORE, MOVING, RE
             if (c >= N) continue;
             R* g = f[k];
             R mom[4], imb[3];
-            fast_cell<TR, MOVING, RED>(sw, f[k], c, N, inlet[k], do_collide, do_imb, mom, imb, red);
+            fast_cell<TR, MOVING, RED>(sw, f[k], c, N, inlet[k], do_collide, do_imb, mom, imb, red, do_mom);
             if (do_collide) {
                 T* dst = sw.dst + c;
                 uint32_t plane = 0;

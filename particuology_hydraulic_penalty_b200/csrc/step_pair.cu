@@ -152,8 +152,8 @@ __global__ void __launch_bounds__(STEP_THREADS, (PairOccupancy<STORE, MOVING, RE
             plane += N;
         }
         R mom0[4], imb0[3], mom1[4], imb1[3];
-        fast_cell<TR, MOVING, RED>(sw, g0, c0, N, inlet, do_collide, do_imb, mom0, imb0, red);
-        fast_cell<TR, MOVING, RED>(sw, g1, c1, N, inlet, do_collide, do_imb, mom1, imb1, red);
+        fast_cell<TR, MOVING, RED>(sw, g0, c0, N, inlet, do_collide, do_imb, mom0, imb0, red, do_mom);
+        fast_cell<TR, MOVING, RED>(sw, g1, c1, N, inlet, do_collide, do_imb, mom1, imb1, red, do_mom);
         if (do_collide) {
             T* dst = sw.dst + c0;
             uint32_t pl = 0;
