@@ -79,3 +79,27 @@ def test_config2_linearity_mass_and_closure():
     total = float(np.abs(s.hydro_forces).sum())
     assert total > 0.0
     assert d["momentum_residual"] <= 1e-9 * total
+
+
+def test_batch24_5000_steps_permeability_equals_solo():
+    """The batched-windows configuration at its stated length: the 24 seeded windows (edges 48-160,
+    FP32, one persistent launch per step from CUDA graphs) run 5000 steps, and every window's Darcy
+    permeability equals that of the window run alone for 5000 steps (the populations evolve bit for
+    bit alike; the FP64 window sums group their partial rows differently, hence 1e-12)."""
+    import bench
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    steps = 5000
+    wins = bench.make_windows("batch24", 0)
+    specs = [WindowSpec(w.n, w.particles, bench.TAU, bench.FORCE, bench.SUBSAMPLES) for w in wins]
+    b = PscBatch(specs, precision="fp32", graph_steps=20)
+    b.run(steps)
+    K = b.permeability(b.observe())
+    del b
+    assert np.all(np.isfinite(K)) and np.all(K > 0.0)
+    for k, spec in enumerate(specs):
+        solo = PscBatch([spec], precision="fp32", graph_steps=20)
+        solo.run(steps)
+        Ks = solo.permeability(solo.observe())[0]
+        del solo
+        assert abs(Ks - K[k]) <= 1e-12 * abs(Ks), (k, Ks, K[k])
