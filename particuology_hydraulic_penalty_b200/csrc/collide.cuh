@@ -326,85 +326,54 @@ PSC_HD void collide_fast2(R* g, const WinConst<R>& c, R B, R kb, R usx, R usy, R
         const R os = w * rho * (uu15 - uus15);
         g[0] = omk * g[0] + kb * geq + B * os - c.pw3[0] * uF;
     }
-    if (TRT) {
+    // The collision regrouped per population pair.  With geq = w drho + wrq +- asym, the solid
+    // terms os_i = (g_j - g_i) + e + h, os_j = (g_i - g_j) + e - h (e = -wrq + e_s,
+    // h = asym + h_s, e_s and h_s from the solid velocity), Guo's G = K cu - 3 pref w uF +- A,
+    // and the fluid part relaxing the pair's symmetric half with kb and its antisymmetric half
+    // with kbm (= kb for BGK; TRT: kb omega-/omega+):
+    //   g_i' = a g_i + b g_j + S + T,   g_j' = a g_j + b g_i + S - T,
+    //   a = 1 - (kb + kbm)/2 - B,  b = B + (kbm - kb)/2   (BGK: 1 - kb - B and B),
+    //   S = K cu + (kb - B) wrq + (kb w drho - 3 pref w uF) + B e_s,
+    //   T = 3 (kbm + B) w rho cu + B h_s + A,
+    // and the pair's IMB momentum B (os_i - os_j) = 2 B ((g_j - g_i) + h).  With
+    // wrq = w rho (4.5 cu^2 - 1.5 u^2), S without e_s is the quadratic cu (q cu + K) + b,
+    // q = 4.5 (kb - B) w rho, b = kb w drho - 3 pref w uF - (kb - B) w rho 1.5 u^2: two FMAs per
+    // pair.  The per-weight factors are computed once per cell.
+    const R omB = TRT ? R(1) - R(0.5) * (kb + kbm) - B : omk - B;
+    const R bB = TRT ? B + R(0.5) * (kbm - kb) : B;
+    const R kmB = kb - B, B2 = B + B;
+    const R kbd = kb * drho;
+    const R wr1 = R(W1) * rho, wr2 = R(W2) * rho;
+    const R m1 = kmB * wr1, m2 = kmB * wr2;
+    const R q1 = R(4.5) * m1, q2 = R(4.5) * m2;
+    const R b1 = (R(W1) * kbd - c.pw3[1] * uF) - m1 * uu15, b2 = (R(W2) * kbd - c.pw3[2] * uF) - m2 * uu15;
+    const R kp3 = R(3) * ((TRT ? kbm : kb) + B);
+    const R t1 = kp3 * wr1, t2 = kp3 * wr2;
+    const R a1 = R(3) * wr1, a2 = R(3) * wr2;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const int i = 2 * k + 1, j = i + 1;
-            const int cls = i < 7 ? 1 : 2;
-            const R w = R(wgt(i));
-            const R wrho = w * rho, wdrho = w * drho;
-            const R cu = csel(cxv(i), uex) + csel(cyv(i), uey) + csel(czv(i), uez);
-            const R wrq = wrho * (R(4.5) * cu * cu - uu15);
-            const R asym = R(3) * wrho * cu;
-            R e = -wrq, h = asym;
-            if (MOVING) {
-                const R cus = csel(cxv(i), usx) + csel(cyv(i), usy) + csel(czv(i), usz);
-                e += wrho * (R(4.5) * cus * cus - uus15);
-                h += R(3) * wrho * cus;
-            }
-            const R gi = g[i], gj = g[j];
-            const R d = gj - gi;
-            const R os_i = (d + e) + h;
-            const R os_j = (e - d) - h;
-            const R Gb = c.K[k] * cu - c.pw3[cls] * uF;
-            // symmetric part relaxes with kb, antisymmetric with kb * omega-/omega+
-            const R sym_neq = R(0.5) * (gi + gj) - (wdrho + wrq);
-            const R asym_neq = R(-0.5) * d - asym;
-            const R relax_s = kb * sym_neq, relax_a = kbm * asym_neq;
-            g[i] = gi - relax_s - relax_a + B * os_i + (Gb + c.A[k]);
-            g[j] = gj - relax_s + relax_a + B * os_j + (Gb - c.A[k]);
-            if (IMB) {
-                const R dm = B * (os_i - os_j);
-                ax += csel(cxv(i), dm);
-                ay += csel(cyv(i), dm);
-                az += csel(czv(i), dm);
-            }
+    for (int k = 0; k < 9; ++k) {
+        const int i = 2 * k + 1, j = i + 1;
+        const bool axis = i < 7;
+        const R wr = axis ? wr1 : wr2;
+        const R cu = csel(cxv(i), uex) + csel(cyv(i), uey) + csel(czv(i), uez);
+        R S = cu * ((axis ? q1 : q2) * cu + c.K[k]) + (axis ? b1 : b2);
+        R T = (axis ? t1 : t2) * cu + c.A[k];
+        R h = (axis ? a1 : a2) * cu;
+        if (MOVING) {
+            const R cus = csel(cxv(i), usx) + csel(cyv(i), usy) + csel(czv(i), usz);
+            S += B * (wr * (R(4.5) * cus * cus - uus15));
+            const R hs = R(3) * wr * cus;
+            T += B * hs;
+            h += hs;
         }
-    } else {
-        // BGK with the solid term regrouped.  With geq = w drho + wrq +- asym, the solid terms
-        // os_i = (g_j - g_i) + e + h, os_j = (g_i - g_j) + e - h (e = -wrq + e_s, h = asym + h_s,
-        // e_s and h_s from the solid velocity) and Guo's G = K cu - 3 pref w uF +- A:
-        //   g_i' = (1 - kb - B) g_i + B g_j + S + T,   g_j' = (1 - kb - B) g_j + B g_i + S - T,
-        //   S = K cu + (kb - B) wrq + (kb w drho - 3 pref w uF) + B e_s,
-        //   T = 3 (kb + B) w rho cu + B h_s + A,
-        // and the pair's IMB momentum B (os_i - os_j) = 2 B ((g_j - g_i) + h).  With
-        // wrq = w rho (4.5 cu^2 - 1.5 u^2), S without e_s is the quadratic cu (q cu + K) + b,
-        // q = 4.5 (kb - B) w rho, b = kb w drho - 3 pref w uF - (kb - B) w rho 1.5 u^2: two FMAs per
-        // pair.  The per-weight factors are computed once per cell.
-        const R omB = omk - B, kmB = kb - B, B2 = B + B;
-        const R kbd = kb * drho;
-        const R wr1 = R(W1) * rho, wr2 = R(W2) * rho;
-        const R m1 = kmB * wr1, m2 = kmB * wr2;
-        const R q1 = R(4.5) * m1, q2 = R(4.5) * m2;
-        const R b1 = (R(W1) * kbd - c.pw3[1] * uF) - m1 * uu15, b2 = (R(W2) * kbd - c.pw3[2] * uF) - m2 * uu15;
-        const R kp3 = R(3) * (kb + B);
-        const R t1 = kp3 * wr1, t2 = kp3 * wr2;
-        const R a1 = R(3) * wr1, a2 = R(3) * wr2;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const int i = 2 * k + 1, j = i + 1;
-            const bool axis = i < 7;
-            const R wr = axis ? wr1 : wr2;
-            const R cu = csel(cxv(i), uex) + csel(cyv(i), uey) + csel(czv(i), uez);
-            R S = cu * ((axis ? q1 : q2) * cu + c.K[k]) + (axis ? b1 : b2);
-            R T = (axis ? t1 : t2) * cu + c.A[k];
-            R h = (axis ? a1 : a2) * cu;
-            if (MOVING) {
-                const R cus = csel(cxv(i), usx) + csel(cyv(i), usy) + csel(czv(i), usz);
-                S += B * (wr * (R(4.5) * cus * cus - uus15));
-                const R hs = R(3) * wr * cus;
-                T += B * hs;
-                h += hs;
-            }
-            const R gi = g[i], gj = g[j];
-            g[i] = omB * gi + (B * gj + (S + T));
-            g[j] = omB * gj + (B * gi + (S - T));
-            if (IMB) {
-                const R dm = B2 * ((gj - gi) + h);
-                ax += csel(cxv(i), dm);
-                ay += csel(cyv(i), dm);
-                az += csel(czv(i), dm);
-            }
+        const R gi = g[i], gj = g[j];
+        g[i] = omB * gi + (bB * gj + (S + T));
+        g[j] = omB * gj + (bB * gi + (S - T));
+        if (IMB) {
+            const R dm = B2 * ((gj - gi) + h);
+            ax += csel(cxv(i), dm);
+            ay += csel(cyv(i), dm);
+            az += csel(czv(i), dm);
         }
     }
     if (IMB) {
