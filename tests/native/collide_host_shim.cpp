@@ -50,3 +50,31 @@ extern "C" void fast_collide_cells(const double* g_in, const double* solid, cons
         for (int k = 0; k < 3; ++k) imb_out[(size_t)k * ncell + c] = imb[k];
     }
 }
+
+// The per-window-constant form run by the throughput kernels (collide_fast2):
+// BGK when tau_minus is 0, else TRT.
+extern "C" void fast2_collide_cells(const double* g_in, const double* solid, const double* us, int moving, double tau,
+                                    double tau_minus, double fx, double fy, double fz, int ncell, double* g_out,
+                                    double* imb_out) {
+    using namespace psc;
+    WinConst<double> wc;
+    make_win_const(wc, tau, fx, fy, fz, tau_minus);
+    for (int c = 0; c < ncell; ++c) {
+        double g[Q];
+        for (int i = 0; i < Q; ++i) g[i] = g_in[(size_t)i * ncell + c];
+        const double al = solid[c];
+        const double B = al / (al + tau * (1.0 - al) + 1.0e-14);
+        const double kb = (1.0 - B) / tau;
+        double imb[3], mom[4];
+        const double usx = moving ? us[c] : 0.0, usy = moving ? us[ncell + c] : 0.0, usz = moving ? us[2 * ncell + c] : 0.0;
+        if (tau_minus > 0.0) {
+            if (moving) collide_fast2<double, true, true, true>(g, wc, B, kb, usx, usy, usz, 0.0, mom, imb);
+            else collide_fast2<double, false, true, true>(g, wc, B, kb, usx, usy, usz, 0.0, mom, imb);
+        } else {
+            if (moving) collide_fast2<double, true, true>(g, wc, B, kb, usx, usy, usz, 0.0, mom, imb);
+            else collide_fast2<double, false, true>(g, wc, B, kb, usx, usy, usz, 0.0, mom, imb);
+        }
+        for (int i = 0; i < Q; ++i) g_out[(size_t)i * ncell + c] = g[i];
+        for (int k = 0; k < 3; ++k) imb_out[(size_t)k * ncell + c] = imb[k];
+    }
+}

@@ -33,6 +33,8 @@ def shim(tmp_path_factory):
                                         ctypes.c_double, ctypes.c_int, P, P, P]
     lib.fast_collide_cells.argtypes = [P, P, P, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_int, P, P]
+    lib.fast2_collide_cells.argtypes = [P, P, P, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_int, P, P]
     return lib
 
 
@@ -88,3 +90,42 @@ def test_fast_collision_matches_to_roundoff(shim, moving):
     dev_ref = post.reshape(19, ncell) - orc.W[:, None]
     assert np.abs(go - dev_ref).max() <= 1e-15
     assert np.abs(io - imb.reshape(3, ncell)).max() <= 1e-15
+
+
+@pytest.mark.parametrize("moving", [False, True])
+def test_throughput_collision_matches_to_roundoff(shim, moving):
+    """collide_fast2, the regrouped per-pair form the throughput kernels run (BGK), in FP64 on the
+    host: post-collision deviations and IMB momentum equal the oracle's collision to round-off."""
+    rng = np.random.default_rng(13)
+    ncell = 4096
+    f, solid, us = random_state(rng, ncell, 1e-3)
+    tau, force = 0.8, (1e-6, 2e-7, -3e-7)
+    shp = (ncell, 1, 1)
+    post, imb = orc.collide(f, solid.reshape(shp), us.reshape(3, *shp) if moving else None, tau, force)
+    g = np.ascontiguousarray((f - orc.W[:, None, None, None]).reshape(19, ncell))
+    go = np.zeros_like(g)
+    io = np.zeros((3, ncell))
+    shim.fast2_collide_cells(_p(g), _p(solid), _p(np.ascontiguousarray(us)), int(moving), tau, 0.0, *force, ncell,
+                             _p(go), _p(io))
+    dev_ref = post.reshape(19, ncell) - orc.W[:, None]
+    assert np.abs(go - dev_ref).max() <= 1e-15
+    assert np.abs(io - imb.reshape(3, ncell)).max() <= 1e-15
+
+
+def test_throughput_trt_collision_matches_oracle_extension(shim):
+    """The same form with tau_minus > 0 equals the oracle's TRT extension (static solid) to round-off."""
+    from particuology_hydraulic_penalty_b200.engine import trt_tau_minus
+
+    rng = np.random.default_rng(17)
+    ncell = 4096
+    f, solid, us = random_state(rng, ncell, 1e-3)
+    tau, force = 0.8, (1e-6, 2e-7, -3e-7)
+    tm = trt_tau_minus(tau)
+    shp = (ncell, 1, 1)
+    g4 = f - orc.W[:, None, None, None]
+    ref = orc.collide_trt_deviation(g4, solid.reshape(shp), tau, tm, force).reshape(19, ncell)
+    g = np.ascontiguousarray(g4.reshape(19, ncell))
+    go = np.zeros_like(g)
+    io = np.zeros((3, ncell))
+    shim.fast2_collide_cells(_p(g), _p(solid), _p(np.ascontiguousarray(us)), 0, tau, tm, *force, ncell, _p(go), _p(io))
+    assert np.abs(go - ref).max() <= 1e-15
