@@ -303,3 +303,29 @@ def test_batch_set_particles_all_rejects_a_window_and_keeps_the_rest_consistent(
     for k in range(len(wins)):
         assert np.array_equal(a.loads(k)[1], b.loads(k)[1])
         assert np.array_equal(a.field(k, nat.FIELD_F), b.field(k, nat.FIELD_F))
+
+
+def test_batch_reporting_steps_after_freezing():
+    """Converged windows freeze (their state and loads stay as at convergence) and drop out of the
+    all-windows loads launch; a reporting step afterwards gives the windows still running exactly
+    the loads of a batch that never froze anything, run for the same number of steps."""
+    from particuology_hydraulic_penalty_b200 import _native as nat
+
+    wins = _three()
+    b = _batch(wins, graph_steps=10)
+    st = b.converge(tol=3e-3, check_every=20, max_steps=22)
+    conv = [bool(st[k].converged) for k in range(len(wins))]
+    done = [int(st[k].steps_done) for k in range(len(wins))]
+    assert any(conv) and not all(conv), (conv, done)
+    total = max(done)
+    st2 = b.step(2, nat.RUN_DIAG)
+    ref = _batch(wins, graph_steps=10)
+    ref.step(total + 2, nat.RUN_DIAG)
+    for k in range(len(wins)):
+        if conv[k]:
+            assert st2[k].steps_done == 0
+            continue
+        Fa, Ta = b.loads(k)
+        Fr, Tr = ref.loads(k)
+        assert np.array_equal(Fa, Fr) and np.array_equal(Ta, Tr)
+        assert np.array_equal(b.field(k, nat.FIELD_F), ref.field(k, nat.FIELD_F))
