@@ -274,8 +274,9 @@ def run_fp64_plain(windows, steps: int, warm: int):
     return per_window
 
 
-def run_fp64_exact_dropin(windows, steps: int, warm: int = 2):
-    """Per-window ms/step of the plain FP64 drop-in (reference arithmetic, per-call diagnostics)."""
+def run_fp64_exact_dropin(windows, steps: int, warm: int = E2E_WARMUP):
+    """Per-window ms/step of the plain FP64 drop-in (reference arithmetic, per-call diagnostics).
+    The untimed calls cover the first launches and one CUDA-graph capture per buffer parity."""
     import torch
 
     from particuology_hydraulic_penalty_b200 import SparsePscD3Q19
