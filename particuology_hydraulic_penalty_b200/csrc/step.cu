@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restr
 }
 
 // Window sums of the partial rows (header row: element 0 = row count; the
-// rows follow it), deterministic; for several windows in two launches:
+// rows follow it), deterministic, in two launches:
 //  1. k_reduce_segments: blockIdx.y = window; blocks stride over segments of
 //     REDUCE_SEG consecutive rows; each segment is summed by a fixed tree and
 //     its sum written over the segment's first row (the partials are consumed);
@@ -239,25 +239,6 @@ __global__ void __launch_bounds__(STEP_THREADS) k_reduce_windows(const psc_windo
         for (int k = 0; k < PSC_NRED; ++k) acc[k] += p[k];
     }
     block_reduce_store<PSC_NRED>(acc, s_red, out + (size_t)blockIdx.x * PSC_NRED);
-}
-
-// One window (a solver handle, a one-window batch): both levels in one block,
-// thread t summing rows t, t + 256, ... in order, then the fixed block tree.
-__global__ void __launch_bounds__(STEP_THREADS) k_reduce_single(const psc_window* __restrict__ wins,
-                                                                double* __restrict__ out) {
-    __shared__ double s_red[STEP_THREADS / 32][PSC_NRED];
-    const psc_window& W = wins[0];
-    const int64_t rows = partial_rows(W);
-    const double* body = W.partials + PSC_NRED;
-    double acc[PSC_NRED];
-#pragma unroll
-    for (int k = 0; k < PSC_NRED; ++k) acc[k] = 0.0;
-    for (int64_t r = threadIdx.x; r < rows; r += blockDim.x) {
-        const double* p = body + r * PSC_NRED;
-#pragma unroll
-        for (int k = 0; k < PSC_NRED; ++k) acc[k] += p[k];
-    }
-    block_reduce_store<PSC_NRED>(acc, s_red, out);
 }
 
 template <int STORE>
@@ -397,10 +378,6 @@ cudaError_t launch_step(int store, const psc_window* d_windows, int nwin, int64_
 }
 
 cudaError_t launch_reduce_windows(const psc_window* d_windows, int nwin, double* out, cudaStream_t stream) {
-    if (nwin == 1) {  // one launch instead of two: a reporting call of a solver handle sums twice
-        k_reduce_single<<<1, STEP_THREADS, 0, stream>>>(d_windows, out);
-        return cudaGetLastError();
-    }
     k_reduce_segments<<<dim3(REDUCE_SEG_BLOCKS, (unsigned)nwin), STEP_THREADS, 0, stream>>>(d_windows);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
