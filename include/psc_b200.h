@@ -514,9 +514,9 @@ int psc_batch_destroy(psc_batch* b);
 int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, int nparticles);
 /* psc_batch_set_particles for every window in one call: h_particles[k] is window k's [P_k][10]
  * array (may be NULL when nparticles[k] is 0).  All windows are staged in one host buffer and
- * uploaded with one copy.  If window k's state is rejected (NaN / Inf, null array), windows
- * 0..k-1 keep their new states, window k and the later ones their previous ones, and the call
- * returns the error. */
+ * uploaded with one copy.  Every window is checked before any takes its new state: if one is
+ * rejected (NaN / Inf, null array) the call returns the error and every window keeps its
+ * previous state. */
 int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, const int* h_nparticles);
 /* nsteps steps of every active window.  PSC_RUN_DIAG: diagnostics and loads
  * of every window at the final step into h_status[nwin] (may be NULL). */

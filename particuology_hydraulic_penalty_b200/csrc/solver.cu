@@ -375,26 +375,32 @@ bool copy_same(double* dst, const double* src, const double* ref, size_t n) {
     return diff == 0;
 }
 
-// known_same: 1 when the caller has established that hp equals the last
-// accepted state bit for bit (same count), 0 when not known.
-int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who, int known_same = 0) {
+// Finiteness of a particle state (the reference fails on NaN / Inf) as one
+// sum: v * 0 is NaN exactly for non-finite v.
+bool particles_finite(const double* hp, size_t n) {
+    double probe = 0.0;
+    for (size_t i = 0; i < n; ++i) probe += hp[i] * 0.0;
+    return probe == 0.0;
+}
+
+// known: 0 nothing known; 1 hp equals the last accepted state bit for bit
+// (same count); 2 hp differs from it and is known to be finite.
+int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who, int known = 0) {
     if (P < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
     if (P > 0 && !hp) return fail(PSC_E_INVALID, std::string(who) + ": null particle array");
     // unchanged (bitwise) since the last upload: nothing to validate or record again
     const size_t n10 = (size_t)P * 10;
     const bool same_size = P == w.P && w.hp.size() == n10;
-    const bool differs =
-        !same_size || (!known_same && n10 && std::memcmp(w.hp.data(), hp, n10 * sizeof(double)) != 0);
+    const bool differs = known == 2 || !same_size ||
+                         (known != 1 && n10 && std::memcmp(w.hp.data(), hp, n10 * sizeof(double)) != 0);
     bool mv = w.moving;
     if (differs) {
-        // finiteness (the reference fails on NaN / Inf) as one sum: v * 0 is NaN exactly for
-        // non-finite v; and whether any particle moves
-        double probe = 0.0;
+        if (known != 2 && !particles_finite(hp, n10))
+            return fail(PSC_E_INVALID, std::string(who) + ": particle state contains NaN or Inf");
+        // whether any particle moves
         mv = false;
-        for (size_t i = 0; i < n10; ++i) probe += hp[i] * 0.0;
         for (int p = 0; p < P && !mv; ++p)
             for (int k = 4; k < 10; ++k) mv = mv || hp[(size_t)p * 10 + k] != 0.0;
-        if (!(probe == 0.0)) return fail(PSC_E_INVALID, std::string(who) + ": particle state contains NaN or Inf");
     }
     const bool changed = differs;
     if (P != w.P || !w.particles.p) {
@@ -1482,34 +1488,42 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
         PSC_CUDA(b->up_dev.ensure(total + total / 4 + 64, false, b->stream), who);
     }
     PSC_CUDA(b->up_host.ensure(b->up_dev.n), who);
+    // pass 1: stage every window (an unchanged state is found in the same pass) and validate the
+    // changed ones; one rejected window leaves every window as it was
+    std::vector<int> known(nwin, 0);
     int64_t off = 0;
-    int st = PSC_OK;
-    for (size_t k = 0; k < nwin && st == PSC_OK; ++k) {
-        Window& w = *b->w[k];
+    for (size_t k = 0; k < nwin; ++k) {
+        const Window& w = *b->w[k];
         const int P = h_nparticles[k];
-        if (P > 0 && !h_particles[k]) {
-            st = fail(PSC_E_INVALID, std::string(who) + ": null particle array");
-            break;
-        }
-        // stage the window's particles; an unchanged state is found in the same pass
-        const size_t n10 = (size_t)std::max(P, 0) * 10;
-        int same = 0;
+        if (P > 0 && !h_particles[k])
+            return fail(PSC_E_INVALID, std::string(who) + ": null particle array (window " + std::to_string(k) + ")");
+        const size_t n10 = (size_t)P * 10;
+        bool same = P == 0 && w.P == 0 && w.hp.empty();  // (empty before and now)
         if (P > 0 && P == w.P && w.hp.size() == n10)
-            same = copy_same(b->up_host.p + off, h_particles[k], w.hp.data(), n10) ? 1 : 0;
+            same = copy_same(b->up_host.p + off, h_particles[k], w.hp.data(), n10);
         else if (P > 0)
             std::memcpy(b->up_host.p + off, h_particles[k], n10 * sizeof(double));
-        st = window_accept_particles(w, h_particles[k], P, b->stream, who, same);
-        if (st != PSC_OK) break;  // (a rejected window keeps its previous state)
+        if (!same && !particles_finite(h_particles[k], n10))
+            return fail(PSC_E_INVALID,
+                        std::string(who) + ": particle state contains NaN or Inf (window " + std::to_string(k) + ")");
+        known[k] = same ? 1 : 2;
+        off += (int64_t)P * 10;
+    }
+    // pass 2: every window takes its staged state
+    off = 0;
+    for (size_t k = 0; k < nwin; ++k) {
+        Window& w = *b->w[k];
+        const int P = h_nparticles[k];
+        PSC_TRY(window_accept_particles(w, h_particles[k], P, b->stream, who, known[k]));
         w.ext_particles = b->up_dev.p + off;
         off += (int64_t)P * 10;
     }
-    // the windows accepted so far (all of them unless one was rejected) read their staged states
     if (off > 0)
         PSC_CUDA(cudaMemcpyAsync(b->up_dev.p, b->up_host.p, (size_t)off * sizeof(double), cudaMemcpyHostToDevice,
                                  b->stream),
                  who);
     PSC_CUDA(cudaEventRecord(b->up_done, b->stream), who);
-    return st;
+    return PSC_OK;
 }
 
 int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_status) {

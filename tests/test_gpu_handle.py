@@ -280,11 +280,11 @@ def test_dropin_reporting_graph_follows_particle_updates():
     run(parts[:-1], 5, 10)
 
 
-def test_batch_set_particles_all_rejects_a_window_and_keeps_the_rest_consistent():
-    """A non-finite particle state in one window: psc_batch_set_particles_all fails, the windows
-    before it take their new states (staged and uploaded), the rejected window and those after it
-    keep their previous ones.  Torques (arms from the uploaded centres) match a batch given
-    exactly those states."""
+def test_batch_set_particles_all_rejects_a_window_and_keeps_every_state():
+    """A non-finite particle state in one window: psc_batch_set_particles_all fails and no window takes
+    a new state, including the windows before the rejected one (one of them also changes its particle
+    count, which moves every later window's slot in the shared upload buffer).  Fields and torques
+    match a batch that was never given the new states."""
     from particuology_hydraulic_penalty_b200 import _native as nat
 
     wins = _three()
@@ -293,17 +293,25 @@ def test_batch_set_particles_all_rejects_a_window_and_keeps_the_rest_consistent(
     new = [w.particles.copy() for w in wins]
     for m in new:
         m[:, 0] += 0.25
+    new[0] = new[0][:-1]  # one particle fewer in window 0
     bad = [new[0], new[1].copy(), new[2]]
     bad[1][0, 2] = np.nan
     with pytest.raises(nat.PscError):
         b.set_particles_all(bad)
-    a.set_particles(0, new[0])
     a.step(2, nat.RUN_DIAG)
     b.step(2, nat.RUN_DIAG)
     for k in range(len(wins)):
         assert np.array_equal(a.loads(k)[1], b.loads(k)[1])
         assert np.array_equal(a.field(k, nat.FIELD_F), b.field(k, nat.FIELD_F))
-
+    # and a valid set afterwards is taken by every window
+    b.set_particles_all(new)
+    for k, m in enumerate(new):
+        a.set_particles(k, m)
+    a.step(2, nat.RUN_DIAG)
+    b.step(2, nat.RUN_DIAG)
+    for k in range(len(wins)):
+        assert np.array_equal(a.loads(k)[1], b.loads(k)[1])
+        assert np.array_equal(a.field(k, nat.FIELD_F), b.field(k, nat.FIELD_F))
 
 def test_batch_reporting_steps_after_freezing():
     """Converged windows freeze (their state and loads stay as at convergence) and drop out of the
