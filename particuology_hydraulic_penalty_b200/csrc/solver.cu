@@ -1483,11 +1483,8 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
     }
     // one staging buffer and one host-to-device copy for all windows
     PSC_CUDA(cudaEventSynchronize(b->up_done), who);  // the previous upload has left the staging buffer
-    if (b->up_dev.n < total) {
-        PSC_CUDA(cudaStreamSynchronize(b->stream), who);  // kernels may still read the old buffer
-        PSC_CUDA(b->up_dev.ensure(total + total / 4 + 64, false, b->stream), who);
-    }
-    PSC_CUDA(b->up_host.ensure(b->up_dev.n), who);
+    const int64_t cap = b->up_dev.n < total ? total + total / 4 + 64 : b->up_dev.n;
+    PSC_CUDA(b->up_host.ensure(cap), who);
     // pass 1: stage every window (an unchanged state is found in the same pass) and validate the
     // changed ones; one rejected window leaves every window as it was
     std::vector<int> known(nwin, 0);
@@ -1508,6 +1505,16 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
                         std::string(who) + ": particle state contains NaN or Inf (window " + std::to_string(k) + ")");
         known[k] = same ? 1 : 2;
         off += (int64_t)P * 10;
+    }
+    // the device buffer grows only now: until every window is accepted the windows keep reading
+    // the current one
+    if (b->up_dev.n < total) {
+        PSC_CUDA(cudaStreamSynchronize(b->stream), who);  // kernels may still read the old buffer
+        const cudaError_t e = b->up_dev.ensure(cap, false, b->stream);
+        if (e != cudaSuccess) {  // the old buffer is gone: the windows read their own device copies
+            for (auto& wp : b->w) wp->ext_particles = nullptr;
+            return cuda_fail(e, who);
+        }
     }
     // pass 2: every window takes its staged state
     off = 0;

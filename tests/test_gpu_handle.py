@@ -283,8 +283,9 @@ def test_dropin_reporting_graph_follows_particle_updates():
 def test_batch_set_particles_all_rejects_a_window_and_keeps_every_state():
     """A non-finite particle state in one window: psc_batch_set_particles_all fails and no window takes
     a new state, including the windows before the rejected one (one of them also changes its particle
-    count, which moves every later window's slot in the shared upload buffer).  Fields and torques
-    match a batch that was never given the new states."""
+    count, which moves every later window's slot in the shared upload buffer), and a rejected set
+    that would need a larger upload buffer leaves the windows on the buffer they read.  Fields and
+    torques match a batch that was given only the accepted states."""
     from particuology_hydraulic_penalty_b200 import _native as nat
 
     wins = _three()
@@ -307,6 +308,17 @@ def test_batch_set_particles_all_rejects_a_window_and_keeps_every_state():
     b.set_particles_all(new)
     for k, m in enumerate(new):
         a.set_particles(k, m)
+    a.step(2, nat.RUN_DIAG)
+    b.step(2, nat.RUN_DIAG)
+    for k in range(len(wins)):
+        assert np.array_equal(a.loads(k)[1], b.loads(k)[1])
+        assert np.array_equal(a.field(k, nat.FIELD_F), b.field(k, nat.FIELD_F))
+    # a rejected set that needs a larger upload buffer than the last one: the windows keep reading
+    # the states uploaded before (the buffer is not replaced under them)
+    grown = [new[0], np.concatenate([new[1]] * 4), new[2]]
+    grown[1][-1, 0] = np.inf
+    with pytest.raises(nat.PscError):
+        b.set_particles_all(grown)
     a.step(2, nat.RUN_DIAG)
     b.step(2, nat.RUN_DIAG)
     for k in range(len(wins)):
