@@ -12,8 +12,11 @@ GPU) exceed the 126 MB L2, so no flush is needed between steps.
 Also reported on the same line:
   fp64_plain  -- the same windows solved one at a time in FP64 (deviation
                  storage, one launch per step, no graph): MLUPS, windows/hour
-                 at 5000 steps, and the FP32/FP64 permeability difference
-                 after the same number of steps from rest
+                 at 5000 steps
+  perm_error  -- the accuracy gate (<= 1e-4): the benchmark batch's per-window
+                 Darcy K in FP32 against FP64 storage at the same step count
+                 (1000 steps from rest, both counts printed), and the 96^3
+                 packed-bed windows run to steady state in both precisions
   fp64_exact_dropin -- the plain FP64 drop-in (reference arithmetic, per-call
                  diagnostics), one window at a time, and the windows/hour ratio
   e2e         -- MLUPS through the batched C ABI with host buffers: every step
@@ -113,17 +116,56 @@ def cpu_model() -> str:
 # clocks
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU, polled through NVML from a thread every ~1 ms
+    (read-only queries), so that even a timed region of a few milliseconds holds several samples.
+    ``mark(True)`` / ``mark(False)`` bracket the timed region; ``stop()`` reports the samples taken
+    inside it (and says so), else every sample of the sampler's window.  Falls back to
+    ``nvidia-smi -lms 100`` when NVML is unavailable."""
+
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NVML_REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                    ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_s: float = 0.001):
         self.index = index
+        self.period = period_s
         self.proc = None
-        self.t_on = None
-        self.t_off = None
+        self.thread = None
+        self.samples = []  # (t, sm_mhz, sm_max_mhz, reasons bitmask)
+        self.region = [None, None]
+        self._stop = None
+        self.t0 = None
+
+    def _poll(self, nvml, handle):
+        import time as _t
+
+        smax = nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            try:
+                sm = nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)
+                rs = nvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                self.samples.append((_t.perf_counter(), float(sm), float(smax), int(rs)))
+            except Exception:  # a failed query drops one sample
+                pass
+            self._stop.wait(self.period)
 
     def start(self):
+        import threading
+
+        self.t0 = time.perf_counter()
+        try:
+            import pynvml as nvml
+
+            nvml.nvmlInit()
+            handle = nvml.nvmlDeviceGetHandleByIndex(self.index)
+            self._stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nvml, handle), daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -131,7 +173,25 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def mark(self, begin: bool):
+        self.region[0 if begin else 1] = time.perf_counter()
+
     def stop(self) -> dict:
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join(timeout=5)
+            a, b = self.region
+            inside = [s for s in self.samples if a is not None and b is not None and a <= s[0] <= b]
+            use = inside or self.samples
+            if not use:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            reasons = sorted({name for s in use for name, bit in self.NVML_REASONS if s[3] & bit})
+            out = {"sm_mhz": statistics.median(s[1] for s in use), "sm_max_mhz": max(s[2] for s in use),
+                   "reasons": reasons, "samples": len(use), "source": "nvml, ~1 ms polling",
+                   "window": "timed region" if inside else "whole GPU phase (no sample fell inside the timed region)"}
+            if a is not None and b is not None:
+                out["timed_region_ms"] = round((b - a) * 1e3, 2)
+            return out
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -157,7 +217,8 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi -lms 100",
+                "window": "whole GPU phase (100 ms sampling cannot resolve the timed region)"}
 
 
 def measured_peak_hbm():
@@ -194,45 +255,92 @@ def ncu_traffic(kernel_tag: str, launch_kernel: str = "direct"):
 # ---------------------------------------------------------------------------
 # GPU side
 # ---------------------------------------------------------------------------
-def dist_setup():
+def free_port() -> int:
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return int(s.getsockname()[1])
+
+
+def spawn_ranks(n: int, cmd: list[str], timeout_s: float | None = None) -> int:
+    """Run ``cmd`` as ``n`` local ranks (one process per GPU), the way torchrun would: RANK,
+    LOCAL_RANK, WORLD_SIZE, LOCAL_WORLD_SIZE and MASTER_ADDR / MASTER_PORT (127.0.0.1, a free port)
+    set per process.  Rank 0 keeps this process's stdout (it prints the JSON line); the other
+    ranks' stdout is discarded, their stderr kept.  If a rank fails, the others are terminated
+    after a grace period (their next collective would wait for it until the process-group
+    timeout).  Returns the first non-zero exit code, else 0."""
+    port = free_port()
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen(cmd, env=env, stdout=None if r == 0 else subprocess.DEVNULL))
+    t0 = time.monotonic()
+    failed_at = None
+    while True:
+        codes = [p.poll() for p in procs]
+        if all(c is not None for c in codes):
+            break
+        if failed_at is None and any(c not in (None, 0) for c in codes):
+            failed_at = time.monotonic()
+        late = failed_at is not None and time.monotonic() - failed_at > 30.0
+        over = timeout_s is not None and time.monotonic() - t0 > timeout_s
+        if late or over:
+            for p in procs:
+                if p.poll() is None:
+                    p.terminate()
+            for p in procs:
+                try:
+                    p.wait(timeout=30)
+                except subprocess.TimeoutExpired:
+                    p.kill()
+                    p.wait()
+            break
+        time.sleep(0.05)
+    codes = [p.returncode for p in procs]
+    return next((c for c in codes if c != 0), 0)
+
+
+def dist_setup(backend: str | None = None):
+    """(world, rank, local rank) from the torchrun environment; initialises the process group when
+    world > 1 (NCCL on GPUs, gloo for CPU-only processes) with a short timeout."""
     import torch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+    if backend == "nccl":
+        torch.cuda.set_device(local if world > 1 else 0)
     if world > 1:
         import datetime
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(0)
+        kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
     return world, rank, local
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def _reduce_scalar(x: float, world: int, op: str) -> float:
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    return _reduce_scalar(x, world, "max")
 
 
 def sum_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce_scalar(x, world, "sum")
 
 
 def barrier(world: int):
@@ -365,6 +473,63 @@ def run_e2e_batch(windows, steps: int, graph_steps: int):
                    "all windows", "steps": steps}
 
 
+ACCURACY_STEPS = 1000  # equal-step FP32 / FP64 comparison of the benchmark batch
+
+
+def perm_error_equal_steps(specs, batch32, graph_steps: int, steps: int = ACCURACY_STEPS) -> dict:
+    """Darcy K of the FP32 batch against the same windows in FP64 storage at the SAME step count from
+    rest: the FP32 batch (the timed one) is advanced to ``steps`` (or kept where it is if it went
+    further), a fresh FP64 batch runs exactly as many; both counts are reported."""
+    import torch
+
+    from particuology_hydraulic_penalty_b200.batch import PscBatch
+
+    target = max(int(steps), batch32.steps_done)
+    batch32.run(target - batch32.steps_done)
+    k32 = batch32.permeability()
+    b64 = PscBatch(specs, precision="fp64", graph_steps=graph_steps)
+    b64.run(target)
+    k64 = b64.permeability()
+    s32, s64 = batch32.steps_done, b64.steps_done
+    del b64
+    torch.cuda.empty_cache()
+    if s32 != s64:
+        raise RuntimeError(f"FP32 / FP64 step counts differ: {s32} vs {s64}")
+    err = np.abs(k32 - k64) / np.maximum(np.abs(k64), 1e-300)
+    return {"steps_fp32": int(s32), "steps_fp64": int(s64), "max": float(err.max()),
+            "median": float(np.median(err)), "windows": len(err),
+            "what": "per-window Darcy K, FP32 deviation storage vs FP64 deviation storage, same windows, "
+                    "same step count from rest"}
+
+
+def perm_error_steady(tol: float = 1.0e-8, check_every: int = 200, max_steps: int = 100000) -> dict:
+    """The packed-bed permeability case (one seeded 96^3 window in its three geometries) run to
+    steady state in FP32 and in FP64 storage; relative K error of FP32 against FP64."""
+    import torch
+
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+    from particuology_hydraulic_penalty_b200.batch import PscBatch, WindowSpec
+
+    wins = [wgen.make_window(96, kind, 1000) for kind in wgen.GEOMETRY_TYPES]
+    specs = [WindowSpec(w.n, w.particles, TAU, FORCE, SUBSAMPLES, name=w.kind) for w in wins]
+    res = {}
+    for prec in ("fp64", "fp32"):
+        b = PscBatch(specs, precision=prec, graph_steps=20)
+        r = b.run_to_convergence(tol=tol, check_every=check_every, max_steps=max_steps)
+        res[prec] = r
+        del b
+        torch.cuda.empty_cache()
+    k64, k32 = res["fp64"]["permeability"], res["fp32"]["permeability"]
+    err = np.abs(k32 - k64) / np.abs(k64)
+    return {"windows": [w.kind for w in wins], "rel_err": [float(e) for e in err], "max": float(err.max()),
+            "K_fp64": [float(k) for k in k64],
+            "steps_fp64": [int(s) for s in res["fp64"]["steps"]], "steps_fp32": [int(s) for s in res["fp32"]["steps"]],
+            "converged": bool(res["fp64"]["converged"].all() and res["fp32"]["converged"].all()),
+            "criterion": f"per-step relative change of K < {tol:g}, checked every {check_every} steps",
+            "what": "96^3 skeleton / passive fines / preloaded fines, S=4, tau=0.8, F=1e-6 x, each precision "
+                    "run to its own steady state"}
+
+
 WORKLOADS = {
     "batch24": "batch24: 24 uneven periodic pore windows, edges {{48,64,96,128,160}}, S=4, BGK tau=0.8, "
                "F=1e-6 x, {prec} deviation storage, one persistent launch per step, CUDA graph",
@@ -411,11 +576,16 @@ def run_ours(args):
     batch.prepare()  # graph capture of both buffer parities happens here, outside the timed region
     batch.run(args.warmup)
     torch.cuda.synchronize()
-    ms = timed(lambda: batch.run(args.steps), world)
+
+    def timed_steps():
+        clocks.mark(True)
+        batch.run(args.steps)
+
+    ms = timed(timed_steps, world)
+    clocks.mark(False)
     clk = clocks.stop()
     ms_max = max_over_ranks(ms, world)
     red = batch.observe()
-    k32 = batch.permeability(red)
     nonfinite = bool(batch.nonfinite(red).any())
     cells_rank = batch.total_cells
     cells_all = sum_over_ranks(float(cells_rank), world)
@@ -446,15 +616,11 @@ def run_ours(args):
         "nonfinite": nonfinite,
     }
     if rank == 0 and world == 1 and not args.no_fp64:
-        # FP32 vs FP64 permeability after the same number of steps from rest
+        # the accuracy gate: FP32 vs FP64 permeability at equal step counts, and at steady state
+        acc_equal = perm_error_equal_steps(specs, batch, args.graph_steps) if args.precision == "fp32" else None
         del batch
         torch.cuda.empty_cache()
-        b64 = PscBatch(specs, precision="fp64", graph_steps=args.graph_steps)
-        b64.run(args.warmup + args.steps)
-        k64 = b64.permeability()
-        del b64
-        torch.cuda.empty_cache()
-        err = np.abs(k32 - k64) / np.maximum(np.abs(k64), 1e-300)
+        acc_steady = perm_error_steady() if args.precision == "fp32" and not args.no_steady else None
         per_ms = run_fp64_plain(wins, steps=args.fp64_steps, warm=3)
         t_plain_h = sum(STEPS_PER_WINDOW * m * 1e-3 for m in per_ms) / 3600.0
         t_batch_h = STEPS_PER_WINDOW * (ms / args.steps) * 1e-3 / 3600.0  # all windows advance together
@@ -472,10 +638,13 @@ def run_ours(args):
             "windows_per_hour": round(len(wins) / t_plain_h, 1),
             "fp32_batched_windows_per_hour": round(len(wins) / t_batch_h, 1),
             "windows_per_hour_ratio": round(t_plain_h / t_batch_h, 3),
-            "perm_rel_err_max_fp32_vs_fp64": float(err.max()),
-            "perm_rel_err_note": f"after {args.warmup + args.steps} steps from rest, same windows",
             "steps_per_window_assumed": STEPS_PER_WINDOW,
         }
+        if acc_equal is not None:
+            out["fp64_plain"]["perm_rel_err_max_fp32_vs_fp64"] = acc_equal["max"]
+            out["perm_error"] = {"bound": 1e-4, "batch_equal_steps": acc_equal, "steady_state": acc_steady,
+                                 "within_bound": bool(acc_equal["max"] <= 1e-4 and
+                                                      (acc_steady is None or acc_steady["max"] <= 1e-4))}
     if rank == 0 and world == 1 and not args.no_e2e:
         out["e2e"] = run_e2e_batch(wins, steps=args.e2e_steps, graph_steps=args.graph_steps)
         out["e2e_dropin"] = run_e2e_dropin(wins, steps=max(3, args.e2e_steps // 4))
@@ -542,9 +711,18 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-steady", action="store_true", help="skip the steady-state FP32/FP64 permeability leg")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.gpus < 1:
+        ap.error("--gpus must be >= 1")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # not under torchrun: start one rank per GPU here, each running this same command line
+        sys.exit(spawn_ranks(args.gpus, [sys.executable, str(Path(__file__).resolve()), *sys.argv[1:]]))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        print(f"bench.py: WORLD_SIZE={world} overrides --gpus {args.gpus}", file=sys.stderr)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -14,6 +14,8 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -41,25 +43,43 @@ def needs_rebuild() -> bool:
     return any(p.stat().st_mtime > t for p in deps if p.exists())
 
 
+def _run(cmd: list[str]) -> subprocess.CompletedProcess:
+    return subprocess.run(cmd, cwd=str(PKG), capture_output=True, text=True, env=dict(os.environ))
+
+
 def build(verbose: bool = False, force: bool = False) -> Path:
+    """Compile every ``csrc/*.cu`` to an object in parallel (no device code crosses files, so no
+    relocatable device code is needed), then link the shared library."""
     if not force and not needs_rebuild():
         return LIB
-    cmd = [
-        nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-        "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared",
+    flags = [
+        *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+        "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
         "-I", str(PKG.parent / "include"),
-        "-o", str(LIB) + ".tmp", *map(str, sources()),
     ]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    env = dict(os.environ)
-    proc = subprocess.run(cmd, cwd=str(PKG), capture_output=True, text=True, env=env)
-    if proc.returncode != 0:
-        sys.stderr.write(proc.stdout + proc.stderr)
-        raise RuntimeError("nvcc failed building libpscb200.so")
-    if verbose:
-        sys.stderr.write(proc.stdout + proc.stderr)
-    os.replace(str(LIB) + ".tmp", LIB)
+        flags.insert(0, "-Xptxas=-v")
+    objdir = Path(tempfile.mkdtemp(prefix="pscb200_build_"))
+    try:
+        srcs = sources()
+        objs = [objdir / (s.stem + ".o") for s in srcs]
+        jobs = [[nvcc_path(), *flags, "-c", str(s), "-o", str(o)] for s, o in zip(srcs, objs)]
+        with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+            results = list(pool.map(_run, jobs))
+        failed = [(s, r) for s, r in zip(srcs, results) if r.returncode != 0]
+        for s, r in zip(srcs, results):
+            if verbose or r.returncode != 0:
+                sys.stderr.write(f"== {s.name}\n{r.stdout}{r.stderr}")
+        if failed:
+            raise RuntimeError("nvcc failed on " + ", ".join(s.name for s, _ in failed))
+        link = _run([nvcc_path(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB) + ".tmp",
+                     *map(str, objs)])
+        if link.returncode != 0:
+            sys.stderr.write(link.stdout + link.stderr)
+            raise RuntimeError("nvcc failed linking libpscb200.so")
+        os.replace(str(LIB) + ".tmp", LIB)
+    finally:
+        shutil.rmtree(objdir, ignore_errors=True)
     return LIB
 
 

@@ -91,10 +91,11 @@ def test_reference_smoke_assertions():
 
 
 # relative (vector-norm) error bounds of the deviation-storage modes after
-# the golden run, against the reference's FP64 result
+# the golden run, against the reference's FP64 result (measured on a B200: FP64
+# at most 5.4e-11, FP32 at most 7.7e-7 over these four cases)
 FAST_TOL = {
     "fp64": {"u": 1e-10, "F": 1e-10},
-    "fp32": {"u": 2e-4, "F": 2e-4},
+    "fp32": {"u": 1e-5, "F": 1e-5},
 }
 
 
