@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define PSC_ABI_VERSION 3
+#define PSC_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------- */
 #define PSC_OK 0
@@ -188,7 +188,28 @@ typedef struct psc_geometry {
     double smooth_eps;
     double* ent_alpha;        /* [capacity_entries] smooth alpha per entry (smooth mode) */
     int32_t* cl_ent;          /* [capacity_entries] entry index per cell-list slot (smooth mode) */
+    /* Loads list, for a geometry used by more than one loads call (static
+     * particles).  Every load chunk is reduced by PSC_LOAD_THREADS threads, thread
+     * t taking the chunk's entries t, t + PSC_LOAD_THREADS, ...  The list keeps,
+     * per chunk and thread, that thread's entries with a non-zero sample count in
+     * their order: slot k of thread t of chunk c is c * chunk_entries +
+     * k * PSC_LOAD_THREADS + t, holding the entry's owner weight
+     * alpha_p / max(alpha_sum, 1e-14) (load_w) and its bbox-local cell a | b << 11
+     * | k << 22 (load_abk); load_n[c * PSC_LOAD_THREADS + t] counts them.  With the
+     * three arrays set and list_ready == 0, psc_particle_loads also writes the
+     * list; with list_ready == 1 it reduces from the list instead of the whole
+     * boxes (same sums, bit for bit: each thread adds the same entries in the same
+     * order).  The caller sets list_ready after a call on the same geometry.
+     * Needs chunk_entries a multiple of PSC_LOAD_THREADS, at most 64 of them, and
+     * nx, ny <= 2048, nz <= 1024; NULL arrays = no list. */
+    double* load_w;           /* [capacity_chunks * chunk_entries] or NULL */
+    uint32_t* load_abk;       /* [capacity_chunks * chunk_entries] or NULL */
+    uint8_t* load_n;          /* [capacity_chunks * PSC_LOAD_THREADS] or NULL */
+    int32_t list_ready;
+    int32_t reserved;
 } psc_geometry;
+
+#define PSC_LOAD_THREADS 256 /* threads reducing one load chunk */
 
 /* Arguments of the adjoint kernels (one window, deviation storage F64/F32).
  * The adjoint state lambda has the arithmetic type of the storage mode
@@ -278,7 +299,9 @@ int psc_reduce_windows(const struct psc_window* d_windows, int nwin, double* out
 
 /* ---- particle loads (psc3d.py:255-281 / 375-407) ------------------------ */
 /* Per-particle force and torque from the node IMB momentum imb [3][N]
- * (imb_type 0 = float64, 1 = float32), owner weights alpha_p / alpha_sum.
+ * (imb_type 0 = float64, 1 = float32), owner weights alpha_p / alpha_sum
+ * (computed per bbox entry, or read from the geometry's loads list when
+ * list_ready).
  * chunk_partials: [capacity_chunks][6] scratch.  imb_sums: device [3] sum of
  * the node IMB momentum (PSC_RED_IMB* of the same step).  Writes forces
  * [P][3], torques [P][3] and diag [PSC_NDIAG]. */
@@ -311,8 +334,9 @@ int psc_bounceback_step(const double* f_src, double* f_dst, const uint8_t* solid
 /* ---- particle loads without caller scratch (no counterpart in the reference)
  * For callers that cannot allocate device memory -- a solver embedded in a
  * program that owns the device memory budget, or a coupling loop that must
- * not call cudaMalloc after start-up (it synchronises the device).  Same
- * results as psc_particle_loads(), but the per-chunk partial sums live in a
+ * not call cudaMalloc after start-up (it synchronises the device).  The same
+ * loads as psc_particle_loads() to round-off (its per-particle sums add the
+ * chunk partials in another order), but the per-chunk partial sums live in a
  * fixed array inside the library: PSC_LOADS_STATIC_MAX_CHUNKS x 6 doubles
  * (768 KiB) held by every GPU that loads the library until exit.
  * h_geo->capacity_chunks must not exceed PSC_LOADS_STATIC_MAX_CHUNKS
@@ -380,7 +404,8 @@ typedef struct psc_config {
     void* stream;             /* cudaStream_t for all work of the handle; NULL = a stream of its own */
     int32_t open_x;           /* 1: velocity inlet at x = 0, zero-gradient outflow at x = nx - 1
                                  (PSC_WIN_OPEN_X; not in the reference); 0: periodic */
-    int32_t reserved;         /* 0 */
+    int32_t conv_check_every; /* PSC_RUN_CONVERGE: evaluate the criterion every k steps (on steps k - 1 and
+                                 k); 0 or 1 = every step, as the reference's loop does */
     double inlet_rho;         /* open_x: inlet density */
     double inlet_u[3];        /* open_x: inlet velocity */
 } psc_config;
@@ -413,9 +438,11 @@ typedef struct psc_status {
 
 /* psc_step() flags */
 #define PSC_RUN_DIAG 1u     /* diagnostics and particle loads of the final step */
-#define PSC_RUN_CONVERGE 2u /* diagnostics every step; stop at the first step k >= conv_min_steps with
-                               |mean_uz_k - mean_uz_{k-1}| / |mean_uz_k| < conv_tol (lbm_converge,
-                               couple_psc_liggghts.py:284-296); implies PSC_RUN_DIAG */
+#define PSC_RUN_CONVERGE 2u /* stop at the first step k >= conv_min_steps, k a multiple of
+                               conv_check_every, with |mean_uz_k - mean_uz_{k-1}| / |mean_uz_k| < conv_tol
+                               (lbm_converge, couple_psc_liggghts.py:284-296; the criterion is evaluated on
+                               the device, the host reads its outcome once per block of steps); particle
+                               loads and diagnostics of the final step only; implies PSC_RUN_DIAG */
 #define PSC_RUN_FIELDS 4u   /* also write the rho / u fields of the final state (else made on demand) */
 
 /* psc_get_fields() selectors; every field is returned as float64 */
@@ -457,6 +484,15 @@ int psc_rebuild_geometry(psc_solver* h);
 int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status);
 /* Field `which` (PSC_FIELD_*) as float64 into h_dst ([N], or [19][N] for PSC_FIELD_F). */
 int psc_get_fields(psc_solver* h, int which, double* h_dst);
+/* lbm_converge (coupling_sync/couple_psc_liggghts.py:284-296) as one call: up to max_steps steps,
+ * stopping at the first step k >= min_steps (k a multiple of check_every, or max_steps) with
+ * |mean_uz_k - mean_uz_{k-1}| / max(|mean_uz_k|, 1e-30) < tol.  check_every = 1 evaluates every
+ * step, as the reference does (same iterations and residual); a larger k takes the criterion on
+ * steps k - 1 and k only and runs the steps in between without reductions.  The criterion runs on
+ * the device; the state, loads and diagnostics returned are those of the stopping step
+ * (h_status: steps_done = iterations, residual, converged, diag).  flags: 0 or PSC_RUN_FIELDS. */
+int psc_converge(psc_solver* h, int max_steps, double tol, int min_steps, int check_every, unsigned flags,
+                 psc_status* h_status);
 /* Set the post-stream populations (PscD3Q19.f = ...), absolute float64 [19][N]. */
 int psc_set_populations(psc_solver* h, const double* h_f);
 /* hydro_forces / hydro_torques [P][3] of the last step (accumulate_particle_loads,

@@ -14,7 +14,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libpscb200.so"
 HEADER_PATH = Path(__file__).resolve().parents[1] / "include" / "psc_b200.h"
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 # status codes
 PSC_OK = 0
@@ -92,6 +92,8 @@ class PscGeometry(ctypes.Structure):
         ("cl_pid", c_void_p), ("cl_cnt", c_void_p), ("alpha_sum", c_void_p), ("solid", c_void_p),
         ("level", c_void_p), ("scan_tmp", c_void_p),
         ("smooth_eps", c_double), ("ent_alpha", c_void_p), ("cl_ent", c_void_p),
+        ("load_w", c_void_p), ("load_abk", c_void_p), ("load_n", c_void_p), ("list_ready", c_int32),
+        ("reserved", c_int32),
     ]
 
 
@@ -117,7 +119,7 @@ class PscConfig(ctypes.Structure):
         ("nx", c_int32), ("ny", c_int32), ("nz", c_int32), ("subsamples", c_int32), ("store", c_int32),
         ("static_geometry", c_int32), ("device", c_int32), ("conv_min_steps", c_int32),
         ("tau", c_double), ("tau_minus", c_double), ("force", c_double * 3), ("store_scale", c_double),
-        ("conv_tol", c_double), ("stream", c_void_p), ("open_x", c_int32), ("reserved", c_int32),
+        ("conv_tol", c_double), ("stream", c_void_p), ("open_x", c_int32), ("conv_check_every", c_int32),
         ("inlet_rho", c_double), ("inlet_u", c_double * 3),
     ]
 
@@ -187,6 +189,7 @@ SIGNATURES = {
     "psc_set_particles": (c_int, [c_void_p, c_void_p, c_int]),
     "psc_rebuild_geometry": (c_int, [c_void_p]),
     "psc_step": (c_int, [c_void_p, c_int, c_uint, POINTER(PscStatus)]),
+    "psc_converge": (c_int, [c_void_p, c_int, c_double, c_int, c_int, c_uint, POINTER(PscStatus)]),
     "psc_get_fields": (c_int, [c_void_p, c_int, c_void_p]),
     "psc_set_populations": (c_int, [c_void_p, c_void_p]),
     "psc_get_loads": (c_int, [c_void_p, c_void_p, c_void_p]),

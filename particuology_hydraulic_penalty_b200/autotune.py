@@ -5,6 +5,9 @@ changes speed):
   * direct kernel, 1 or 2 cells per thread;
   * pair kernel (two consecutive z cells per thread, 2-element accesses),
     when every window has an even nz;
+  * for the direct (1 cell per thread) and pair kernels, the persistent grid:
+    the occupancy default, or 1, 2 or 4 CTAs per SM (each CTA walks a
+    contiguous run of tiles; more CTAs than fit run in waves);
   * TMA row-staged kernel, 2 / 3 / 4 pipeline stages, with the rows per tile
     chosen per window SIZE CLASS (windows of equal extent share a class).
 
@@ -97,15 +100,21 @@ def tune(batch, steps: int = 20, use_cache: bool = True, verbose: bool = False) 
     results = []
     elem = batch.windows[0].f[0].element_size()
     tma_ok = all((w.nz * elem) % 16 == 0 and w.nz % 16 == 0 for w in batch.windows)
+    sm = torch.cuda.get_device_properties(batch.device).multi_processor_count
+    grids = (0, sm, 2 * sm, 4 * sm)  # 0: SM count x occupancy
+    grid0 = batch.grid_ctas
     try:
         for cpt in (1, 2):
-            batch.configure(nat.KERNEL_DIRECT, cells_per_thread=cpt)
-            results.append(({"kernel": "direct", "cells_per_thread": cpt}, _time(batch, steps)))
-            _restore(batch, snap)
+            for grid in (grids if cpt == 1 else (0,)):
+                batch.configure(nat.KERNEL_DIRECT, cells_per_thread=cpt, grid_ctas=grid)
+                results.append(({"kernel": "direct", "cells_per_thread": cpt, "grid_ctas": grid}, _time(batch, steps)))
+                _restore(batch, snap)
         if all(w.nz % 2 == 0 for w in batch.windows):
-            batch.configure(nat.KERNEL_PAIR)
-            results.append(({"kernel": "pair"}, _time(batch, steps)))
-            _restore(batch, snap)
+            for grid in grids:
+                batch.configure(nat.KERNEL_PAIR, grid_ctas=grid)
+                results.append(({"kernel": "pair", "grid_ctas": grid}, _time(batch, steps)))
+                _restore(batch, snap)
+        batch.grid_ctas = grid0
         if tma_ok:
             # per size class: best rows (2 stages), timed on a batch of that class only
             classes = sorted({(w.nx, w.ny, w.nz) for w in batch.windows})
@@ -125,11 +134,13 @@ def tune(batch, steps: int = 20, use_cache: bool = True, verbose: bool = False) 
             for stages in (2, 3, 4):
                 if max(r * w.nz * (19 * elem + 1) for r, w in zip(rows, batch.windows)) * stages > 200 * 1024:
                     continue
-                batch.configure(nat.KERNEL_TMA, rows_per_window=rows, stages=stages)
-                results.append(({"kernel": "tma", "stages": stages, "rows_per_window": rows}, _time(batch, steps)))
+                batch.configure(nat.KERNEL_TMA, rows_per_window=rows, stages=stages, grid_ctas=0)
+                results.append(({"kernel": "tma", "stages": stages, "rows_per_window": rows, "grid_ctas": 0},
+                                _time(batch, steps)))
                 _restore(batch, snap)
     finally:
         batch.graph_steps = graph_steps
+        batch.grid_ctas = grid0
     best = min(results, key=lambda x: x[1])
     cfg = dict(best[0])
     cfg["ms_per_step"] = best[1]
@@ -149,12 +160,14 @@ def tune(batch, steps: int = 20, use_cache: bool = True, verbose: bool = False) 
 
 
 def _apply(batch, cfg: dict) -> None:
+    grid = int(cfg.get("grid_ctas", 0))
     if cfg.get("kernel") == "tma":
-        batch.configure(nat.KERNEL_TMA, stages=int(cfg["stages"]), rows_per_window=cfg["rows_per_window"])
+        batch.configure(nat.KERNEL_TMA, stages=int(cfg["stages"]), rows_per_window=cfg["rows_per_window"],
+                        grid_ctas=grid)
     elif cfg.get("kernel") == "direct":
-        batch.configure(nat.KERNEL_DIRECT, cells_per_thread=int(cfg["cells_per_thread"]))
+        batch.configure(nat.KERNEL_DIRECT, cells_per_thread=int(cfg["cells_per_thread"]), grid_ctas=grid)
     elif cfg.get("kernel") == "pair":
-        batch.configure(nat.KERNEL_PAIR)
+        batch.configure(nat.KERNEL_PAIR, grid_ctas=grid)
 
 
 class _SubBatch:

@@ -175,7 +175,8 @@ class PscBatch:
         return {"kernel": {nat.KERNEL_DIRECT: "direct", nat.KERNEL_TMA: "tma",
                            nat.KERNEL_PAIR: "pair"}[self.kernel_eff],
                 "cells_per_thread": self.cells_per_thread, "tile_rows": self.tile_rows, "stages": self.stages,
-                "rows_per_window": self.rows_per_window, "stage_bytes": self.stage_bytes}
+                "rows_per_window": self.rows_per_window, "stage_bytes": self.stage_bytes,
+                "grid_ctas": self.grid_ctas}
 
     @property
     def nwin(self) -> int:

@@ -63,11 +63,21 @@ def psc_particles_from_state(x, v, omega, radius, resolution: int, velocity_lu_s
     return out
 
 
-def lbm_converge(solver, residual_tol: float = 1.0e-8, min_steps: int = 1, max_steps: int = 20000):
+def lbm_converge(solver, residual_tol: float = 1.0e-8, min_steps: int = 1, max_steps: int = 20000,
+                 check_every: int = 1):
     """Step until |mean_uz_k - mean_uz_{k-1}| / |mean_uz_k| < tol (couple_psc_liggghts.py:284-296).
 
-    Returns (iterations, residual, converged, last diagnostics).
+    Returns (iterations, residual, converged, last diagnostics).  This package's solvers run the
+    loop natively (``run_to_convergence``: the criterion on the device, loads and diagnostics of
+    the stopping step only; ``check_every`` = k evaluates it every k steps, 1 = every step as the
+    reference).  Any other object with the reference's ``collide_stream_psc()`` runs the
+    reference's per-step loop (check_every must then be 1).
     """
+    native = getattr(solver, "run_to_convergence", None)
+    if native is not None:
+        return native(residual_tol=residual_tol, min_steps=min_steps, max_steps=max_steps, check_every=check_every)
+    if int(check_every) != 1:
+        raise ValueError("check_every > 1 needs a solver of this package")
     previous = None
     residual = math.inf
     diag: dict = {}

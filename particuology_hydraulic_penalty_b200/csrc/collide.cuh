@@ -28,7 +28,12 @@ namespace psc {
 // ===========================================================================
 struct ExactMoments {
     double rho, ux, uy, uz;
+    Divisor by_rho;  // rho with its reciprocal
 };
+
+// x / c_s^2 and x / c_s^4, correctly rounded (Markstein's correction, d3q19.cuh)
+PSC_HD double div_cs2(double x) { return xdiv_r(x, CS2, RCS2); }
+PSC_HD double div_cs2sq(double x) { return xdiv_r(x, CS2SQ, RCS2SQ); }
 
 // rho and u = (m + F/2)/rho of absolute populations f, psc3d.py:211-214.
 PSC_HD ExactMoments moments_exact(const double* f, double hfx, double hfy, double hfz) {
@@ -37,9 +42,10 @@ PSC_HD ExactMoments moments_exact(const double* f, double hfx, double hfy, doubl
 #pragma unroll
     for (int i = 1; i < Q; ++i) rho = xadd(rho, f[i]);
     m.rho = rho;
-    m.ux = xdiv(xadd(seq_moment_exact<0>(f), hfx), rho);
-    m.uy = xdiv(xadd(seq_moment_exact<1>(f), hfy), rho);
-    m.uz = xdiv(xadd(seq_moment_exact<2>(f), hfz), rho);
+    m.by_rho = make_divisor(rho);
+    m.ux = xdiv_d(xadd(seq_moment_exact<0>(f), hfx), m.by_rho);
+    m.uy = xdiv_d(xadd(seq_moment_exact<1>(f), hfy), m.by_rho);
+    m.uz = xdiv_d(xadd(seq_moment_exact<2>(f), hfz), m.by_rho);
     return m;
 }
 
@@ -51,7 +57,7 @@ PSC_HD double cm(int c, double x) { return c == 0 ? 0.0 : (c > 0 ? x : -x); }
 // face area.  This is that term, in the operation order of the oracle.
 PSC_HD double inlet_correction_exact(int i, double r, double x, double y, double z) {
     const double cu = xadd(xadd(cm(cxv(i), x), cm(cyv(i), y)), cm(czv(i), z));
-    return xdiv(xmul(xmul(2.0, xmul(wgt(i), r)), cu), CS2);
+    return div_cs2(xmul(xmul(2.0, xmul(wgt(i), r)), cu));
 }
 
 // The directions entering x = 0 from outside (c_x = +1).
@@ -64,24 +70,25 @@ PSC_HD void collide_exact(double* f, const ExactMoments& mo, double solid, bool 
                           double usz, double tau, double fx, double fy, double fz, double hfx, double hfy,
                           double hfz, double* imb) {
     const double rho = mo.rho;
+    const Divisor by_tau = make_divisor(tau);
     // u_eff = u + 0.5 F / rho   (psc3d.py:217-219)
-    const double uex = xadd(mo.ux, xdiv(hfx, rho));
-    const double uey = xadd(mo.uy, xdiv(hfy, rho));
-    const double uez = xadd(mo.uz, xdiv(hfz, rho));
+    const double uex = xadd(mo.ux, xdiv_d(hfx, mo.by_rho));
+    const double uey = xadd(mo.uy, xdiv_d(hfy, mo.by_rho));
+    const double uez = xadd(mo.uz, xdiv_d(hfz, mo.by_rho));
     // equilibrium pieces shared by all directions (psc3d.py:98, :102)
     const double uu = xadd(xadd(xmul(uex, uex), xmul(uey, uey)), xmul(uez, uez));
-    const double ct = xdiv(xmul(0.5, uu), CS2);
+    const double ct = div_cs2(xmul(0.5, uu));
     double uus = 0.0, cts = 0.0;
     if (moving) {
         uus = xadd(xadd(xmul(usx, usx), xmul(usy, usy)), xmul(usz, usz));
-        cts = xdiv(xmul(0.5, uus), CS2);
+        cts = div_cs2(xmul(0.5, uus));
     }
     // B (psc3d.py:228-229)
     const double al = solid < 0.0 ? 0.0 : (solid > 1.0 ? 1.0 : solid);
     const double B = xdiv(al, xadd(xadd(al, xmul(tau, xsub(1.0, al))), 1.0e-14));
     const double omB = xsub(1.0, B);
     // Guo prefactor and u.F (psc3d.py:108-109)
-    const double pref = xsub(1.0, xdiv(0.5, tau));
+    const double pref = xsub(1.0, xdiv_d(0.5, by_tau));
     const double uf = xadd(xadd(xmul(uex, fx), xmul(uey, fy)), xmul(uez, fz));
 
     double ix = 0.0, iy = 0.0, iz = 0.0;  // imb accumulators, index order from +0
@@ -93,9 +100,9 @@ PSC_HD void collide_exact(double* f, const ExactMoments& mo, double solid, bool 
         const double feqs = moving ? xmul(wr, xsub(1.0, cts)) : wr;
         const double f0 = f[0];
         const double os = xsub(feqs, feqf);  // (f0 - f0) + feqs - feqf
-        const double obgk = -xdiv(xsub(f0, feqf), tau);
+        const double obgk = -xdiv_d(xsub(f0, feqf), by_tau);
         const double coll = xadd(xmul(omB, obgk), xmul(B, os));
-        const double g = xmul(xmul(pref, W0), xdiv(-uf, CS2));
+        const double g = xmul(xmul(pref, W0), div_cs2(-uf));
         f[0] = xadd(f0, xadd(coll, g));
     }
 #pragma unroll
@@ -105,15 +112,15 @@ PSC_HD void collide_exact(double* f, const ExactMoments& mo, double solid, bool 
         const double wr = xmul(w, rho);
         // feq with u_eff: cu_j = -cu_i exactly, so q_j = -q_i and b_j = b_i
         const double cu = xadd(xadd(cm(cxv(i), uex), cm(cyv(i), uey)), cm(czv(i), uez));
-        const double q = xdiv(cu, CS2);
-        const double b = xdiv(xmul(xmul(0.5, cu), cu), CS2SQ);
+        const double q = div_cs2(cu);
+        const double b = div_cs2sq(xmul(xmul(0.5, cu), cu));
         const double feqf_i = xmul(wr, xsub(xadd(xadd(1.0, q), b), ct));
         const double feqf_j = xmul(wr, xsub(xadd(xadd(1.0, -q), b), ct));
         double feqs_i = wr, feqs_j = wr;  // u_s = 0: feq = w rho exactly
         if (moving) {
             const double cus = xadd(xadd(cm(cxv(i), usx), cm(cyv(i), usy)), cm(czv(i), usz));
-            const double qs = xdiv(cus, CS2);
-            const double bs = xdiv(xmul(xmul(0.5, cus), cus), CS2SQ);
+            const double qs = div_cs2(cus);
+            const double bs = div_cs2sq(xmul(xmul(0.5, cus), cus));
             feqs_i = xmul(wr, xsub(xadd(xadd(1.0, qs), bs), cts));
             feqs_j = xmul(wr, xsub(xadd(xadd(1.0, -qs), bs), cts));
         }
@@ -122,16 +129,16 @@ PSC_HD void collide_exact(double* f, const ExactMoments& mo, double solid, bool 
         const double os_i = xsub(xadd(xsub(fj, fi), feqs_i), feqf_j);
         const double os_j = xsub(xadd(xsub(fi, fj), feqs_j), feqf_i);
         // Omega_bgk = -(f - feq_f) / tau   (psc3d.py:221)
-        const double ob_i = -xdiv(xsub(fi, feqf_i), tau);
-        const double ob_j = -xdiv(xsub(fj, feqf_j), tau);
+        const double ob_i = -xdiv_d(xsub(fi, feqf_i), by_tau);
+        const double ob_j = -xdiv_d(xsub(fj, feqf_j), by_tau);
         const double coll_i = xadd(xmul(omB, ob_i), xmul(B, os_i));
         const double coll_j = xadd(xmul(omB, ob_j), xmul(B, os_j));
         // Guo: pref W ((cf - uf)/cs2 + cu cf / cs2^2), cf_j = -cf_i   (psc3d.py:110-113)
         const double cf = xadd(xadd(cm(cxv(i), fx), cm(cyv(i), fy)), cm(czv(i), fz));
         const double pw = xmul(pref, w);
-        const double t2 = xdiv(xmul(cu, cf), CS2SQ);
-        const double g_i = xmul(pw, xadd(xdiv(xsub(cf, uf), CS2), t2));
-        const double g_j = xmul(pw, xadd(xdiv(xsub(-cf, uf), CS2), t2));
+        const double t2 = div_cs2sq(xmul(cu, cf));
+        const double g_i = xmul(pw, xadd(div_cs2(xsub(cf, uf)), t2));
+        const double g_j = xmul(pw, xadd(div_cs2(xsub(-cf, uf)), t2));
         f[i] = xadd(fi, xadd(coll_i, g_i));
         f[j] = xadd(fj, xadd(coll_j, g_j));
         // node IMB momentum, sequential in index order (i then j)
@@ -414,14 +421,15 @@ PSC_HD void collide_bb_exact(double* f, bool solid, double tau, double fx, doubl
     mom[2] = mo.uy;
     mom[3] = mo.uz;
     const double rho = mo.rho, ux = mo.ux, uy = mo.uy, uz = mo.uz;
+    const Divisor by_tau = make_divisor(tau);
     const double uu = xadd(xadd(xmul(ux, ux), xmul(uy, uy)), xmul(uz, uz));
-    const double ct = xdiv(xmul(0.5, uu), CS2);
-    const double pref = xsub(1.0, xdiv(0.5, tau));
+    const double ct = div_cs2(xmul(0.5, uu));
+    const double pref = xsub(1.0, xdiv_d(0.5, by_tau));
     const double uf = xadd(xadd(xmul(ux, fx), xmul(uy, fy)), xmul(uz, fz));
     {
         const double feq = xmul(xmul(W0, rho), xsub(1.0, ct));
-        const double g = xmul(xmul(pref, W0), xdiv(-uf, CS2));
-        f[0] = xadd(xsub(f[0], xdiv(xsub(f[0], feq), tau)), g);
+        const double g = xmul(xmul(pref, W0), div_cs2(-uf));
+        f[0] = xadd(xsub(f[0], xdiv_d(xsub(f[0], feq), by_tau)), g);
     }
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
@@ -429,17 +437,17 @@ PSC_HD void collide_bb_exact(double* f, bool solid, double tau, double fx, doubl
         const double w = wgt(i);
         const double wr = xmul(w, rho);
         const double cu = xadd(xadd(cm(cxv(i), ux), cm(cyv(i), uy)), cm(czv(i), uz));
-        const double q = xdiv(cu, CS2);
-        const double b = xdiv(xmul(xmul(0.5, cu), cu), CS2SQ);
+        const double q = div_cs2(cu);
+        const double b = div_cs2sq(xmul(xmul(0.5, cu), cu));
         const double feq_i = xmul(wr, xsub(xadd(xadd(1.0, q), b), ct));
         const double feq_j = xmul(wr, xsub(xadd(xadd(1.0, -q), b), ct));
         const double cf = xadd(xadd(cm(cxv(i), fx), cm(cyv(i), fy)), cm(czv(i), fz));
         const double pw = xmul(pref, w);
-        const double t2 = xdiv(xmul(cu, cf), CS2SQ);
-        const double g_i = xmul(pw, xadd(xdiv(xsub(cf, uf), CS2), t2));
-        const double g_j = xmul(pw, xadd(xdiv(xsub(-cf, uf), CS2), t2));
-        f[i] = xadd(xsub(f[i], xdiv(xsub(f[i], feq_i), tau)), g_i);
-        f[j] = xadd(xsub(f[j], xdiv(xsub(f[j], feq_j), tau)), g_j);
+        const double t2 = div_cs2sq(xmul(cu, cf));
+        const double g_i = xmul(pw, xadd(div_cs2(xsub(cf, uf)), t2));
+        const double g_j = xmul(pw, xadd(div_cs2(xsub(-cf, uf)), t2));
+        f[i] = xadd(xsub(f[i], xdiv_d(xsub(f[i], feq_i), by_tau)), g_i);
+        f[j] = xadd(xsub(f[j], xdiv_d(xsub(f[j], feq_j), by_tau)), g_j);
     }
 }
 

@@ -8,6 +8,8 @@
 
 #include <stdint.h>
 
+#include <cmath>
+
 #if defined(__CUDACC__)
 #define PSC_HD __host__ __device__ __forceinline__
 #else
@@ -53,6 +55,9 @@ PSC_HD constexpr double wgt(int i) { return i == 0 ? W0 : (i < 7 ? W1 : W2); }
 // c_s^2 = 1/3 and (c_s^2)^2 as the reference computes them (psc3d.py:43, :102).
 constexpr double CS2 = 1.0 / 3.0;
 constexpr double CS2SQ = CS2 * CS2;
+// Their correctly rounded reciprocals (compile-time IEEE divisions), for xdiv_r.
+constexpr double RCS2 = 1.0 / CS2;
+constexpr double RCS2SQ = 1.0 / CS2SQ;
 
 // The nine directions 2k+1 (k = 0..8) each have their opposite at 2k+2.
 
@@ -73,6 +78,58 @@ PSC_HD double xsub(double a, double b) { return a - b; }
 PSC_HD double xmul(double a, double b) { return a * b; }
 PSC_HD double xdiv(double a, double b) { return a / b; }
 #endif
+
+#if defined(__CUDA_ARCH__)
+PSC_HD double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+#else
+PSC_HD double xfma(double a, double b, double c) { return std::fma(a, b, c); }  // correctly rounded (C99 fma)
+#endif
+
+// ---------------------------------------------------------------------------
+// Correctly rounded x / y from r = RN(1/y), for a divisor known in advance.
+//
+// Markstein's theorem (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990;
+// "IA-64 and Elementary Functions", 2000): if r = RN(1/y) and q is a faithful
+// approximation of x/y, the remainder e = x - q y is exactly representable (an
+// FMA computes it exactly) and RN(q + e r) = RN(x/y).
+//   q0 = RN(x r) is within 1.5 ulp of x/y (|x r - x/y| <= u |x/y| <= ulp, plus
+//        half an ulp of rounding), not necessarily faithful;
+//   q1 = RN(q0 + RN(x - q0 y) r) has error 1/2 ulp + O(u) ulp: faithful;
+//   q2 = RN(q1 + (x - q1 y) r) = RN(x/y) by the theorem.
+// Range: 2^-8 <= |y| <= 2^8 (checked by the caller: c_s^2, c_s^4, tau and rho
+// here) and 2^-900 <= |x| <= 2^900, so that no remainder is subnormal and no
+// quotient overflows.  x = +-0 gives x r (the signed zero of x / y); any other
+// x outside the range (subnormal, huge, inf, NaN) takes the IEEE division.
+// ---------------------------------------------------------------------------
+PSC_HD bool div_r_divisor_ok(double y) {
+    const double a = y < 0.0 ? -y : y;
+    return a >= 0x1p-8 && a <= 0x1p8;
+}
+
+PSC_HD double xdiv_r(double x, double y, double r) {
+    const double q0 = xmul(x, r);
+    const double q1 = xfma(xfma(-q0, y, x), r, q0);
+    const double q2 = xfma(xfma(-q1, y, x), r, q1);
+    const double ax = x < 0.0 ? -x : x;
+    if (ax >= 0x1p-900 && ax <= 0x1p900) return q2;
+    return x == 0.0 ? q0 : xdiv(x, y);
+}
+
+// A divisor with its reciprocal RN(1/y): x / y by xdiv_r when y is in range,
+// else by the IEEE division.
+struct Divisor {
+    double y, r;
+    bool ok;
+};
+PSC_HD Divisor make_divisor(double y) {
+    Divisor d;
+    d.y = y;
+    d.ok = div_r_divisor_ok(y);
+    d.r = d.ok ? xdiv(1.0, y) : 0.0;
+    return d;
+}
+PSC_HD double xdiv_d(double x, const Divisor& d) { return d.ok ? xdiv_r(x, d.y, d.r) : xdiv(x, d.y); }
 
 // c * x for a lattice component c in {-1, 0, 1}.  A zero product is returned
 // as +0; it only ever feeds an addition with a non-zero partner or an exact

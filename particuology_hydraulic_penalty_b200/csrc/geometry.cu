@@ -427,15 +427,20 @@ __device__ __forceinline__ void cp_async_wait() {
 // fixed mixed-radix stride with carries (one 32-bit division per chunk).
 // s_al holds count / S^3 for every count; cap_entries is the length of
 // ent_cnt (the count pairs are read as aligned 32-bit words inside it).
+//
+// With lw set, the thread's entries with a non-zero count also go into the
+// loads list (slots slot0, slot0 + blockDim.x, ...: owner weight and bbox-local
+// cell, in this order); returns how many.
 template <typename I>
-__device__ __forceinline__ void chunk_thread_sums(const ChunkDesc& dsc, const double* particles,
-                                                  const uint16_t* ent_cnt, int64_t cap_entries,
-                                                  const double* alpha_sum, const I* imb, uint32_t N, uint32_t ny,
-                                                  uint32_t nz, const double* s_al, LoadRing<I>& ring,
-                                                  double (&acc)[6]) {
+__device__ __forceinline__ uint32_t chunk_thread_sums(const ChunkDesc& dsc, const double* particles,
+                                                      const uint16_t* ent_cnt, int64_t cap_entries,
+                                                      const double* alpha_sum, const I* imb, uint32_t N, uint32_t ny,
+                                                      uint32_t nz, const double* s_al, LoadRing<I>& ring,
+                                                      double (&acc)[6], double* lw, uint32_t* labk, int64_t slot0) {
     const int64_t e0 = dsc.e0, e1 = dsc.e1;
     const int tid = threadIdx.x;
-    if (e0 + tid >= e1) return;
+    uint32_t listed = 0;
+    if (e0 + tid >= e1) return listed;
     const double* q = particles + (size_t)dsc.p * PF;
     const uint32_t ey = (uint32_t)dsc.ey, ez = (uint32_t)dsc.ez;
     // bbox-local coordinates of this thread's first entry, and the stride
@@ -490,6 +495,12 @@ __device__ __forceinline__ void chunk_thread_sums(const ChunkDesc& dsc, const do
             // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
             const double al = s_al[cnt];
             const double ow = xdiv(al, as > 1.0e-14 ? as : 1.0e-14);
+            if (lw) {
+                const int64_t sl = slot0 + (int64_t)listed * blockDim.x;
+                lw[sl] = ow;
+                labk[sl] = a | (b << 11) | (k << 22);
+                ++listed;
+            }
             const double nfx = -xmul(ow, mx);
             const double nfy = -xmul(ow, my);
             const double nfz = -xmul(ow, mz);
@@ -517,6 +528,7 @@ __device__ __forceinline__ void chunk_thread_sums(const ChunkDesc& dsc, const do
         a += step_a + cb;
     }
     cp_async_wait<0>();  // nothing in flight into the ring when the next chunk starts
+    return listed;
 }
 
 // One block per chunk of one particle's bbox entries.
@@ -537,8 +549,108 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
         // thread 0 overwrites the row with the chunk's sums
         const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        chunk_thread_sums<I>(dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum, imb, N, (uint32_t)g.ny,
-                             (uint32_t)g.nz, s_al, ring, acc);
+        const bool list = g.load_w && g.load_abk && g.load_n;  // write the loads list too
+        const uint32_t listed = chunk_thread_sums<I>(
+            dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum, imb, N, (uint32_t)g.ny, (uint32_t)g.nz, s_al,
+            ring, acc, list ? g.load_w : nullptr, g.load_abk, chunk * g.chunk_entries + threadIdx.x);
+        if (list) g.load_n[chunk * LOAD_THREADS + threadIdx.x] = (uint8_t)listed;
+        block_sum<6>(acc, s);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
+        }
+    }
+}
+
+// The list path: the chunk's sums from the loads list a previous call on the
+// same geometry wrote.  Thread t reads its own entries of the chunk (slots
+// slot0 + k * blockDim.x, k < its count: coalesced over the threads) in the
+// order chunk_thread_sums visits them and does the same arithmetic on each, so
+// the sums are bitwise the same; gone are the zero-count entries, the count
+// and alpha-sum gathers and the FP64 division.  A thread loads the weights and
+// cells of U list entries, then their IMB momentum, and only then sums: up to
+// U + U and then 3U loads in flight per thread.
+// List entries per pass: enough loads in flight at two CTAs per SM without
+// spilling (the many-window kernel holds its job's fields in registers, the
+// single-window one reads them from kernel parameters).
+#ifndef PSC_LIST_UNROLL
+#define PSC_LIST_UNROLL 8
+#endif
+#ifndef PSC_LIST_UNROLL_MULTI
+#define PSC_LIST_UNROLL_MULTI 6
+#endif
+template <typename I, bool MULTI>
+constexpr int list_unroll() {
+    return sizeof(I) == 8 ? 4 : (MULTI ? PSC_LIST_UNROLL_MULTI : PSC_LIST_UNROLL);
+}
+static_assert(LOAD_THREADS == PSC_LOAD_THREADS, "the loads list layout assumes PSC_LOAD_THREADS threads per chunk");
+
+template <typename I, int U>
+__device__ __forceinline__ void chunk_thread_sums_list(const ChunkDesc& dsc, const double* particles,
+                                                       const double* lw, const uint32_t* labk, uint32_t n_t,
+                                                       int64_t slot0, const I* imb, uint32_t N, uint32_t ny,
+                                                       uint32_t nz, double (&acc)[6]) {
+    if (n_t == 0) return;
+    const double* q = particles + (size_t)dsc.p * PF;
+    const uint32_t bx = (uint32_t)dsc.x0, by = (uint32_t)dsc.y0, bz = (uint32_t)dsc.z0;
+    const double qx = q[0], qy = q[1], qz = q[2];
+    const int64_t stride = blockDim.x;
+    for (uint32_t k0 = 0; k0 < n_t; k0 += U) {
+        double ow[U];
+        uint32_t abk[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool in = k0 + u < n_t;
+            const int64_t sl = slot0 + (int64_t)(k0 + u) * stride;
+            ow[u] = in ? __ldg(lw + sl) : 0.0;
+            abk[u] = in ? __ldg(labk + sl) : 0u;
+        }
+        I m[U][3];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            m[u][0] = m[u][1] = m[u][2] = I(0);
+            if (k0 + u < n_t) {
+                const uint32_t a = abk[u] & 0x7ffu, b = (abk[u] >> 11) & 0x7ffu, k = abk[u] >> 22;
+                const uint32_t cell = ((bx + a) * ny + (by + b)) * nz + (bz + k);
+                m[u][0] = __ldg(imb + cell);
+                m[u][1] = __ldg(imb + (size_t)N + cell);
+                m[u][2] = __ldg(imb + 2 * (size_t)N + cell);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (k0 + u < n_t) {
+                const uint32_t a = abk[u] & 0x7ffu, b = (abk[u] >> 11) & 0x7ffu, k = abk[u] >> 22;
+                const double nfx = -xmul(ow[u], (double)m[u][0]);
+                const double nfy = -xmul(ow[u], (double)m[u][1]);
+                const double nfz = -xmul(ow[u], (double)m[u][2]);
+                // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
+                const double rx = xsub(xadd((double)(bx + a), 0.5), qx);
+                const double ry = xsub(xadd((double)(by + b), 0.5), qy);
+                const double rz = xsub(xadd((double)(bz + k), 0.5), qz);
+                acc[0] += nfx;
+                acc[1] += nfy;
+                acc[2] += nfz;
+                acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
+                acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
+                acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
+            }
+        }
+    }
+}
+
+template <typename I>
+__global__ void __launch_bounds__(LOAD_THREADS, 2) k_loads_chunks_list(psc_geometry g, const I* imb, double* part) {
+    __shared__ double s[LOAD_THREADS / 32][6];
+    const int64_t C = g.totals[1];
+    const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
+        const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
+        const uint32_t n_t = g.load_n[chunk * LOAD_THREADS + threadIdx.x];
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        chunk_thread_sums_list<I, list_unroll<I, false>()>(dsc, g.particles, g.load_w, g.load_abk, n_t,
+                                               chunk * g.chunk_entries + threadIdx.x, imb, N, (uint32_t)g.ny,
+                                               (uint32_t)g.nz, acc);
         block_sum<6>(acc, s);
         if (threadIdx.x == 0) {
 #pragma unroll
@@ -664,9 +776,38 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS)
             cur_S = S;
         }
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        chunk_thread_sums<I>(dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum,
-                             reinterpret_cast<const I*>(jobs[dsc.pad].imb), (uint32_t)g.nx * g.ny * g.nz,
-                             (uint32_t)g.ny, (uint32_t)g.nz, s_al, ring, acc);
+        const int64_t local = chunk - chunk_base[dsc.pad];  // the chunk's index in its job
+        const bool list = g.load_w && g.load_abk && g.load_n;  // write the job's loads list too
+        const uint32_t listed = chunk_thread_sums<I>(
+            dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum, reinterpret_cast<const I*>(jobs[dsc.pad].imb),
+            (uint32_t)g.nx * g.ny * g.nz, (uint32_t)g.ny, (uint32_t)g.nz, s_al, ring, acc,
+            list ? g.load_w : nullptr, g.load_abk, local * g.chunk_entries + threadIdx.x);
+        if (list) g.load_n[local * LOAD_THREADS + threadIdx.x] = (uint8_t)listed;
+        block_sum<6>(acc, s);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
+        }
+    }
+}
+
+// The list path for many windows: every job's loads list is current.
+template <typename I>
+__global__ void __launch_bounds__(LOAD_THREADS, 2) k_loads_chunks_list_multi(const LoadsJob* jobs,
+                                                                        const int64_t* chunk_base, int njobs,
+                                                                        double* part) {
+    __shared__ double s[LOAD_THREADS / 32][6];
+    const int64_t C = chunk_base[njobs];
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
+        const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
+        const LoadsJob& J = jobs[dsc.pad];
+        const int64_t local = chunk - chunk_base[dsc.pad];
+        const uint32_t n_t = J.g.load_n[local * LOAD_THREADS + threadIdx.x];
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        chunk_thread_sums_list<I, list_unroll<I, true>()>(dsc, J.g.particles, J.g.load_w, J.g.load_abk, n_t,
+                                               local * J.g.chunk_entries + threadIdx.x,
+                                               reinterpret_cast<const I*>(J.imb), (uint32_t)J.g.nx * J.g.ny * J.g.nz,
+                                               (uint32_t)J.g.ny, (uint32_t)J.g.nz, acc);
         block_sum<6>(acc, s);
         if (threadIdx.x == 0) {
 #pragma unroll
@@ -838,12 +979,20 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
         cudaError_t e0 = loads_smem_optin();
         if (e0 != cudaSuccess) return e0;
         k_chunk_desc<<<(unsigned)(cg < cap ? cg : cap), 256, 0, stream>>>(g, chunk_partials);
-        if (imb_type == 0)
+        if (g.load_w && g.load_abk && g.load_n && g.list_ready) {  // this geometry's loads list is written
+            if (imb_type == 0)
+                k_loads_chunks_list<double><<<grid, LOAD_THREADS, 0, stream>>>(
+                    g, reinterpret_cast<const double*>(imb), chunk_partials);
+            else
+                k_loads_chunks_list<float><<<grid, LOAD_THREADS, 0, stream>>>(
+                    g, reinterpret_cast<const float*>(imb), chunk_partials);
+        } else if (imb_type == 0) {  // (writes the loads list when its arrays are given)
             k_loads_chunks<double><<<grid, LOAD_THREADS, lut, stream>>>(g, reinterpret_cast<const double*>(imb),
                                                                         chunk_partials);
-        else
+        } else {
             k_loads_chunks<float><<<grid, LOAD_THREADS, lut, stream>>>(g, reinterpret_cast<const float*>(imb),
                                                                        chunk_partials);
+        }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -858,8 +1007,8 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
 
 cudaError_t launch_particle_loads_multi(const LoadsJob* d_jobs, const int64_t* d_chunk_base,
                                         const int64_t* d_particle_base, int njobs, int64_t total_chunks,
-                                        int64_t total_particles, int imb_type, int max_subsamples, double* part,
-                                        cudaStream_t stream) {
+                                        int64_t total_particles, int imb_type, int max_subsamples,
+                                        bool list_ready, double* part, cudaStream_t stream) {
     if (njobs <= 0) return cudaSuccess;
     const int64_t cap = (int64_t)sm_count() * 16;
     if (total_chunks > 0) {
@@ -869,7 +1018,11 @@ cudaError_t launch_particle_loads_multi(const LoadsJob* d_jobs, const int64_t* d
         k_chunk_desc_multi<<<(unsigned)(cg < cap ? cg : cap), 256, 0, stream>>>(d_jobs, d_chunk_base, njobs, part);
         const unsigned grid = (unsigned)(total_chunks < cap ? total_chunks : cap);
         const size_t lut = (size_t)(max_subsamples * max_subsamples * max_subsamples + 1) * sizeof(double);
-        if (imb_type == 0)
+        if (list_ready && imb_type == 0)
+            k_loads_chunks_list_multi<double><<<grid, LOAD_THREADS, 0, stream>>>(d_jobs, d_chunk_base, njobs, part);
+        else if (list_ready)
+            k_loads_chunks_list_multi<float><<<grid, LOAD_THREADS, 0, stream>>>(d_jobs, d_chunk_base, njobs, part);
+        else if (imb_type == 0)
             k_loads_chunks_multi<double><<<grid, LOAD_THREADS, lut, stream>>>(d_jobs, d_chunk_base, njobs, part);
         else
             k_loads_chunks_multi<float><<<grid, LOAD_THREADS, lut, stream>>>(d_jobs, d_chunk_base, njobs, part);

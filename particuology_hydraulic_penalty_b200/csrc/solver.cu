@@ -12,12 +12,17 @@
 // One call runs any number of steps with no host work between them except
 // where the caller asks for per-step diagnostics (the lbm_converge loop).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstddef>
 #include <cstring>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.cuh"
@@ -38,9 +43,13 @@ namespace {
 
 constexpr int kQ = 19;
 constexpr int kChunkEntries = 4096;  // bbox entries per load-reduction chunk
+static_assert(kChunkEntries % PSC_LOAD_THREADS == 0 && kChunkEntries / PSC_LOAD_THREADS <= 64,
+              "the loads list holds at most 64 entries per thread and chunk");
 constexpr int kOutLen = 2 * PSC_NRED + PSC_NDIAG;  // [red_pre][red_post][diag]
 
-// Owned device array (contents are not kept when it grows).
+// Owned device array (contents are not kept when it grows).  A grow allocates
+// the new block before it frees the old one, so a failed grow leaves the array
+// (and every pointer to it) as it was.
 template <class T>
 struct DArray {
     T* p = nullptr;
@@ -57,12 +66,11 @@ struct DArray {
     cudaError_t ensure(int64_t m, bool zero, cudaStream_t s) {
         if (m < 1) m = 1;
         if (p && m <= n) return cudaSuccess;
+        T* q = nullptr;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&q), (size_t)m * sizeof(T));
+        if (e != cudaSuccess) return e;
         release();
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), (size_t)m * sizeof(T));
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return e;
-        }
+        p = q;
         n = m;
         return zero ? cudaMemsetAsync(p, 0, (size_t)m * sizeof(T), s) : cudaSuccess;
     }
@@ -93,6 +101,93 @@ struct HArray {
         n = m;
         return cudaSuccess;
     }
+};
+
+// A few host threads kept by a handle for its per-window host work (staging
+// particle arrays into page-locked memory): run(n, f) calls f(0) .. f(n - 1),
+// spread over the workers and the calling thread, and returns when every call
+// has finished and no worker is still looking for work, so one run's tasks
+// never mix with the next run's.  f must not throw.  Handles are
+// single-threaded, so run() is never reentered.
+class HostPool {
+  public:
+    HostPool() = default;
+    HostPool(const HostPool&) = delete;
+    HostPool& operator=(const HostPool&) = delete;
+    ~HostPool() {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            stop_ = true;
+        }
+        wake_.notify_all();
+        for (auto& t : threads_) t.join();
+    }
+    // Starts up to `workers` threads (fewer on a machine with fewer cores); false if none started.
+    bool start(int workers) {
+        const int hw = (int)std::thread::hardware_concurrency();
+        workers = std::min(workers, std::max(0, hw - 1));
+        for (int i = 0; i < workers; ++i) {
+            try {
+                threads_.emplace_back([this] { loop(); });
+            } catch (...) {
+                break;
+            }
+        }
+        return !threads_.empty();
+    }
+    bool ready() const { return !threads_.empty(); }
+    void run(int n, const std::function<void(int)>& f) {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            job_.store(&f);
+            count_.store(n);
+            done_ = 0;
+            next_.store(0);
+            ++generation_;
+        }
+        wake_.notify_all();
+        work();
+        std::unique_lock<std::mutex> lock(m_);
+        finished_.wait(lock, [this] { return done_ == count_.load() && active_ == 0; });
+        job_.store(nullptr);
+        count_.store(0);
+    }
+
+  private:
+    void work() {
+        int finished_here = 0;
+        for (int i = next_.fetch_add(1); i < count_.load(); i = next_.fetch_add(1)) {
+            (*job_.load())(i);
+            ++finished_here;
+        }
+        std::lock_guard<std::mutex> lock(m_);
+        done_ += finished_here;
+        finished_.notify_all();
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lock(m_);
+                wake_.wait(lock, [&] { return stop_ || generation_ != seen; });
+                if (stop_) return;
+                seen = generation_;
+                ++active_;
+            }
+            work();
+            std::lock_guard<std::mutex> lock(m_);
+            --active_;
+            finished_.notify_all();
+        }
+    }
+    std::vector<std::thread> threads_;
+    std::mutex m_;
+    std::condition_variable wake_, finished_;
+    std::atomic<const std::function<void(int)>*> job_{nullptr};
+    std::atomic<int> count_{0}, next_{0};
+    int done_ = 0, active_ = 0;
+    uint64_t generation_ = 0;
+    bool stop_ = false;
 };
 
 // Makes the handle's device current for the duration of a call.
@@ -187,6 +282,7 @@ int check_config(const psc_config& c, const char* who) {
     if (!(std::isfinite(c.store_scale) && c.store_scale >= 0.0))
         return fail(PSC_E_INVALID, w + ": store_scale must be >= 0 (0 = default)");
     if (!(std::isfinite(c.conv_tol) && c.conv_tol >= 0.0)) return fail(PSC_E_INVALID, w + ": conv_tol must be >= 0");
+    if (c.conv_check_every < 0) return fail(PSC_E_INVALID, w + ": conv_check_every must be >= 0");
     if (c.device < 0) return fail(PSC_E_INVALID, w + ": negative device ordinal");
     if (c.open_x != 0 && c.open_x != 1) return fail(PSC_E_INVALID, w + ": open_x must be 0 or 1");
     if (c.open_x && !(std::isfinite(c.inlet_rho) && c.inlet_rho > 0.0 && finite3(c.inlet_u)))
@@ -232,6 +328,13 @@ struct Window {
     double smooth_eps = 0.0;  // > 0: smooth solid fraction (the adjoint's differentiable surrogate)
     DArray<double> ent_alpha;
     DArray<int32_t> cl_ent;
+    // loads list (owner weights and cells of the non-zero bbox entries), written
+    // by the first loads call on a geometry and read by the later ones
+    // (list_version == built_version); kept only where the list's packing fits
+    DArray<double> load_w;
+    DArray<uint32_t> load_abk;
+    DArray<uint8_t> load_n;
+    uint64_t list_version = 0;
     int64_t cap_entries = 0, cap_chunks = 0, n_entries = 0, n_chunks = 0;
     DArray<double> forces, torques;
     uint64_t pversion = 1, built_version = 0, us_version = 0;
@@ -280,7 +383,19 @@ struct Window {
         g.smooth_eps = smooth_eps;
         g.ent_alpha = smooth_eps > 0.0 && cap_entries ? ent_alpha.p : nullptr;
         g.cl_ent = smooth_eps > 0.0 && cap_entries ? cl_ent.p : nullptr;
+        const bool list = list_allowed() && cap_chunks && load_n.p;
+        g.load_w = list ? load_w.p : nullptr;
+        g.load_abk = list ? load_abk.p : nullptr;
+        g.load_n = list ? load_n.p : nullptr;
+        g.list_ready = list && built && list_version == built_version ? 1 : 0;
         return g;
+    }
+    // The loads list packs bbox-local cells into 11 + 11 + 10 bits.
+    bool list_allowed() const { return !(smooth_eps > 0.0) && cfg.nx <= 2048 && cfg.ny <= 2048 && cfg.nz <= 1024; }
+    // A loads launch with geometry() has been enqueued: the list it writes is
+    // what the next launches on this geometry read (stream order).
+    void loads_enqueued() {
+        if (load_n.p && built) list_version = built_version;
     }
 
     // Descriptor reading buffer `src` (tile fields unset).
@@ -383,8 +498,35 @@ bool particles_finite(const double* hp, size_t n) {
     return probe == 0.0;
 }
 
+// Every fallible step a particle count of P needs (the per-particle device and
+// pinned buffers), taken before any window takes a new state.  A buffer that had
+// to move loses its contents, so the window's geometry and loads are made again
+// from its accepted state at the next step.
+int window_reserve_particles(Window& w, int P, cudaStream_t s, const char* who) {
+    if (P == w.P && w.particles.p) return PSC_OK;
+    PSC_CUDA(cudaEventSynchronize(w.upload_done), who);  // the old staging buffer may still be read
+    const void* before[7] = {w.particles.p, w.bbox.p, w.ent_off.p, w.chunk_off.p, w.forces.p, w.torques.p, w.pinned.p};
+    cudaError_t e = w.particles.ensure((int64_t)P * 10, true, s);
+    if (e == cudaSuccess) e = w.bbox.ensure((int64_t)std::max(P, 1) * 6, true, s);
+    if (e == cudaSuccess) e = w.ent_off.ensure((int64_t)P + 1, true, s);
+    if (e == cudaSuccess) e = w.chunk_off.ensure((int64_t)P + 1, true, s);
+    if (e == cudaSuccess) e = w.forces.ensure((int64_t)P * 3, true, s);
+    if (e == cudaSuccess) e = w.torques.ensure((int64_t)P * 3, true, s);
+    if (e == cudaSuccess) e = w.pinned.ensure((int64_t)P * 10);
+    const void* after[7] = {w.particles.p, w.bbox.p, w.ent_off.p, w.chunk_off.p, w.forces.p, w.torques.p, w.pinned.p};
+    if (std::memcmp(before, after, sizeof(before)) != 0) {
+        w.built = false;
+        w.loads_ready = false;
+        w.diag_ready = false;
+        w.touch();
+    }
+    if (e != cudaSuccess) return cuda_fail(e, who);
+    return PSC_OK;
+}
+
 // known: 0 nothing known; 1 hp equals the last accepted state bit for bit
-// (same count); 2 hp differs from it and is known to be finite.
+// (same count); 2 hp differs from it and is known to be finite.  With the
+// buffers reserved (window_reserve_particles) and known != 0 nothing here fails.
 int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, const char* who, int known = 0) {
     if (P < 0) return fail(PSC_E_INVALID, std::string(who) + ": negative particle count");
     if (P > 0 && !hp) return fail(PSC_E_INVALID, std::string(who) + ": null particle array");
@@ -403,20 +545,11 @@ int window_accept_particles(Window& w, const double* hp, int P, cudaStream_t s, 
             for (int k = 4; k < 10; ++k) mv = mv || hp[(size_t)p * 10 + k] != 0.0;
     }
     const bool changed = differs;
-    if (P != w.P || !w.particles.p) {
-        PSC_CUDA(cudaEventSynchronize(w.upload_done), who);  // the old staging buffer may still be read
-        PSC_CUDA(w.particles.ensure((int64_t)P * 10, true, s), who);
-        PSC_CUDA(w.bbox.ensure((int64_t)std::max(P, 1) * 6, true, s), who);
-        PSC_CUDA(w.ent_off.ensure((int64_t)P + 1, true, s), who);
-        PSC_CUDA(w.chunk_off.ensure((int64_t)P + 1, true, s), who);
-        PSC_CUDA(w.forces.ensure((int64_t)P * 3, true, s), who);
-        PSC_CUDA(w.torques.ensure((int64_t)P * 3, true, s), who);
-        PSC_CUDA(w.pinned.ensure((int64_t)P * 10), who);
-        if (P != w.P) {
-            w.built = false;
-            w.loads_ready = false;
-            w.diag_ready = false;
-        }
+    PSC_TRY(window_reserve_particles(w, P, s, who));
+    if (P != w.P) {
+        w.built = false;
+        w.loads_ready = false;
+        w.diag_ready = false;
         w.P = P;
     }
     if (changed) {
@@ -469,12 +602,19 @@ int window_rebuild(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* 
     if (w.n_chunks > w.cap_chunks) {
         const int64_t cap = w.n_chunks + w.n_chunks / 4 + 16;
         PSC_CUDA(w.chunk_partials.ensure(cap * 6, false, s), who);
+        if (w.list_allowed()) {
+            PSC_CUDA(w.load_w.ensure(cap * kChunkEntries, false, s), who);
+            PSC_CUDA(w.load_abk.ensure(cap * kChunkEntries, false, s), who);
+            PSC_CUDA(w.load_n.ensure(cap * PSC_LOAD_THREADS, false, s), who);
+        }
         w.cap_chunks = cap;
     }
+    w.built = false;  // until the build below is enqueued (the stored owner weights belong to the old one)
     g = w.geometry();
     PSC_TRY(psc_geometry_build(&g, s));
     w.built = true;
     w.built_version = w.pversion;
+    w.list_version = 0;
     w.us_version = 0;
     w.loads_ready = false;
     w.diag_ready = false;
@@ -540,6 +680,7 @@ int window_loads(Window& w, cudaStream_t s) {
     psc_geometry g = w.geometry();
     PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
                                w.forces.p, w.torques.p, diag_dev(w), s));
+    w.loads_enqueued();
     w.loads_ready = true;
     return PSC_OK;
 }
@@ -754,10 +895,17 @@ struct psc_solver {
     cudaGraphExec_t report_graph[2] = {nullptr, nullptr};
     std::vector<unsigned char> report_key[2];   // key of report_graph[parity]
     std::vector<unsigned char> report_seen[2];  // key of the last eager run of that parity
+    // device-side convergence (psc_converge): criterion state [kConvState] + reductions snapshot,
+    // and two pinned status slots the host polls
+    DArray<double> conv;
+    HArray<double> conv_host;
+    cudaEvent_t conv_ev[2] = {nullptr, nullptr};
 
     ~psc_solver() {
         for (auto& g : report_graph)
             if (g) cudaGraphExecDestroy(g);
+        for (auto& e : conv_ev)
+            if (e) cudaEventDestroy(e);
     }
 };
 
@@ -788,6 +936,44 @@ int solver_report(psc_solver& h, bool loads, bool fields, bool post = true) {
     fill_diag(w, h.host_out.p, w.last);
     w.diag_ready = loads;
     return PSC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// lbm_converge on the device (couple_psc_liggghts.py:284-296)
+// ---------------------------------------------------------------------------
+// Criterion state, doubles: [0] mean_uz of the last check, [1] its step,
+// [2] converged flag, [3] stopping step, [4] residual of the last check;
+// [kConvState ..) the out row (red_pre, red_post) of the stopping step.
+constexpr int kConvState = 8;
+
+// One check after step `step` of the call: out holds red_pre (the reductions
+// of the state before the step, i.e. the previous step's post-stream state)
+// and red_post (the post-stream state of the step).  mean_uz of the previous
+// step is the value this kernel kept when it checked that step (every step
+// checked: the reference's sequence of values), else red_pre's.  Step 1 has
+// no previous value (residual inf, as the reference's first iteration).  On
+// convergence the out row is kept and the window is marked inactive in both
+// descriptor tables, so the launches already enqueued after it do nothing.
+__global__ void k_converge_check(const double* out, double* cs, psc_window* tab0, psc_window* tab1, int step,
+                                 int min_steps, double tol, double N) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || cs[2] != 0.0) return;
+    const double now = out[PSC_NRED + PSC_RED_UZ] / N;
+    double resid = __longlong_as_double(0x7ff0000000000000ll);  // +inf
+    if (step > 1) {
+        const double prev = cs[1] == (double)(step - 1) ? cs[0] : out[PSC_RED_UZ] / N;
+        const double a = fabs(now);
+        resid = fabs(now - prev) / (a < 1.0e-30 ? 1.0e-30 : a);
+    }
+    cs[0] = now;
+    cs[1] = (double)step;
+    cs[4] = resid;
+    if (step >= min_steps && resid < tol) {
+        cs[2] = 1.0;
+        cs[3] = (double)step;
+        for (int k = 0; k < 2 * PSC_NRED; ++k) cs[kConvState + k] = out[k];
+        tab0->flags |= PSC_WIN_INACTIVE;
+        tab1->flags |= PSC_WIN_INACTIVE;
+    }
 }
 
 // One collide_stream_psc step; `imb` writes the IMB field and reduces the
@@ -863,6 +1049,7 @@ int report_step_work(psc_solver& h, int par) {
     psc_geometry g = w.geometry();
     PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
                                w.forces.p, w.torques.p, diag_dev(w), h.lanes.lane(0)));
+    w.loads_enqueued();
     PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par ^ 1].p, 1, w.solo_tiles, PSC_STEP_REDUCE | mv, &c, s));
     PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_post(w), s));
     PSC_CUDA(h.lanes.end(s), "psc_step");
@@ -922,6 +1109,90 @@ int solver_report_step(psc_solver& h) {
     PSC_CUDA(cudaStreamSynchronize(s), "psc_step");
     fill_diag(w, h.host_out.p, w.last);
     w.diag_ready = true;
+    return PSC_OK;
+}
+
+// lbm_converge as one call (psc_converge, PSC_RUN_CONVERGE): steps are
+// enqueued in blocks with the criterion evaluated on the device at every
+// check step (a multiple of check_every, and the last step); the host reads
+// the criterion state once per block, one block behind, and stops enqueuing
+// once it reports convergence.  Steps enqueued after the stopping step find
+// the window inactive and do nothing, so the populations stay those of the
+// stopping step: buffer parity start ^ (steps & 1).
+int solver_converge(psc_solver& h, int nsteps, double tol, int min_steps, int check_every, bool fields,
+                    psc_status& st) {
+    Window& w = h.w;
+    cudaStream_t s = h.stream;
+    const char* who = "psc_converge";
+    PSC_TRY(window_ensure_imb(w, s));
+    PSC_TRY(window_upload_solo(w, s));
+    // from here on the device may mark the window inactive in its descriptor tables: whatever
+    // path leaves this function, the next launch uploads them afresh
+    w.solo_dirty = true;
+    PSC_CUDA(h.conv.ensure(kConvState + 2 * PSC_NRED, false, s), who);
+    PSC_CUDA(h.conv_host.ensure(2 * kConvState), who);
+    for (auto& e : h.conv_ev)
+        if (!e) PSC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), who);
+    PSC_CUDA(cudaMemsetAsync(h.conv.p, 0, kConvState * sizeof(double), s), who);
+    const unsigned mv = w.moving ? PSC_STEP_MOVING : 0u;
+    const psc_launch c = {0, 1, w.solo_kernel, 0, 0};
+    const int start = w.cur;
+    // steps per poll: ~3e7 lattice updates (about a millisecond of the step kernel), 4 .. 256 steps
+    const int64_t per = std::max<int64_t>(4, std::min<int64_t>(256, 30000000 / std::max<int64_t>(w.N, 1)));
+    const int block = (int)std::max<int64_t>(check_every, per);
+    int t = 0, polls = 0, pending = -1;
+    bool stop = false;
+    while (t < nsteps && !stop) {
+        const int end = (int)std::min<int64_t>(nsteps, (int64_t)t + block);
+        for (int u = t + 1; u <= end; ++u) {
+            const int par = start ^ ((u - 1) & 1);
+            if (u % check_every != 0 && u != nsteps) {
+                PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par].p, 1, w.solo_tiles, PSC_STEP_COLLIDE | mv, &c, s));
+                continue;
+            }
+            PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par].p, 1, w.solo_tiles,
+                                        PSC_STEP_COLLIDE | PSC_STEP_IMB | PSC_STEP_REDUCE | mv, &c, s));
+            PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_pre(w), s));
+            PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par ^ 1].p, 1, w.solo_tiles, PSC_STEP_REDUCE | mv, &c, s));
+            PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_post(w), s));
+            k_converge_check<<<1, 32, 0, s>>>(w.out.p, h.conv.p, w.solo[0].p, w.solo[1].p, u, min_steps, tol,
+                                              (double)w.N);
+            PSC_CUDA(cudaGetLastError(), who);
+        }
+        t = end;
+        const int slot = polls & 1;
+        PSC_CUDA(cudaMemcpyAsync(h.conv_host.p + slot * kConvState, h.conv.p, kConvState * sizeof(double),
+                                 cudaMemcpyDeviceToHost, s),
+                 who);
+        PSC_CUDA(cudaEventRecord(h.conv_ev[slot], s), who);
+        if (pending >= 0) {
+            PSC_CUDA(cudaEventSynchronize(h.conv_ev[pending]), who);
+            stop = h.conv_host.p[pending * kConvState + 2] != 0.0;
+        }
+        pending = slot;
+        ++polls;
+    }
+    PSC_CUDA(cudaStreamSynchronize(s), who);
+    const double* cs = h.conv_host.p + pending * kConvState;  // covers every enqueued step
+    const bool converged = cs[2] != 0.0;
+    const int done = converged ? (int)cs[3] : nsteps;
+    st.converged = converged ? 1 : 0;
+    st.steps_done = done;
+    st.residual = cs[4];
+    w.cur = start ^ (done & 1);
+    w.stepped = true;
+    w.moments_ready = false;
+    w.loads_ready = false;
+    w.diag_ready = false;
+    if (converged)  // the reductions of the stopping step (later enqueued reductions read no new partials)
+        PSC_CUDA(cudaMemcpyAsync(w.out.p, h.conv.p + kConvState, 2 * PSC_NRED * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, s),
+                 who);
+    PSC_TRY(window_upload_solo(w, s));  // the descriptor tables without the inactive flag
+    // loads and diagnostics of the stopping step (its IMB field; the post-stream reductions are
+    // taken already unless the fields are wanted)
+    PSC_TRY(solver_report(h, true, fields, fields));
+    st.diag = w.last;
     return PSC_OK;
 }
 
@@ -1010,30 +1281,36 @@ int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status) {
         if (h_status) *h_status = st;
         return PSC_OK;
     }
-    double previous = NAN;
-    int k = 0;
-    for (k = 1; k <= nsteps; ++k) {
-        const bool last = k == nsteps;
-        PSC_TRY(solver_collide(*h, last || converge));
-        if (converge) {
-            PSC_TRY(solver_report(*h, false, false));
-            const double current = w.last.mean_uz;
-            if (!std::isnan(previous)) st.residual = std::fabs(current - previous) / std::max(std::fabs(current), 1.0e-30);
-            previous = current;
-            if (k >= min_steps && st.residual < tol) {
-                st.converged = 1;
-                break;
-            }
-        }
+    if (converge && nsteps > 0) {
+        PSC_TRY(solver_converge(*h, nsteps, tol, min_steps, std::max(1, w.cfg.conv_check_every), fields, st));
+        if (h_status) *h_status = st;
+        return PSC_OK;
     }
-    st.steps_done = std::min(k, nsteps);
+    for (int k = 1; k <= nsteps; ++k) PSC_TRY(solver_collide(*h, k == nsteps));
+    st.steps_done = nsteps;
     if (nsteps > 0 && (diag || fields)) {
-        // under PSC_RUN_CONVERGE the post-stream reductions of the last step are taken already
-        PSC_TRY(solver_report(*h, diag, fields, !converge));
+        PSC_TRY(solver_report(*h, diag, fields));
         if (diag) st.diag = w.last;
     } else if (nsteps > 0) {
         PSC_CUDA(cudaGetLastError(), "psc_step");
     }
+    if (h_status) *h_status = st;
+    return PSC_OK;
+}
+
+int psc_converge(psc_solver* h, int max_steps, double tol, int min_steps, int check_every, unsigned flags,
+                 psc_status* h_status) {
+    if (!h) return fail(PSC_E_INVALID, "psc_converge: null handle");
+    if (max_steps < 1 || check_every < 1 || !(tol >= 0.0) || !std::isfinite(tol))
+        return fail(PSC_E_INVALID, "psc_converge: need max_steps >= 1, check_every >= 1 and a finite tol >= 0");
+    if (flags & ~PSC_RUN_FIELDS) return fail(PSC_E_INVALID, "psc_converge: unknown flags");
+    DeviceScope ds(h->device);
+    if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_converge: cudaSetDevice");
+    psc_status st{};
+    st.residual = INFINITY;
+    PSC_TRY(window_prepare(h->w, h->stream, h->tot, "psc_converge"));
+    PSC_TRY(solver_converge(*h, max_steps, tol, std::max(1, min_steps), check_every, (flags & PSC_RUN_FIELDS) != 0,
+                            st));
     if (h_status) *h_status = st;
     return PSC_OK;
 }
@@ -1150,6 +1427,8 @@ struct psc_batch {
     HArray<double> up_host;    // every window's particles, staged for one upload
     DArray<double> up_dev;
     cudaEvent_t up_done = nullptr;
+    HostPool pool;             // stages large particle uploads window by window in parallel
+    bool pool_tried = false;
     // particle loads of all active windows in one launch sequence: job table
     // [LoadsJob x n][chunk bases n+1][particle bases n+1], as last uploaded
     std::vector<unsigned char> jobs_last;
@@ -1158,6 +1437,7 @@ struct psc_batch {
     DArray<double> loads_part;  // chunk partials of all jobs
     int jobs_n = 0, jobs_max_s = 1;
     int64_t jobs_chunks = 0, jobs_particles = 0;
+    bool jobs_list_ready = false;  // every job's loads list is written (the list path of the loads)
 
     ~psc_batch() {
         for (auto& g : graph)
@@ -1177,12 +1457,14 @@ int batch_loads_table(psc_batch& b, const char* who) {
     std::vector<LoadsJob> jobs;
     std::vector<int64_t> cb(1, 0), pb(1, 0);
     int max_s = 1;
+    bool ready = true;
     for (int k = 0; k < nwin; ++k) {
         if (b.frozen[(size_t)k] >= 0) continue;
         const Window& w = *b.w[(size_t)k];
         LoadsJob j;
         std::memset(&j, 0, sizeof(j));  // padding too: the table is compared bytewise
         j.g = w.geometry();
+        ready = ready && (w.P == 0 || j.g.list_ready);
         j.imb = w.imb.p;
         j.imb_sums = b.red_pre.p + (size_t)k * PSC_NRED + PSC_RED_IMBX;
         j.forces = w.forces.p;
@@ -1203,6 +1485,7 @@ int batch_loads_table(psc_batch& b, const char* who) {
     b.jobs_max_s = max_s;
     b.jobs_chunks = cb.back();
     b.jobs_particles = pb.back();
+    b.jobs_list_ready = ready;
     if (bytes == b.jobs_last) return PSC_OK;
     // kernels of earlier steps may still read the old table or partials, the copy the pinned buffer
     PSC_CUDA(cudaStreamSynchronize(b.stream), who);
@@ -1488,36 +1771,47 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
     // pass 1: stage every window (an unchanged state is found in the same pass) and validate the
     // changed ones; one rejected window leaves every window as it was
     std::vector<int> known(nwin, 0);
-    int64_t off = 0;
+    std::vector<int64_t> offs(nwin + 1, 0);
     for (size_t k = 0; k < nwin; ++k) {
-        const Window& w = *b->w[k];
-        const int P = h_nparticles[k];
-        if (P > 0 && !h_particles[k])
+        if (h_nparticles[k] > 0 && !h_particles[k])
             return fail(PSC_E_INVALID, std::string(who) + ": null particle array (window " + std::to_string(k) + ")");
+        offs[k + 1] = offs[k] + (int64_t)h_nparticles[k] * 10;
+    }
+    // window k: copy into the staging buffer, note whether it equals the accepted state, check a
+    // changed one for NaN / Inf (known[k] = 1 same, 2 changed and finite, -1 non-finite)
+    auto stage = [&](int k) {
+        const Window& w = *b->w[(size_t)k];
+        const int P = h_nparticles[k];
         const size_t n10 = (size_t)P * 10;
+        double* dst = b->up_host.p + offs[(size_t)k];
         bool same = P == 0 && w.P == 0 && w.hp.empty();  // (empty before and now)
-        if (P > 0 && P == w.P && w.hp.size() == n10)
-            same = copy_same(b->up_host.p + off, h_particles[k], w.hp.data(), n10);
-        else if (P > 0)
-            std::memcpy(b->up_host.p + off, h_particles[k], n10 * sizeof(double));
-        if (!same && !particles_finite(h_particles[k], n10))
+        if (P > 0 && P == w.P && w.hp.size() == n10) same = copy_same(dst, h_particles[k], w.hp.data(), n10);
+        else if (P > 0) std::memcpy(dst, h_particles[k], n10 * sizeof(double));
+        known[(size_t)k] = same ? 1 : (particles_finite(h_particles[k], n10) ? 2 : -1);
+    };
+    // more than 256 KiB of particle state: the windows are staged on the handle's host threads
+    if (total * 8 > (1 << 18) && nwin > 1 && !b->pool_tried) {
+        b->pool_tried = true;
+        b->pool.start(3);
+    }
+    if (total * 8 > (1 << 18) && nwin > 1 && b->pool.ready()) b->pool.run((int)nwin, stage);
+    else
+        for (size_t k = 0; k < nwin; ++k) stage((int)k);
+    for (size_t k = 0; k < nwin; ++k)
+        if (known[k] < 0)
             return fail(PSC_E_INVALID,
                         std::string(who) + ": particle state contains NaN or Inf (window " + std::to_string(k) + ")");
-        known[k] = same ? 1 : 2;
-        off += (int64_t)P * 10;
-    }
+    // every fallible step of the windows that change their particle count, before any window
+    // takes its new state
+    for (size_t k = 0; k < nwin; ++k) PSC_TRY(window_reserve_particles(*b->w[k], h_nparticles[k], b->stream, who));
     // the device buffer grows only now: until every window is accepted the windows keep reading
-    // the current one
+    // the current one (a failed grow leaves it in place)
     if (b->up_dev.n < total) {
         PSC_CUDA(cudaStreamSynchronize(b->stream), who);  // kernels may still read the old buffer
-        const cudaError_t e = b->up_dev.ensure(cap, false, b->stream);
-        if (e != cudaSuccess) {  // the old buffer is gone: the windows read their own device copies
-            for (auto& wp : b->w) wp->ext_particles = nullptr;
-            return cuda_fail(e, who);
-        }
+        PSC_CUDA(b->up_dev.ensure(cap, false, b->stream), who);
     }
-    // pass 2: every window takes its staged state
-    off = 0;
+    // pass 2: every window takes its staged state (nothing here fails: validated and reserved above)
+    int64_t off = 0;
     for (size_t k = 0; k < nwin; ++k) {
         Window& w = *b->w[k];
         const int P = h_nparticles[k];
@@ -1557,10 +1851,14 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
         PSC_CUDA(b->lanes.begin(b->stream), "psc_batch_step");
         PSC_CUDA(launch_particle_loads_multi(reinterpret_cast<const LoadsJob*>(b->jobs_dev.p), batch_chunk_base(*b),
                                              batch_particle_base(*b), b->jobs_n, b->jobs_chunks, b->jobs_particles,
-                                             b->w[0]->field_type(), b->jobs_max_s, b->loads_part.p, b->lanes.lane(0)),
+                                             b->w[0]->field_type(), b->jobs_max_s, b->jobs_list_ready,
+                                             b->loads_part.p, b->lanes.lane(0)),
                  "psc_batch_step: particle loads");
         for (int k = 0; k < nwin; ++k)
-            if (b->frozen[(size_t)k] < 0) b->w[(size_t)k]->loads_ready = true;
+            if (b->frozen[(size_t)k] < 0) {
+                b->w[(size_t)k]->loads_enqueued();
+                b->w[(size_t)k]->loads_ready = true;
+            }
         PSC_TRY(batch_launch(*b, PSC_STEP_REDUCE | (fields ? PSC_STEP_MOMENTS : 0u)));
         PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_post.p, b->stream));
         PSC_CUDA(b->lanes.end(b->stream), "psc_batch_step");

@@ -20,8 +20,11 @@
 
 namespace psc {
 
+// The exact FP64 variant is bound by its FP64 dependency chains: two CTAs per SM
+// (at most 128 registers) hide their latency better than one.
 template <int STORE, bool MOVING>
-__global__ void __launch_bounds__(STEP_THREADS) k_step(const psc_window* __restrict__ wins, int nwin,
+__global__ void __launch_bounds__(STEP_THREADS, STORE == PSC_STORE_F64_EXACT ? 2 : 1)
+    k_step(const psc_window* __restrict__ wins, int nwin,
                                                         int64_t total_tiles, unsigned flags) {
     using TR = StoreTraits<STORE>;
     using T = typename TR::T;

@@ -36,7 +36,8 @@ def _diag_dict(d: nat.PscDiag) -> dict:
 
 def make_config(shape, *, tau: float, force, subsamples: int, store: int, static_geometry: bool = True,
                 device_index: int = 0, tau_minus: float = 0.0, store_scale: float | None = None,
-                conv_tol: float = 0.0, conv_min_steps: int = 1, inlet=None) -> nat.PscConfig:
+                conv_tol: float = 0.0, conv_min_steps: int = 1, conv_check_every: int = 1,
+                inlet=None) -> nat.PscConfig:
     c = nat.PscConfig()
     c.nx, c.ny, c.nz = (int(v) for v in shape)
     c.subsamples = int(subsamples)
@@ -52,6 +53,7 @@ def make_config(shape, *, tau: float, force, subsamples: int, store: int, static
     c.force[0], c.force[1], c.force[2] = f
     c.store_scale = 0.0 if store_scale is None else float(store_scale)
     c.conv_tol = float(conv_tol)
+    c.conv_check_every = int(conv_check_every)
     c.stream = None
     if inlet is not None:  # (rho_in, (ux, uy, uz)): open along x
         c.open_x = 1
@@ -103,6 +105,14 @@ class SolverHandle:
     def step(self, nsteps: int = 1, flags: int = nat.RUN_DIAG) -> nat.PscStatus:
         st = self._status
         self._check(self._step_fn(self._h, int(nsteps), int(flags), ctypes.byref(st)), "psc_step")
+        return st
+
+    def converge(self, max_steps: int, tol: float = 1.0e-8, min_steps: int = 1, check_every: int = 1,
+                 flags: int = 0) -> nat.PscStatus:
+        """``psc_converge``: lbm_converge (couple_psc_liggghts.py:284-296) with the criterion on the device."""
+        st = self._status
+        self._check(self._lib.psc_converge(self._h, int(max_steps), float(tol), int(min_steps), int(check_every),
+                                           int(flags), ctypes.byref(st)), "psc_converge")
         return st
 
     # results ------------------------------------------------------------------

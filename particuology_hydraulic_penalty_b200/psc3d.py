@@ -31,7 +31,7 @@ import torch
 
 from . import _native as nat
 from .engine import check_inlet, particles_array, require_cuda, store_mode, trt_tau_minus
-from .handle import SolverHandle, make_config
+from .handle import SolverHandle, _diag_dict, make_config
 
 # D3Q19 velocity set in the reference's index order (psc3d.py:17-43).
 C = np.array(
@@ -190,6 +190,64 @@ class PscD3Q19:
             "max_force": float(d.max_force),
             "max_torque": float(d.max_torque),
         }
+
+    def advance(self, steps: int) -> dict:
+        """``steps`` collide_stream_psc() steps in one native call, with the loads and diagnostics of
+        the last one (the populations are those of ``steps`` single calls; the steps before the last
+        take no reductions or loads).  Returns the last step's diagnostics dictionary."""
+        steps = int(steps)
+        if steps < 1:
+            raise ValueError("steps must be >= 1")
+        if steps == 1:
+            return self.collide_stream_psc()
+        self._upload_particles()
+        d = self._h.step(steps, nat.RUN_DIAG).diag
+        self._geometry_built = True
+        self._stepped = True
+        self._loads_host = None
+        self._cache.clear()
+        self._momentum_residual = float(d.momentum_residual)
+        if d.nonfinite_cells > 0:
+            self._nonfinite = True
+        return {"solid_volume_lu": float(d.solid_volume_lu), "mean_uz": float(d.mean_uz),
+                "momentum_residual": float(d.momentum_residual), "max_force": float(d.max_force),
+                "max_torque": float(d.max_torque)}
+
+    def step_diagnostics(self) -> dict:
+        """Every diagnostic of the last step: the reference's five keys plus the Darcy quantities
+        (mean and superficial velocity, fluid volume, IMB and force sums, permeability along the body
+        force, non-finite cell count).  No GPU work: the values were taken with the step."""
+        return _diag_dict(self._h.diag())
+
+    def run_to_convergence(self, residual_tol: float = 1.0e-8, min_steps: int = 1, max_steps: int = 20000,
+                           check_every: int = 1):
+        """lbm_converge (coupling_sync/couple_psc_liggghts.py:284-296) as one native call.
+
+        Steps until |mean_uz_k - mean_uz_{k-1}| / |mean_uz_k| < residual_tol at a step
+        k >= min_steps, at most max_steps steps; returns (iterations, residual, converged,
+        diagnostics of the last step) like the reference's loop.  The criterion is evaluated on the
+        device; the loads and diagnostics are taken for the stopping step only.  check_every = 1
+        evaluates it every step (the reference's iterations and residual); check_every = k evaluates
+        it on steps k - 1 and k of every k, with no reductions on the steps in between.
+        """
+        self._upload_particles()
+        st = self._h.converge(int(max_steps), float(residual_tol), int(min_steps), int(check_every))
+        d = st.diag
+        self._geometry_built = True
+        self._stepped = True
+        self._loads_host = None
+        self._cache.clear()
+        self._momentum_residual = float(d.momentum_residual)
+        if d.nonfinite_cells > 0:
+            self._nonfinite = True
+        diag = {
+            "solid_volume_lu": float(d.solid_volume_lu),
+            "mean_uz": float(d.mean_uz),
+            "momentum_residual": float(d.momentum_residual),
+            "max_force": float(d.max_force),
+            "max_torque": float(d.max_torque),
+        }
+        return int(st.steps_done), float(st.residual), bool(st.converged), diag
 
     # loads are copied to the host when read ------------------------------
     def _fetch_loads(self) -> None:

@@ -47,3 +47,31 @@ def test_converge_semantics():
     assert not ok and it == 5
     steps, res, ok, diag = coupling.lbm_transient_advance(_FakeSolver(), 4)
     assert steps == 4 and ok and math.isclose(diag["mean_uz"], 1 - 0.5 ** 4)
+
+
+def test_validation_profiles_and_steady_rule():
+    """The validation campaign's profile grids are those the golden rows were made with, and the
+    steady-state rule (validation/run_precision_validation.py:148-158, :223-233) on known series."""
+    import json
+    from pathlib import Path
+
+    from particuology_hydraulic_penalty_b200 import validation as val
+
+    gold = json.loads((Path(__file__).resolve().parent / "golden" / "validation_quick.json").read_text())
+    prof = val.PROFILES["quick"]
+    runs = [prof.settling, *prof.hasimoto, *prof.permeability]
+    assert [(r["n"], r["radius_lu"], r["subsamples"]) for r in gold["rows"]] == \
+        [(g.n, g.radius, prof.subsamples) for g in runs]
+    assert [len(val.PROFILES[p].hasimoto) for p in ("quick", "standard", "high")] == [2, 3, 3]
+    flat = [1.0] * 8
+    assert val.steady_metrics(flat) == (0.0, 0.0)
+    run = val.GridRun(20, 2.5, 100, 800, 20)
+    assert not val.should_stop(99, run, flat, 1e-2)          # before min_steps
+    assert not val.should_stop(200, run, flat[:7], 1e-2)     # fewer than 8 samples
+    assert val.should_stop(200, run, flat, 1e-2)
+    assert not val.should_stop(200, run, flat, 1e-2, extra_check=lambda: False)
+    rising = [1.0 + 0.01 * k for k in range(8)]
+    std_rel, drift_rel = val.steady_metrics(rising)
+    assert drift_rel > 1e-2 and not val.should_stop(200, run, rising, 1e-2)
+    assert abs(val.hasimoto_factor(2.5, 20.0) - 1.0 / (1.0 - 2.837297 * 0.125 + 4.19 * 0.125 ** 3
+                                                        - 27.4 * 0.125 ** 6)) < 1e-15

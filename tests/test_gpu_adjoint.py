@@ -102,3 +102,19 @@ def test_native_adjoint_handle_matches_python_problem():
     # a second run on the same handle gives the same answer
     assert h.forward(w.particles) == K_c
     assert np.array_equal(h.backward(), g_c)
+
+
+def test_full_size_adjoint_case_gradient_and_cost():
+    """The adjoint sensitivity case at its stated size: a preloaded 96^3 window with 64 fines (radius
+    0.15x the skeleton's), 2000 forward steps checkpointed every 100, FP32 populations with FP64
+    reductions.  On 8 seeded fines the FP64 adjoint matches FP64 central differences of K (step
+    1e-3 lu) to 1e-3 relative in every (x, y, z, r) component, the FP32 adjoint the FP64 one to
+    1e-3, and forward + backward costs at most 4x the forward pass (CUDA events)."""
+    from particuology_hydraulic_penalty_b200 import validation
+
+    r = validation.adjoint_check(n=96, n_fines=64, steps=2000, every=100, n_check=8)
+    assert r["n_fines"] == 64
+    assert r["fd_vs_adjoint_fp64_max_rel"] <= 1e-3, r["fd_vs_adjoint_fp64_max_rel"]
+    assert r["adjoint_fp32_vs_fp64_norm_rel"] <= 1e-3, r["adjoint_fp32_vs_fp64_norm_rel"]
+    assert r["adjoint_plus_forward_over_forward"] <= 4.0, r["adjoint_plus_forward_over_forward"]
+    assert abs(r["K_fp32"] - r["K_fp64"]) <= 1e-4 * abs(r["K_fp64"])
