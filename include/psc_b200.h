@@ -484,6 +484,11 @@ int psc_rebuild_geometry(psc_solver* h);
 int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status);
 /* Field `which` (PSC_FIELD_*) as float64 into h_dst ([N], or [19][N] for PSC_FIELD_F). */
 int psc_get_fields(psc_solver* h, int which, double* h_dst);
+/* Message of the last failed call on this handle ("" if none).  A call that
+ * fails also sets the calling thread's psc_last_error(); psc_create reports
+ * there only (it returns no handle on failure).  Valid until the next failing
+ * call on the handle or psc_destroy. */
+const char* psc_solver_last_error(const psc_solver* h);
 /* lbm_converge (coupling_sync/couple_psc_liggghts.py:284-296) as one call: up to max_steps steps,
  * stopping at the first step k >= min_steps (k a multiple of check_every, or max_steps) with
  * |mean_uz_k - mean_uz_{k-1}| / max(|mean_uz_k|, 1e-30) < tol.  check_every = 1 evaluates every
@@ -527,6 +532,8 @@ typedef struct psc_adjoint psc_adjoint;
 int psc_adjoint_create(const psc_config* h_cfg, double smooth_eps, int steps, int checkpoint_every,
                        psc_adjoint** out);
 int psc_adjoint_destroy(psc_adjoint* a);
+/* Message of the last failed call on this adjoint handle ("" if none), as psc_solver_last_error. */
+const char* psc_adjoint_last_error(const psc_adjoint* a);
 /* K after the forward run with h_particles [P][10] (velocities ignored: static particles). */
 int psc_adjoint_forward(psc_adjoint* a, const double* h_particles, int nparticles, double* h_K);
 /* h_grad [P][4] = dK/d(x, y, z, r) of every particle for the last forward run. */
@@ -546,6 +553,8 @@ typedef struct psc_batch psc_batch;
 int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_launch, int graph_steps,
                      psc_batch** out);
 int psc_batch_destroy(psc_batch* b);
+/* Message of the last failed call on this batch ("" if none), as psc_solver_last_error. */
+const char* psc_batch_last_error(const psc_batch* b);
 /* Particles of window `win`; a changed array re-voxelises that window before the next step. */
 int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, int nparticles);
 /* psc_batch_set_particles for every window in one call: h_particles[k] is window k's [P_k][10]

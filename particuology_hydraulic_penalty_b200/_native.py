@@ -190,6 +190,9 @@ SIGNATURES = {
     "psc_rebuild_geometry": (c_int, [c_void_p]),
     "psc_step": (c_int, [c_void_p, c_int, c_uint, POINTER(PscStatus)]),
     "psc_converge": (c_int, [c_void_p, c_int, c_double, c_int, c_int, c_uint, POINTER(PscStatus)]),
+    "psc_solver_last_error": (ctypes.c_char_p, [c_void_p]),
+    "psc_batch_last_error": (ctypes.c_char_p, [c_void_p]),
+    "psc_adjoint_last_error": (ctypes.c_char_p, [c_void_p]),
     "psc_get_fields": (c_int, [c_void_p, c_int, c_void_p]),
     "psc_set_populations": (c_int, [c_void_p, c_void_p]),
     "psc_get_loads": (c_int, [c_void_p, c_void_p, c_void_p]),

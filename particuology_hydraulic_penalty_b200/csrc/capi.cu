@@ -11,8 +11,15 @@
 namespace psc {
 
 static thread_local std::string g_last_error;
+static thread_local uint64_t g_error_seq = 0;  // errors set on this thread so far
 
-void set_error(const std::string& msg) { g_last_error = msg; }
+void set_error(const std::string& msg) {
+    g_last_error = msg;
+    ++g_error_seq;
+}
+
+uint64_t error_seq() { return g_error_seq; }
+const std::string& last_error_string() { return g_last_error; }
 
 int fail(int code, const std::string& msg) {
     set_error(msg);

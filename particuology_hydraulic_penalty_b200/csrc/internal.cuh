@@ -11,8 +11,11 @@
 
 namespace psc {
 
-// Thread-local last-error slot behind psc_last_error().
+// Thread-local last-error slot behind psc_last_error(), and the number of
+// errors set on this thread (a handle copies the message when it changes).
 void set_error(const std::string& msg);
+uint64_t error_seq();
+const std::string& last_error_string();
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t err, const char* what);
 

@@ -207,6 +207,17 @@ struct DeviceScope {
     }
 };
 
+// Keeps a handle's last error: every error set on this thread while the
+// guard lives (one call on the handle) is copied into the handle's message.
+struct ErrorCapture {
+    std::string* dst;
+    uint64_t seq0;
+    explicit ErrorCapture(std::string& d) : dst(&d), seq0(error_seq()) {}
+    ~ErrorCapture() {
+        if (error_seq() != seq0) *dst = last_error_string();
+    }
+};
+
 // Auxiliary streams of a handle for work of one step that is independent of
 // the main stream's (particle loads beside the post-stream reduction pass):
 // begin() makes every lane wait for the main stream's work so far, end()
@@ -881,6 +892,7 @@ using namespace psc;
 // single-window solver
 // ---------------------------------------------------------------------------
 struct psc_solver {
+    std::string last_error;  // message of the last failed call on this handle
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -1249,18 +1261,21 @@ int psc_destroy(psc_solver* h) {
 
 int psc_set_particles(psc_solver* h, const double* h_particles, int nparticles) {
     if (!h) return fail(PSC_E_INVALID, "psc_set_particles: null handle");
+    ErrorCapture errors_(h->last_error);
     DeviceScope ds(h->device);
     return window_set_particles(h->w, h_particles, nparticles, h->stream, "psc_set_particles");
 }
 
 int psc_rebuild_geometry(psc_solver* h) {
     if (!h) return fail(PSC_E_INVALID, "psc_rebuild_geometry: null handle");
+    ErrorCapture errors_(h->last_error);
     DeviceScope ds(h->device);
     return window_rebuild(h->w, h->stream, h->tot, "psc_rebuild_geometry");
 }
 
 int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status) {
     if (!h) return fail(PSC_E_INVALID, "psc_step: null handle");
+    ErrorCapture errors_(h->last_error);
     if (nsteps < 0) return fail(PSC_E_INVALID, "psc_step: negative step count");
     if (flags & ~(PSC_RUN_DIAG | PSC_RUN_CONVERGE | PSC_RUN_FIELDS)) return fail(PSC_E_INVALID, "psc_step: unknown flags");
     DeviceScope ds(h->device);
@@ -1301,6 +1316,7 @@ int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status) {
 int psc_converge(psc_solver* h, int max_steps, double tol, int min_steps, int check_every, unsigned flags,
                  psc_status* h_status) {
     if (!h) return fail(PSC_E_INVALID, "psc_converge: null handle");
+    ErrorCapture errors_(h->last_error);
     if (max_steps < 1 || check_every < 1 || !(tol >= 0.0) || !std::isfinite(tol))
         return fail(PSC_E_INVALID, "psc_converge: need max_steps >= 1, check_every >= 1 and a finite tol >= 0");
     if (flags & ~PSC_RUN_FIELDS) return fail(PSC_E_INVALID, "psc_converge: unknown flags");
@@ -1317,18 +1333,21 @@ int psc_converge(psc_solver* h, int max_steps, double tol, int min_steps, int ch
 
 int psc_get_fields(psc_solver* h, int which, double* h_dst) {
     if (!h) return fail(PSC_E_INVALID, "psc_get_fields: null handle");
+    ErrorCapture errors_(h->last_error);
     DeviceScope ds(h->device);
     return window_get_field(h->w, which, h_dst, h->stream, h->tot, "psc_get_fields");
 }
 
 int psc_set_populations(psc_solver* h, const double* h_f) {
     if (!h) return fail(PSC_E_INVALID, "psc_set_populations: null handle");
+    ErrorCapture errors_(h->last_error);
     DeviceScope ds(h->device);
     return window_set_populations(h->w, h_f, h->stream, "psc_set_populations");
 }
 
 int psc_get_loads(psc_solver* h, double* h_forces, double* h_torques) {
     if (!h) return fail(PSC_E_INVALID, "psc_get_loads: null handle");
+    ErrorCapture errors_(h->last_error);
     Window& w = h->w;
     if (w.P > 0 && (!h_forces || !h_torques)) return fail(PSC_E_INVALID, "psc_get_loads: null output");
     if (w.P == 0) return PSC_OK;
@@ -1352,6 +1371,7 @@ int psc_get_loads(psc_solver* h, double* h_forces, double* h_torques) {
 
 int psc_accumulate_particle_loads(psc_solver* h) {
     if (!h) return fail(PSC_E_INVALID, "psc_accumulate_particle_loads: null handle");
+    ErrorCapture errors_(h->last_error);
     Window& w = h->w;
     if (!w.stepped || !w.imb.p) return fail(PSC_E_INVALID, "psc_accumulate_particle_loads: no step has run");
     DeviceScope ds(h->device);
@@ -1379,9 +1399,12 @@ int psc_get_diag(psc_solver* h, psc_diag* h_diag) {
 
 int psc_get_sparse_alpha(psc_solver* h, int64_t* h_offsets, int64_t* h_ids, double* h_vals, int64_t capacity) {
     if (!h) return fail(PSC_E_INVALID, "psc_get_sparse_alpha: null handle");
+    ErrorCapture errors_(h->last_error);
     DeviceScope ds(h->device);
     return window_sparse_alpha(h->w, h_offsets, h_ids, h_vals, capacity, h->stream, "psc_get_sparse_alpha");
 }
+
+const char* psc_solver_last_error(const psc_solver* h) { return h ? h->last_error.c_str() : ""; }
 
 size_t psc_config_size(void) { return sizeof(psc_config); }
 
@@ -1402,6 +1425,7 @@ int psc_solver_info(psc_solver* h, int* h_nparticles, int64_t* h_cells) {
 // batches
 // ---------------------------------------------------------------------------
 struct psc_batch {
+    std::string last_error;  // message of the last failed call on this handle
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -1750,12 +1774,14 @@ int psc_batch_destroy(psc_batch* b) {
 
 int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, int nparticles) {
     if (!b || win < 0 || win >= (int)b->w.size()) return fail(PSC_E_INVALID, "psc_batch_set_particles: bad window");
+    ErrorCapture errors_(b->last_error);
     DeviceScope ds(b->device);
     return window_set_particles(*b->w[(size_t)win], h_particles, nparticles, b->stream, "psc_batch_set_particles");
 }
 
 int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, const int* h_nparticles) {
     if (!b || !h_particles || !h_nparticles) return fail(PSC_E_INVALID, "psc_batch_set_particles_all: null argument");
+    ErrorCapture errors_(b->last_error);
     DeviceScope ds(b->device);
     const char* who = "psc_batch_set_particles_all";
     const size_t nwin = b->w.size();
@@ -1829,6 +1855,7 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
 
 int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_status) {
     if (!b) return fail(PSC_E_INVALID, "psc_batch_step: null handle");
+    ErrorCapture errors_(b->last_error);
     if (nsteps < 0) return fail(PSC_E_INVALID, "psc_batch_step: negative step count");
     if (flags & ~(PSC_RUN_DIAG | PSC_RUN_FIELDS)) return fail(PSC_E_INVALID, "psc_batch_step: unknown flags");
     DeviceScope ds(b->device);
@@ -1904,6 +1931,7 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
 int psc_batch_converge(psc_batch* b, double tol, int check_every, int max_steps, int min_steps, int freeze,
                        psc_status* h_status) {
     if (!b) return fail(PSC_E_INVALID, "psc_batch_converge: null handle");
+    ErrorCapture errors_(b->last_error);
     if (!(tol > 0.0) || check_every < 2 || max_steps < 2 || min_steps < 0)
         return fail(PSC_E_INVALID, "psc_batch_converge: need tol > 0, check_every >= 2, max_steps >= 2");
     DeviceScope ds(b->device);
@@ -1959,9 +1987,12 @@ int psc_batch_converge(psc_batch* b, double tol, int check_every, int max_steps,
     return PSC_OK;
 }
 
+const char* psc_batch_last_error(const psc_batch* b) { return b ? b->last_error.c_str() : ""; }
+
 int psc_batch_get_diag(psc_batch* b, int win, psc_diag* h_diag) {
     if (!b || !h_diag || win < 0 || win >= (int)b->w.size())
         return fail(PSC_E_INVALID, "psc_batch_get_diag: bad arguments");
+    ErrorCapture errors_(b->last_error);
     if (!b->have_diag[(size_t)win])
         return fail(PSC_E_INVALID, "psc_batch_get_diag: no PSC_RUN_DIAG step has run for this window");
     *h_diag = b->last[(size_t)win];
@@ -1970,6 +2001,7 @@ int psc_batch_get_diag(psc_batch* b, int win, psc_diag* h_diag) {
 
 int psc_batch_get_loads(psc_batch* b, int win, double* h_forces, double* h_torques) {
     if (!b || win < 0 || win >= (int)b->w.size()) return fail(PSC_E_INVALID, "psc_batch_get_loads: bad window");
+    ErrorCapture errors_(b->last_error);
     Window& w = *b->w[(size_t)win];
     if (w.P == 0) return PSC_OK;
     if (!h_forces || !h_torques) return fail(PSC_E_INVALID, "psc_batch_get_loads: null output");
@@ -1985,6 +2017,7 @@ int psc_batch_get_loads(psc_batch* b, int win, double* h_forces, double* h_torqu
 
 int psc_batch_get_fields(psc_batch* b, int win, int which, double* h_dst) {
     if (!b || win < 0 || win >= (int)b->w.size()) return fail(PSC_E_INVALID, "psc_batch_get_fields: bad window");
+    ErrorCapture errors_(b->last_error);
     DeviceScope ds(b->device);
     Window& w = *b->w[(size_t)win];
     batch_sync_cur(*b);
@@ -1997,6 +2030,7 @@ int psc_batch_get_fields(psc_batch* b, int win, int which, double* h_dst) {
 // adjoint of the permeability (no counterpart in the reference)
 // ---------------------------------------------------------------------------
 struct psc_adjoint {
+    std::string last_error;  // message of the last failed call on this handle
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -2119,6 +2153,8 @@ int psc_adjoint_create(const psc_config* h_cfg, double smooth_eps, int steps, in
     return PSC_OK;
 }
 
+const char* psc_adjoint_last_error(const psc_adjoint* a) { return a ? a->last_error.c_str() : ""; }
+
 int psc_adjoint_destroy(psc_adjoint* a) {
     if (!a) return PSC_OK;
     DeviceScope ds(a->device);
@@ -2132,6 +2168,7 @@ int psc_adjoint_destroy(psc_adjoint* a) {
 
 int psc_adjoint_forward(psc_adjoint* a, const double* h_particles, int nparticles, double* h_K) {
     if (!a || !h_K) return fail(PSC_E_INVALID, "psc_adjoint_forward: null argument");
+    ErrorCapture errors_(a->last_error);
     DeviceScope ds(a->device);
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_adjoint_forward: cudaSetDevice");
     Window& w = a->w;
@@ -2172,6 +2209,7 @@ int psc_adjoint_forward(psc_adjoint* a, const double* h_particles, int nparticle
 
 int psc_adjoint_backward(psc_adjoint* a, double* h_grad) {
     if (!a) return fail(PSC_E_INVALID, "psc_adjoint_backward: null handle");
+    ErrorCapture errors_(a->last_error);
     if (!a->forward_done) return fail(PSC_E_INVALID, "psc_adjoint_backward: call psc_adjoint_forward first");
     Window& w = a->w;
     if (w.P > 0 && !h_grad) return fail(PSC_E_INVALID, "psc_adjoint_backward: null output");

@@ -349,3 +349,32 @@ def test_batch_reporting_steps_after_freezing():
         Fr, Tr = ref.loads(k)
         assert np.array_equal(Fa, Fr) and np.array_equal(Ta, Tr)
         assert np.array_equal(b.field(k, nat.FIELD_F), ref.field(k, nat.FIELD_F))
+
+
+def test_errors_are_kept_per_handle():
+    """A failing call leaves its message on its own handle (and on the calling thread); other handles
+    keep theirs."""
+    import ctypes
+
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200.handle import BatchHandle, SolverHandle, make_config
+
+    lib = nat.load()
+    cfg = make_config((16, 16, 16), tau=0.8, force=(0.0, 0.0, 1e-6), subsamples=2, store=nat.STORE_F32)
+    a, b = SolverHandle(cfg), SolverHandle(cfg)
+    st = nat.PscStatus()
+    assert lib.psc_solver_last_error(b._h) == b""
+    assert lib.psc_step(a._h, -1, 0, ctypes.byref(st)) == nat.PSC_E_INVALID
+    assert b"negative step count" in lib.psc_solver_last_error(a._h)
+    assert b"negative step count" in lib.psc_last_error()
+    assert lib.psc_solver_last_error(b._h) == b""
+    assert lib.psc_converge(b._h, 0, 1e-8, 1, 1, 0, ctypes.byref(st)) == nat.PSC_E_INVALID
+    assert b"max_steps" in lib.psc_solver_last_error(b._h)
+    assert b"negative step count" in lib.psc_solver_last_error(a._h)
+    a.step(1, nat.RUN_DIAG)  # a successful call keeps the last failure's message
+    assert b"negative step count" in lib.psc_solver_last_error(a._h)
+    bh = BatchHandle([cfg, cfg], graph_steps=0)
+    assert lib.psc_batch_step(bh._h, -1, 0, None) == nat.PSC_E_INVALID
+    assert b"negative step count" in lib.psc_batch_last_error(bh._h)
+    for h in (a, b, bh):
+        h.close()
