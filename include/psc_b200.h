@@ -200,7 +200,7 @@ typedef struct psc_geometry {
      * list; with list_ready == 1 it reduces from the list instead of the whole
      * boxes (same sums, bit for bit: each thread adds the same entries in the same
      * order).  The caller sets list_ready after a call on the same geometry.
-     * Needs chunk_entries a multiple of PSC_LOAD_THREADS, at most 64 of them, and
+     * Needs chunk_entries a multiple of PSC_LOAD_THREADS, at most 16 of them, and
      * nx, ny <= 2048, nz <= 1024; NULL arrays = no list. */
     double* load_w;           /* [capacity_chunks * chunk_entries] or NULL */
     uint32_t* load_abk;       /* [capacity_chunks * chunk_entries] or NULL */

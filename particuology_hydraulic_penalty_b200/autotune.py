@@ -191,6 +191,9 @@ class _SubBatch:
         b.cells = parent.cells[idx]
         b.parity = parent.parity
         b.steps_done = 1
+        b.frozen = {}
+        b._frozen_red = {}
+        b._tables = None
         b._graphs = {}
         b._red = parent._red
         b.kernel = nat.KERNEL_TMA

@@ -51,9 +51,8 @@ __device__ __forceinline__ void offsets(int32_t* off, int32_t xm, int32_t xp, in
     }
 }
 
-__device__ __forceinline__ void cell_offsets(uint32_t cell, int nx, int ny, int nz, int32_t* off) {
-    uint32_t ix, iy, iz;
-    decode(cell, nx, ny, nz, ix, iy, iz);
+__device__ __forceinline__ void coord_offsets(uint32_t ix, uint32_t iy, uint32_t iz, int nx, int ny, int nz,
+                                              int32_t* off) {
     const int32_t nyz = ny * nz;
     const int32_t xm = ix == 0 ? (nx - 1) * nyz : -nyz;
     const int32_t xp = ix == (uint32_t)(nx - 1) ? -(nx - 1) * nyz : nyz;
@@ -63,6 +62,36 @@ __device__ __forceinline__ void cell_offsets(uint32_t cell, int nx, int ny, int 
     const int32_t zp = iz == (uint32_t)(nz - 1) ? -(nz - 1) : 1;
     offsets(off, xm, xp, ym, yp, zm, zp);
 }
+
+__device__ __forceinline__ void cell_offsets(uint32_t cell, int nx, int ny, int nz, int32_t* off) {
+    uint32_t ix, iy, iz;
+    decode(cell, nx, ny, nz, ix, iy, iz);
+    coord_offsets(ix, iy, iz, nx, ny, nz, off);
+}
+
+// Cell coordinates of a grid-stride loop: decoded once, then advanced by the
+// stride's own (x, y, z) digits with carries (no division per cell).
+struct StrideWalk {
+    uint32_t ix, iy, iz, sx, sy, sz, ny, nz;
+    __device__ __forceinline__ StrideWalk(uint32_t cell, uint32_t stride, int nx, int ny_, int nz_) {
+        ny = (uint32_t)ny_;
+        nz = (uint32_t)nz_;
+        decode(cell, nx, ny_, nz_, ix, iy, iz);
+        sz = stride % nz;
+        const uint32_t q = stride / nz;
+        sy = q % ny;
+        sx = q / ny;
+    }
+    __device__ __forceinline__ void next() {
+        iz += sz;
+        const uint32_t cz = iz >= nz;
+        iz -= cz ? nz : 0u;
+        iy += sy + cz;
+        const uint32_t cy = iy >= ny;
+        iy -= cy ? ny : 0u;
+        ix += sx + cy;
+    }
+};
 
 }  // namespace
 
@@ -103,9 +132,11 @@ __global__ void __launch_bounds__(256) k_adjoint_step(psc_adjoint_args a) {
     R* lout = reinterpret_cast<R*>(a.lam_out);
     const R tau = (R)a.tau, inv_tau = R(1) / tau, pref = R(1) - R(0.5) / tau;
     const R Fx = (R)a.force[0], Fy = (R)a.force[1], Fz = (R)a.force[2];
-    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < N; cell += gridDim.x * blockDim.x) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    StrideWalk at(blockIdx.x * blockDim.x + threadIdx.x, stride, a.nx, a.ny, a.nz);
+    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < N; cell += stride, at.next()) {
         int32_t off[Q];
-        cell_offsets(cell, a.nx, a.ny, a.nz, off);
+        coord_offsets(at.ix, at.iy, at.iz, a.nx, a.ny, a.nz, off);
         R g[Q], lam[Q];
 #pragma unroll
         for (int i = 0; i < Q; ++i) {

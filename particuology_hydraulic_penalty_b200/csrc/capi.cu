@@ -293,10 +293,10 @@ int psc_particle_loads(const psc_geometry* h_geo, int imb_type, const void* imb,
     const int lists = (h_geo->load_w != nullptr) + (h_geo->load_abk != nullptr) + (h_geo->load_n != nullptr);
     if (lists != 0 && lists != 3)
         return fail(PSC_E_INVALID, "psc_particle_loads: give all three loads-list arrays or none");
-    if (lists == 3 && (h_geo->chunk_entries % PSC_LOAD_THREADS != 0 || h_geo->chunk_entries / PSC_LOAD_THREADS > 64 ||
+    if (lists == 3 && (h_geo->chunk_entries % PSC_LOAD_THREADS != 0 || h_geo->chunk_entries / PSC_LOAD_THREADS > 16 ||
                        h_geo->nx > 2048 || h_geo->ny > 2048 || h_geo->nz > 1024))
         return fail(PSC_E_INVALID, "psc_particle_loads: the loads list needs chunk_entries a multiple of "
-                                   "PSC_LOAD_THREADS (at most 64 of them) and nx, ny <= 2048, nz <= 1024");
+                                   "PSC_LOAD_THREADS (at most 16 of them) and nx, ny <= 2048, nz <= 1024");
     if (lists == 0 && h_geo->list_ready)
         return fail(PSC_E_INVALID, "psc_particle_loads: list_ready without the loads-list arrays");
     cudaError_t e = launch_particle_loads(*h_geo, imb_type, imb, chunk_partials, imb_sums, forces, torques, diag,

@@ -563,99 +563,111 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
 }
 
 // The list path: the chunk's sums from the loads list a previous call on the
-// same geometry wrote.  Thread t reads its own entries of the chunk (slots
-// slot0 + k * blockDim.x, k < its count: coalesced over the threads) in the
-// order chunk_thread_sums visits them and does the same arithmetic on each, so
-// the sums are bitwise the same; gone are the zero-count entries, the count
-// and alpha-sum gathers and the FP64 division.  A thread loads the weights and
-// cells of U list entries, then their IMB momentum, and only then sums: up to
-// U + U and then 3U loads in flight per thread.
-// List entries per pass: enough loads in flight at two CTAs per SM without
-// spilling (the many-window kernel holds its job's fields in registers, the
-// single-window one reads them from kernel parameters).
-#ifndef PSC_LIST_UNROLL
-#define PSC_LIST_UNROLL 8
-#endif
-#ifndef PSC_LIST_UNROLL_MULTI
-#define PSC_LIST_UNROLL_MULTI 6
-#endif
-template <typename I, bool MULTI>
-constexpr int list_unroll() {
-    return sizeof(I) == 8 ? 4 : (MULTI ? PSC_LIST_UNROLL_MULTI : PSC_LIST_UNROLL);
-}
+// same geometry wrote.  Thread t reduces its own entries of the chunk (slots
+// slot0 + k * blockDim.x, k < its count) in the order chunk_thread_sums visits
+// them, with the same arithmetic on each, so the sums are bitwise the same;
+// gone are the zero-count entries, the count and alpha-sum gathers and the FP64
+// division.
+//
+// The gathers are latency-bound, so a chunk is staged in two asynchronous
+// copies into the thread's own shared-memory column (cp.async, no registers
+// held, no barrier: a thread reads only what it copied): first every list
+// entry of the thread (weight and cell), then the IMB momentum of those cells;
+// the next chunk's descriptor and counts are loaded meanwhile.  Two memory
+// round trips per chunk instead of one per dependent load.
+constexpr int LIST_MAX_K = 16;  // list entries per thread and chunk the staging holds (chunk_entries <= 4096)
 static_assert(LOAD_THREADS == PSC_LOAD_THREADS, "the loads list layout assumes PSC_LOAD_THREADS threads per chunk");
 
-template <typename I, int U>
-__device__ __forceinline__ void chunk_thread_sums_list(const ChunkDesc& dsc, const double* particles,
-                                                       const double* lw, const uint32_t* labk, uint32_t n_t,
-                                                       int64_t slot0, const I* imb, uint32_t N, uint32_t ny,
-                                                       uint32_t nz, double (&acc)[6]) {
-    if (n_t == 0) return;
-    const double* q = particles + (size_t)dsc.p * PF;
-    const uint32_t bx = (uint32_t)dsc.x0, by = (uint32_t)dsc.y0, bz = (uint32_t)dsc.z0;
-    const double qx = q[0], qy = q[1], qz = q[2];
+template <typename I>
+constexpr size_t list_stage_bytes() {
+    return (size_t)LIST_MAX_K * LOAD_THREADS * (sizeof(double) + sizeof(uint32_t) + 3 * sizeof(I));
+}
+
+struct ListCursor {
+    ChunkDesc dsc;
+    uint32_t n_t;
+};
+
+// One chunk's sums of this thread from its staged list column.
+template <typename I>
+__device__ __forceinline__ void list_chunk_sums(const ListCursor& cur, int64_t slot0, const double* particles,
+                                                const double* lw, const uint32_t* labk, const I* imb, uint32_t N,
+                                                uint32_t ny, uint32_t nz, unsigned char* stage, double (&acc)[6]) {
+    const int t = threadIdx.x;
+    const uint32_t n_t = cur.n_t;
+    double* s_w = reinterpret_cast<double*>(stage);
+    uint32_t* s_abk = reinterpret_cast<uint32_t*>(s_w + LIST_MAX_K * LOAD_THREADS);
+    I* s_imb = reinterpret_cast<I*>(s_abk + LIST_MAX_K * LOAD_THREADS);
     const int64_t stride = blockDim.x;
-    for (uint32_t k0 = 0; k0 < n_t; k0 += U) {
-        double ow[U];
-        uint32_t abk[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const bool in = k0 + u < n_t;
-            const int64_t sl = slot0 + (int64_t)(k0 + u) * stride;
-            ow[u] = in ? __ldg(lw + sl) : 0.0;
-            abk[u] = in ? __ldg(labk + sl) : 0u;
-        }
-        I m[U][3];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            m[u][0] = m[u][1] = m[u][2] = I(0);
-            if (k0 + u < n_t) {
-                const uint32_t a = abk[u] & 0x7ffu, b = (abk[u] >> 11) & 0x7ffu, k = abk[u] >> 22;
-                const uint32_t cell = ((bx + a) * ny + (by + b)) * nz + (bz + k);
-                m[u][0] = __ldg(imb + cell);
-                m[u][1] = __ldg(imb + (size_t)N + cell);
-                m[u][2] = __ldg(imb + 2 * (size_t)N + cell);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (k0 + u < n_t) {
-                const uint32_t a = abk[u] & 0x7ffu, b = (abk[u] >> 11) & 0x7ffu, k = abk[u] >> 22;
-                const double nfx = -xmul(ow[u], (double)m[u][0]);
-                const double nfy = -xmul(ow[u], (double)m[u][1]);
-                const double nfz = -xmul(ow[u], (double)m[u][2]);
-                // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
-                const double rx = xsub(xadd((double)(bx + a), 0.5), qx);
-                const double ry = xsub(xadd((double)(by + b), 0.5), qy);
-                const double rz = xsub(xadd((double)(bz + k), 0.5), qz);
-                acc[0] += nfx;
-                acc[1] += nfy;
-                acc[2] += nfz;
-                acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
-                acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
-                acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
-            }
-        }
+    for (uint32_t k = 0; k < n_t; ++k) {
+        cp_async<8>(&s_w[k * LOAD_THREADS + t], lw + slot0 + (int64_t)k * stride);
+        cp_async<4>(&s_abk[k * LOAD_THREADS + t], labk + slot0 + (int64_t)k * stride);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    const uint32_t bx = (uint32_t)cur.dsc.x0, by = (uint32_t)cur.dsc.y0, bz = (uint32_t)cur.dsc.z0;
+    for (uint32_t k = 0; k < n_t; ++k) {
+        const uint32_t abk = s_abk[k * LOAD_THREADS + t];
+        const uint32_t a = abk & 0x7ffu, b = (abk >> 11) & 0x7ffu, kz = abk >> 22;
+        const uint32_t cell = ((bx + a) * ny + (by + b)) * nz + (bz + kz);
+        cp_async<sizeof(I)>(&s_imb[(k * 3 + 0) * LOAD_THREADS + t], imb + cell);
+        cp_async<sizeof(I)>(&s_imb[(k * 3 + 1) * LOAD_THREADS + t], imb + (size_t)N + cell);
+        cp_async<sizeof(I)>(&s_imb[(k * 3 + 2) * LOAD_THREADS + t], imb + 2 * (size_t)N + cell);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    if (n_t == 0) return;
+    const double* q = particles + (size_t)cur.dsc.p * PF;
+    const double qx = q[0], qy = q[1], qz = q[2];
+    for (uint32_t k = 0; k < n_t; ++k) {
+        const uint32_t abk = s_abk[k * LOAD_THREADS + t];
+        const uint32_t a = abk & 0x7ffu, b = (abk >> 11) & 0x7ffu, kz = abk >> 22;
+        const double ow = s_w[k * LOAD_THREADS + t];
+        const double nfx = -xmul(ow, (double)s_imb[(k * 3 + 0) * LOAD_THREADS + t]);
+        const double nfy = -xmul(ow, (double)s_imb[(k * 3 + 1) * LOAD_THREADS + t]);
+        const double nfz = -xmul(ow, (double)s_imb[(k * 3 + 2) * LOAD_THREADS + t]);
+        // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
+        const double rx = xsub(xadd((double)(bx + a), 0.5), qx);
+        const double ry = xsub(xadd((double)(by + b), 0.5), qy);
+        const double rz = xsub(xadd((double)(bz + kz), 0.5), qz);
+        acc[0] += nfx;
+        acc[1] += nfy;
+        acc[2] += nfz;
+        acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
+        acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
+        acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
     }
 }
 
 template <typename I>
-__global__ void __launch_bounds__(LOAD_THREADS, 2) k_loads_chunks_list(psc_geometry g, const I* imb, double* part) {
+__global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list(psc_geometry g, const I* imb, double* part) {
     __shared__ double s[LOAD_THREADS / 32][6];
+    extern __shared__ __align__(16) unsigned char list_stage[];
     const int64_t C = g.totals[1];
     const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
-    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
-        const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
-        const uint32_t n_t = g.load_n[chunk * LOAD_THREADS + threadIdx.x];
+    ListCursor cur{};
+    int64_t chunk = blockIdx.x;
+    if (chunk < C) {
+        cur.dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
+        cur.n_t = g.load_n[chunk * LOAD_THREADS + threadIdx.x];
+    }
+    for (; chunk < C; chunk += gridDim.x) {  // block-uniform
+        // the next chunk's descriptor (its row is overwritten only when this block reduces it) and counts
+        const int64_t nxt = chunk + gridDim.x;
+        ListCursor nc{};
+        if (nxt < C) {
+            nc.dsc = *reinterpret_cast<const ChunkDesc*>(part + nxt * 6);
+            nc.n_t = g.load_n[nxt * LOAD_THREADS + threadIdx.x];
+        }
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        chunk_thread_sums_list<I, list_unroll<I, false>()>(dsc, g.particles, g.load_w, g.load_abk, n_t,
-                                               chunk * g.chunk_entries + threadIdx.x, imb, N, (uint32_t)g.ny,
-                                               (uint32_t)g.nz, acc);
+        list_chunk_sums<I>(cur, chunk * g.chunk_entries + threadIdx.x, g.particles, g.load_w, g.load_abk, imb, N,
+                           (uint32_t)g.ny, (uint32_t)g.nz, list_stage, acc);
         block_sum<6>(acc, s);
         if (threadIdx.x == 0) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
         }
+        cur = nc;
     }
 }
 
@@ -793,26 +805,37 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS)
 
 // The list path for many windows: every job's loads list is current.
 template <typename I>
-__global__ void __launch_bounds__(LOAD_THREADS, 2) k_loads_chunks_list_multi(const LoadsJob* jobs,
+__global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list_multi(const LoadsJob* jobs,
                                                                         const int64_t* chunk_base, int njobs,
                                                                         double* part) {
     __shared__ double s[LOAD_THREADS / 32][6];
+    extern __shared__ __align__(16) unsigned char list_stage[];
     const int64_t C = chunk_base[njobs];
-    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
-        const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
-        const LoadsJob& J = jobs[dsc.pad];
-        const int64_t local = chunk - chunk_base[dsc.pad];
-        const uint32_t n_t = J.g.load_n[local * LOAD_THREADS + threadIdx.x];
+    ListCursor cur{};
+    int64_t chunk = blockIdx.x;
+    if (chunk < C) {
+        cur.dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
+        cur.n_t = jobs[cur.dsc.pad].g.load_n[(chunk - chunk_base[cur.dsc.pad]) * LOAD_THREADS + threadIdx.x];
+    }
+    for (; chunk < C; chunk += gridDim.x) {  // block-uniform
+        const int64_t nxt = chunk + gridDim.x;
+        ListCursor nc{};
+        if (nxt < C) {
+            nc.dsc = *reinterpret_cast<const ChunkDesc*>(part + nxt * 6);
+            nc.n_t = jobs[nc.dsc.pad].g.load_n[(nxt - chunk_base[nc.dsc.pad]) * LOAD_THREADS + threadIdx.x];
+        }
+        const LoadsJob& J = jobs[cur.dsc.pad];
+        const int64_t local = chunk - chunk_base[cur.dsc.pad];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        chunk_thread_sums_list<I, list_unroll<I, true>()>(dsc, J.g.particles, J.g.load_w, J.g.load_abk, n_t,
-                                               local * J.g.chunk_entries + threadIdx.x,
-                                               reinterpret_cast<const I*>(J.imb), (uint32_t)J.g.nx * J.g.ny * J.g.nz,
-                                               (uint32_t)J.g.ny, (uint32_t)J.g.nz, acc);
+        list_chunk_sums<I>(cur, local * J.g.chunk_entries + threadIdx.x, J.g.particles, J.g.load_w, J.g.load_abk,
+                           reinterpret_cast<const I*>(J.imb), (uint32_t)J.g.nx * J.g.ny * J.g.nz, (uint32_t)J.g.ny,
+                           (uint32_t)J.g.nz, list_stage, acc);
         block_sum<6>(acc, s);
         if (threadIdx.x == 0) {
 #pragma unroll
             for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
         }
+        cur = nc;
     }
 }
 
@@ -959,7 +982,15 @@ static cudaError_t loads_smem_optin() {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= kMaxDev || done[dev]) return e;
     const int lut = (16 * 16 * 16 + 1) * (int)sizeof(double);
-    if ((e = cudaFuncSetAttribute(k_loads_chunks<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)) ||
+    if ((e = cudaFuncSetAttribute(k_loads_chunks_list<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)list_stage_bytes<float>())) ||
+        (e = cudaFuncSetAttribute(k_loads_chunks_list<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)list_stage_bytes<double>())) ||
+        (e = cudaFuncSetAttribute(k_loads_chunks_list_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)list_stage_bytes<float>())) ||
+        (e = cudaFuncSetAttribute(k_loads_chunks_list_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)list_stage_bytes<double>())) ||
+        (e = cudaFuncSetAttribute(k_loads_chunks<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)) ||
         (e = cudaFuncSetAttribute(k_loads_chunks<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)) ||
         (e = cudaFuncSetAttribute(k_loads_chunks_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)) ||
         (e = cudaFuncSetAttribute(k_loads_chunks_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lut)))
@@ -981,10 +1012,10 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
         k_chunk_desc<<<(unsigned)(cg < cap ? cg : cap), 256, 0, stream>>>(g, chunk_partials);
         if (g.load_w && g.load_abk && g.load_n && g.list_ready) {  // this geometry's loads list is written
             if (imb_type == 0)
-                k_loads_chunks_list<double><<<grid, LOAD_THREADS, 0, stream>>>(
+                k_loads_chunks_list<double><<<grid, LOAD_THREADS, list_stage_bytes<double>(), stream>>>(
                     g, reinterpret_cast<const double*>(imb), chunk_partials);
             else
-                k_loads_chunks_list<float><<<grid, LOAD_THREADS, 0, stream>>>(
+                k_loads_chunks_list<float><<<grid, LOAD_THREADS, list_stage_bytes<float>(), stream>>>(
                     g, reinterpret_cast<const float*>(imb), chunk_partials);
         } else if (imb_type == 0) {  // (writes the loads list when its arrays are given)
             k_loads_chunks<double><<<grid, LOAD_THREADS, lut, stream>>>(g, reinterpret_cast<const double*>(imb),
@@ -1019,9 +1050,11 @@ cudaError_t launch_particle_loads_multi(const LoadsJob* d_jobs, const int64_t* d
         const unsigned grid = (unsigned)(total_chunks < cap ? total_chunks : cap);
         const size_t lut = (size_t)(max_subsamples * max_subsamples * max_subsamples + 1) * sizeof(double);
         if (list_ready && imb_type == 0)
-            k_loads_chunks_list_multi<double><<<grid, LOAD_THREADS, 0, stream>>>(d_jobs, d_chunk_base, njobs, part);
+            k_loads_chunks_list_multi<double><<<grid, LOAD_THREADS, list_stage_bytes<double>(), stream>>>(
+                d_jobs, d_chunk_base, njobs, part);
         else if (list_ready)
-            k_loads_chunks_list_multi<float><<<grid, LOAD_THREADS, 0, stream>>>(d_jobs, d_chunk_base, njobs, part);
+            k_loads_chunks_list_multi<float><<<grid, LOAD_THREADS, list_stage_bytes<float>(), stream>>>(
+                d_jobs, d_chunk_base, njobs, part);
         else if (imb_type == 0)
             k_loads_chunks_multi<double><<<grid, LOAD_THREADS, lut, stream>>>(d_jobs, d_chunk_base, njobs, part);
         else

@@ -43,8 +43,12 @@ namespace {
 
 constexpr int kQ = 19;
 constexpr int kChunkEntries = 4096;  // bbox entries per load-reduction chunk
-static_assert(kChunkEntries % PSC_LOAD_THREADS == 0 && kChunkEntries / PSC_LOAD_THREADS <= 64,
-              "the loads list holds at most 64 entries per thread and chunk");
+// Host threads (besides the caller's) that stage a batch's particle uploads.
+#ifndef PSC_STAGING_THREADS
+#define PSC_STAGING_THREADS 3
+#endif
+static_assert(kChunkEntries % PSC_LOAD_THREADS == 0 && kChunkEntries / PSC_LOAD_THREADS <= 16,
+              "the loads list holds at most 16 entries per thread and chunk");
 constexpr int kOutLen = 2 * PSC_NRED + PSC_NDIAG;  // [red_pre][red_post][diag]
 
 // Owned device array (contents are not kept when it grows).  A grow allocates
@@ -1818,7 +1822,7 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
     // more than 256 KiB of particle state: the windows are staged on the handle's host threads
     if (total * 8 > (1 << 18) && nwin > 1 && !b->pool_tried) {
         b->pool_tried = true;
-        b->pool.start(3);
+        b->pool.start(PSC_STAGING_THREADS);
     }
     if (total * 8 > (1 << 18) && nwin > 1 && b->pool.ready()) b->pool.run((int)nwin, stage);
     else
