@@ -575,12 +575,12 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
 // entry of the thread (weight and cell), then the IMB momentum of those cells;
 // the next chunk's descriptor and counts are loaded meanwhile.  Two memory
 // round trips per chunk instead of one per dependent load.
-constexpr int LIST_MAX_K = 16;  // list entries per thread and chunk the staging holds (chunk_entries <= 4096)
+constexpr int LIST_STAGE_K = 8;  // list entries per thread staged at a time (a column holds up to 16: two passes)
 static_assert(LOAD_THREADS == PSC_LOAD_THREADS, "the loads list layout assumes PSC_LOAD_THREADS threads per chunk");
 
 template <typename I>
 constexpr size_t list_stage_bytes() {
-    return (size_t)LIST_MAX_K * LOAD_THREADS * (sizeof(double) + sizeof(uint32_t) + 3 * sizeof(I));
+    return (size_t)LIST_STAGE_K * LOAD_THREADS * (sizeof(double) + sizeof(uint32_t) + 3 * sizeof(I));
 }
 
 struct ListCursor {
@@ -588,54 +588,58 @@ struct ListCursor {
     uint32_t n_t;
 };
 
-// One chunk's sums of this thread from its staged list column.
+// One chunk's sums of this thread from its list column, staged LIST_STAGE_K
+// entries at a time; the entries are added in list order.
 template <typename I>
 __device__ __forceinline__ void list_chunk_sums(const ListCursor& cur, int64_t slot0, const double* particles,
                                                 const double* lw, const uint32_t* labk, const I* imb, uint32_t N,
                                                 uint32_t ny, uint32_t nz, unsigned char* stage, double (&acc)[6]) {
     const int t = threadIdx.x;
     const uint32_t n_t = cur.n_t;
-    double* s_w = reinterpret_cast<double*>(stage);
-    uint32_t* s_abk = reinterpret_cast<uint32_t*>(s_w + LIST_MAX_K * LOAD_THREADS);
-    I* s_imb = reinterpret_cast<I*>(s_abk + LIST_MAX_K * LOAD_THREADS);
-    const int64_t stride = blockDim.x;
-    for (uint32_t k = 0; k < n_t; ++k) {
-        cp_async<8>(&s_w[k * LOAD_THREADS + t], lw + slot0 + (int64_t)k * stride);
-        cp_async<4>(&s_abk[k * LOAD_THREADS + t], labk + slot0 + (int64_t)k * stride);
-    }
-    cp_async_commit();
-    cp_async_wait<0>();
-    const uint32_t bx = (uint32_t)cur.dsc.x0, by = (uint32_t)cur.dsc.y0, bz = (uint32_t)cur.dsc.z0;
-    for (uint32_t k = 0; k < n_t; ++k) {
-        const uint32_t abk = s_abk[k * LOAD_THREADS + t];
-        const uint32_t a = abk & 0x7ffu, b = (abk >> 11) & 0x7ffu, kz = abk >> 22;
-        const uint32_t cell = ((bx + a) * ny + (by + b)) * nz + (bz + kz);
-        cp_async<sizeof(I)>(&s_imb[(k * 3 + 0) * LOAD_THREADS + t], imb + cell);
-        cp_async<sizeof(I)>(&s_imb[(k * 3 + 1) * LOAD_THREADS + t], imb + (size_t)N + cell);
-        cp_async<sizeof(I)>(&s_imb[(k * 3 + 2) * LOAD_THREADS + t], imb + 2 * (size_t)N + cell);
-    }
-    cp_async_commit();
-    cp_async_wait<0>();
     if (n_t == 0) return;
+    double* s_w = reinterpret_cast<double*>(stage);
+    uint32_t* s_abk = reinterpret_cast<uint32_t*>(s_w + LIST_STAGE_K * LOAD_THREADS);
+    I* s_imb = reinterpret_cast<I*>(s_abk + LIST_STAGE_K * LOAD_THREADS);
+    const int64_t stride = blockDim.x;
+    const uint32_t bx = (uint32_t)cur.dsc.x0, by = (uint32_t)cur.dsc.y0, bz = (uint32_t)cur.dsc.z0;
     const double* q = particles + (size_t)cur.dsc.p * PF;
     const double qx = q[0], qy = q[1], qz = q[2];
-    for (uint32_t k = 0; k < n_t; ++k) {
-        const uint32_t abk = s_abk[k * LOAD_THREADS + t];
-        const uint32_t a = abk & 0x7ffu, b = (abk >> 11) & 0x7ffu, kz = abk >> 22;
-        const double ow = s_w[k * LOAD_THREADS + t];
-        const double nfx = -xmul(ow, (double)s_imb[(k * 3 + 0) * LOAD_THREADS + t]);
-        const double nfy = -xmul(ow, (double)s_imb[(k * 3 + 1) * LOAD_THREADS + t]);
-        const double nfz = -xmul(ow, (double)s_imb[(k * 3 + 2) * LOAD_THREADS + t]);
-        // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
-        const double rx = xsub(xadd((double)(bx + a), 0.5), qx);
-        const double ry = xsub(xadd((double)(by + b), 0.5), qy);
-        const double rz = xsub(xadd((double)(bz + kz), 0.5), qz);
-        acc[0] += nfx;
-        acc[1] += nfy;
-        acc[2] += nfz;
-        acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
-        acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
-        acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
+    for (uint32_t k0 = 0; k0 < n_t; k0 += LIST_STAGE_K) {
+        const uint32_t m = n_t - k0 < (uint32_t)LIST_STAGE_K ? n_t - k0 : (uint32_t)LIST_STAGE_K;
+        for (uint32_t k = 0; k < m; ++k) {
+            cp_async<8>(&s_w[k * LOAD_THREADS + t], lw + slot0 + (int64_t)(k0 + k) * stride);
+            cp_async<4>(&s_abk[k * LOAD_THREADS + t], labk + slot0 + (int64_t)(k0 + k) * stride);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        for (uint32_t k = 0; k < m; ++k) {
+            const uint32_t abk = s_abk[k * LOAD_THREADS + t];
+            const uint32_t a = abk & 0x7ffu, b = (abk >> 11) & 0x7ffu, kz = abk >> 22;
+            const uint32_t cell = ((bx + a) * ny + (by + b)) * nz + (bz + kz);
+            cp_async<sizeof(I)>(&s_imb[(k * 3 + 0) * LOAD_THREADS + t], imb + cell);
+            cp_async<sizeof(I)>(&s_imb[(k * 3 + 1) * LOAD_THREADS + t], imb + (size_t)N + cell);
+            cp_async<sizeof(I)>(&s_imb[(k * 3 + 2) * LOAD_THREADS + t], imb + 2 * (size_t)N + cell);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        for (uint32_t k = 0; k < m; ++k) {
+            const uint32_t abk = s_abk[k * LOAD_THREADS + t];
+            const uint32_t a = abk & 0x7ffu, b = (abk >> 11) & 0x7ffu, kz = abk >> 22;
+            const double ow = s_w[k * LOAD_THREADS + t];
+            const double nfx = -xmul(ow, (double)s_imb[(k * 3 + 0) * LOAD_THREADS + t]);
+            const double nfy = -xmul(ow, (double)s_imb[(k * 3 + 1) * LOAD_THREADS + t]);
+            const double nfz = -xmul(ow, (double)s_imb[(k * 3 + 2) * LOAD_THREADS + t]);
+            // torque arm (i + 0.5) - X, no periodic wrap   (psc3d.py:397-402)
+            const double rx = xsub(xadd((double)(bx + a), 0.5), qx);
+            const double ry = xsub(xadd((double)(by + b), 0.5), qy);
+            const double rz = xsub(xadd((double)(bz + kz), 0.5), qz);
+            acc[0] += nfx;
+            acc[1] += nfy;
+            acc[2] += nfz;
+            acc[3] += xsub(xmul(ry, nfz), xmul(rz, nfy));
+            acc[4] += xsub(xmul(rz, nfx), xmul(rx, nfz));
+            acc[5] += xsub(xmul(rx, nfy), xmul(ry, nfx));
+        }
     }
 }
 

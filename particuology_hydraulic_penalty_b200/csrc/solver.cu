@@ -12,17 +12,12 @@
 // One call runs any number of steps with no host work between them except
 // where the caller asks for per-step diagnostics (the lbm_converge loop).
 #include <algorithm>
-#include <atomic>
 #include <cmath>
-#include <condition_variable>
 #include <cstddef>
 #include <cstring>
-#include <functional>
 #include <memory>
-#include <mutex>
 #include <new>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "internal.cuh"
@@ -43,10 +38,6 @@ namespace {
 
 constexpr int kQ = 19;
 constexpr int kChunkEntries = 4096;  // bbox entries per load-reduction chunk
-// Host threads (besides the caller's) that stage a batch's particle uploads.
-#ifndef PSC_STAGING_THREADS
-#define PSC_STAGING_THREADS 3
-#endif
 static_assert(kChunkEntries % PSC_LOAD_THREADS == 0 && kChunkEntries / PSC_LOAD_THREADS <= 16,
               "the loads list holds at most 16 entries per thread and chunk");
 constexpr int kOutLen = 2 * PSC_NRED + PSC_NDIAG;  // [red_pre][red_post][diag]
@@ -105,93 +96,6 @@ struct HArray {
         n = m;
         return cudaSuccess;
     }
-};
-
-// A few host threads kept by a handle for its per-window host work (staging
-// particle arrays into page-locked memory): run(n, f) calls f(0) .. f(n - 1),
-// spread over the workers and the calling thread, and returns when every call
-// has finished and no worker is still looking for work, so one run's tasks
-// never mix with the next run's.  f must not throw.  Handles are
-// single-threaded, so run() is never reentered.
-class HostPool {
-  public:
-    HostPool() = default;
-    HostPool(const HostPool&) = delete;
-    HostPool& operator=(const HostPool&) = delete;
-    ~HostPool() {
-        {
-            std::lock_guard<std::mutex> lock(m_);
-            stop_ = true;
-        }
-        wake_.notify_all();
-        for (auto& t : threads_) t.join();
-    }
-    // Starts up to `workers` threads (fewer on a machine with fewer cores); false if none started.
-    bool start(int workers) {
-        const int hw = (int)std::thread::hardware_concurrency();
-        workers = std::min(workers, std::max(0, hw - 1));
-        for (int i = 0; i < workers; ++i) {
-            try {
-                threads_.emplace_back([this] { loop(); });
-            } catch (...) {
-                break;
-            }
-        }
-        return !threads_.empty();
-    }
-    bool ready() const { return !threads_.empty(); }
-    void run(int n, const std::function<void(int)>& f) {
-        {
-            std::lock_guard<std::mutex> lock(m_);
-            job_.store(&f);
-            count_.store(n);
-            done_ = 0;
-            next_.store(0);
-            ++generation_;
-        }
-        wake_.notify_all();
-        work();
-        std::unique_lock<std::mutex> lock(m_);
-        finished_.wait(lock, [this] { return done_ == count_.load() && active_ == 0; });
-        job_.store(nullptr);
-        count_.store(0);
-    }
-
-  private:
-    void work() {
-        int finished_here = 0;
-        for (int i = next_.fetch_add(1); i < count_.load(); i = next_.fetch_add(1)) {
-            (*job_.load())(i);
-            ++finished_here;
-        }
-        std::lock_guard<std::mutex> lock(m_);
-        done_ += finished_here;
-        finished_.notify_all();
-    }
-    void loop() {
-        uint64_t seen = 0;
-        for (;;) {
-            {
-                std::unique_lock<std::mutex> lock(m_);
-                wake_.wait(lock, [&] { return stop_ || generation_ != seen; });
-                if (stop_) return;
-                seen = generation_;
-                ++active_;
-            }
-            work();
-            std::lock_guard<std::mutex> lock(m_);
-            --active_;
-            finished_.notify_all();
-        }
-    }
-    std::vector<std::thread> threads_;
-    std::mutex m_;
-    std::condition_variable wake_, finished_;
-    std::atomic<const std::function<void(int)>*> job_{nullptr};
-    std::atomic<int> count_{0}, next_{0};
-    int done_ = 0, active_ = 0;
-    uint64_t generation_ = 0;
-    bool stop_ = false;
 };
 
 // Makes the handle's device current for the duration of a call.
@@ -1455,8 +1359,6 @@ struct psc_batch {
     HArray<double> up_host;    // every window's particles, staged for one upload
     DArray<double> up_dev;
     cudaEvent_t up_done = nullptr;
-    HostPool pool;             // stages large particle uploads window by window in parallel
-    bool pool_tried = false;
     // particle loads of all active windows in one launch sequence: job table
     // [LoadsJob x n][chunk bases n+1][particle bases n+1], as last uploaded
     std::vector<unsigned char> jobs_last;
@@ -1819,14 +1721,7 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
         else if (P > 0) std::memcpy(dst, h_particles[k], n10 * sizeof(double));
         known[(size_t)k] = same ? 1 : (particles_finite(h_particles[k], n10) ? 2 : -1);
     };
-    // more than 256 KiB of particle state: the windows are staged on the handle's host threads
-    if (total * 8 > (1 << 18) && nwin > 1 && !b->pool_tried) {
-        b->pool_tried = true;
-        b->pool.start(PSC_STAGING_THREADS);
-    }
-    if (total * 8 > (1 << 18) && nwin > 1 && b->pool.ready()) b->pool.run((int)nwin, stage);
-    else
-        for (size_t k = 0; k < nwin; ++k) stage((int)k);
+    for (size_t k = 0; k < nwin; ++k) stage((int)k);
     for (size_t k = 0; k < nwin; ++k)
         if (known[k] < 0)
             return fail(PSC_E_INVALID,
