@@ -588,8 +588,29 @@ struct ListCursor {
     uint32_t n_t;
 };
 
-// One chunk's sums of this thread from its list column, staged LIST_STAGE_K
-// entries at a time; the entries are added in list order.
+// Asynchronous copy of list entries k0 .. k0 + m - 1 of this thread's column
+// (weight and cell) into its stage slots 0 .. m - 1.
+__device__ __forceinline__ void list_issue(int64_t slot0, const double* lw, const uint32_t* labk, uint32_t k0,
+                                           uint32_t m, unsigned char* stage) {
+    const int t = threadIdx.x;
+    double* s_w = reinterpret_cast<double*>(stage);
+    uint32_t* s_abk = reinterpret_cast<uint32_t*>(s_w + LIST_STAGE_K * LOAD_THREADS);
+    const int64_t stride = blockDim.x;
+    for (uint32_t k = 0; k < m; ++k) {
+        cp_async<8>(&s_w[k * LOAD_THREADS + t], lw + slot0 + (int64_t)(k0 + k) * stride);
+        cp_async<4>(&s_abk[k * LOAD_THREADS + t], labk + slot0 + (int64_t)(k0 + k) * stride);
+    }
+    cp_async_commit();
+}
+
+__device__ __forceinline__ uint32_t list_pass_size(uint32_t n_t, uint32_t k0) {
+    return n_t - k0 < (uint32_t)LIST_STAGE_K ? n_t - k0 : (uint32_t)LIST_STAGE_K;
+}
+
+// One chunk's sums of this thread from its list column, LIST_STAGE_K entries
+// at a time, in list order.  The first pass's list copy was issued already
+// (list_issue with k0 = 0); each pass waits for its list entries, copies the
+// IMB momentum of their cells, waits again and adds them up.
 template <typename I>
 __device__ __forceinline__ void list_chunk_sums(const ListCursor& cur, int64_t slot0, const double* particles,
                                                 const double* lw, const uint32_t* labk, const I* imb, uint32_t N,
@@ -600,17 +621,12 @@ __device__ __forceinline__ void list_chunk_sums(const ListCursor& cur, int64_t s
     double* s_w = reinterpret_cast<double*>(stage);
     uint32_t* s_abk = reinterpret_cast<uint32_t*>(s_w + LIST_STAGE_K * LOAD_THREADS);
     I* s_imb = reinterpret_cast<I*>(s_abk + LIST_STAGE_K * LOAD_THREADS);
-    const int64_t stride = blockDim.x;
     const uint32_t bx = (uint32_t)cur.dsc.x0, by = (uint32_t)cur.dsc.y0, bz = (uint32_t)cur.dsc.z0;
     const double* q = particles + (size_t)cur.dsc.p * PF;
     const double qx = q[0], qy = q[1], qz = q[2];
     for (uint32_t k0 = 0; k0 < n_t; k0 += LIST_STAGE_K) {
-        const uint32_t m = n_t - k0 < (uint32_t)LIST_STAGE_K ? n_t - k0 : (uint32_t)LIST_STAGE_K;
-        for (uint32_t k = 0; k < m; ++k) {
-            cp_async<8>(&s_w[k * LOAD_THREADS + t], lw + slot0 + (int64_t)(k0 + k) * stride);
-            cp_async<4>(&s_abk[k * LOAD_THREADS + t], labk + slot0 + (int64_t)(k0 + k) * stride);
-        }
-        cp_async_commit();
+        const uint32_t m = list_pass_size(n_t, k0);
+        if (k0 > 0) list_issue(slot0, lw, labk, k0, m, stage);
         cp_async_wait<0>();
         for (uint32_t k = 0; k < m; ++k) {
             const uint32_t abk = s_abk[k * LOAD_THREADS + t];
@@ -643,6 +659,9 @@ __device__ __forceinline__ void list_chunk_sums(const ListCursor& cur, int64_t s
     }
 }
 
+// A chunk's list entries overlap the previous chunk's block sum: each thread
+// issues the next chunk's first list copy as soon as its own sums are done (its
+// stage slots are free then), before the barrier.
 template <typename I>
 __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list(psc_geometry g, const I* imb, double* part) {
     __shared__ double s[LOAD_THREADS / 32][6];
@@ -654,6 +673,8 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list(psc_geometry
     if (chunk < C) {
         cur.dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
         cur.n_t = g.load_n[chunk * LOAD_THREADS + threadIdx.x];
+        list_issue(chunk * g.chunk_entries + threadIdx.x, g.load_w, g.load_abk, 0, list_pass_size(cur.n_t, 0),
+                   list_stage);
     }
     for (; chunk < C; chunk += gridDim.x) {  // block-uniform
         // the next chunk's descriptor (its row is overwritten only when this block reduces it) and counts
@@ -666,6 +687,9 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list(psc_geometry
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         list_chunk_sums<I>(cur, chunk * g.chunk_entries + threadIdx.x, g.particles, g.load_w, g.load_abk, imb, N,
                            (uint32_t)g.ny, (uint32_t)g.nz, list_stage, acc);
+        if (nxt < C)
+            list_issue(nxt * g.chunk_entries + threadIdx.x, g.load_w, g.load_abk, 0, list_pass_size(nc.n_t, 0),
+                       list_stage);
         block_sum<6>(acc, s);
         if (threadIdx.x == 0) {
 #pragma unroll
@@ -819,7 +843,11 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list_multi(const 
     int64_t chunk = blockIdx.x;
     if (chunk < C) {
         cur.dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
-        cur.n_t = jobs[cur.dsc.pad].g.load_n[(chunk - chunk_base[cur.dsc.pad]) * LOAD_THREADS + threadIdx.x];
+        const psc_geometry& g0 = jobs[cur.dsc.pad].g;
+        const int64_t local0 = chunk - chunk_base[cur.dsc.pad];
+        cur.n_t = g0.load_n[local0 * LOAD_THREADS + threadIdx.x];
+        list_issue(local0 * g0.chunk_entries + threadIdx.x, g0.load_w, g0.load_abk, 0, list_pass_size(cur.n_t, 0),
+                   list_stage);
     }
     for (; chunk < C; chunk += gridDim.x) {  // block-uniform
         const int64_t nxt = chunk + gridDim.x;
@@ -834,6 +862,11 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list_multi(const 
         list_chunk_sums<I>(cur, local * J.g.chunk_entries + threadIdx.x, J.g.particles, J.g.load_w, J.g.load_abk,
                            reinterpret_cast<const I*>(J.imb), (uint32_t)J.g.nx * J.g.ny * J.g.nz, (uint32_t)J.g.ny,
                            (uint32_t)J.g.nz, list_stage, acc);
+        if (nxt < C) {  // the next chunk's first list copy, overlapping this chunk's block sum
+            const psc_geometry& gn = jobs[nc.dsc.pad].g;
+            list_issue((nxt - chunk_base[nc.dsc.pad]) * gn.chunk_entries + threadIdx.x, gn.load_w, gn.load_abk, 0,
+                       list_pass_size(nc.n_t, 0), list_stage);
+        }
         block_sum<6>(acc, s);
         if (threadIdx.x == 0) {
 #pragma unroll
