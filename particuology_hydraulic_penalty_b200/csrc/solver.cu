@@ -552,9 +552,19 @@ int window_solid_velocity(Window& w, cudaStream_t s) {
 }
 
 // Geometry and solid velocity up to date for the next step (psc3d.py:209-210, :215).
+bool window_needs_rebuild(const Window& w) {
+    return !w.built || (!w.cfg.static_geometry && w.built_version != w.pversion);
+}
+bool window_needs_solid_velocity(const Window& w) { return w.moving && w.us_version != w.pversion; }
+
+// Whether window_prepare will launch work that reads the particle array.
+bool window_prepare_reads_particles(const Window& w) {
+    return window_needs_rebuild(w) || window_needs_solid_velocity(w);
+}
+
 int window_prepare(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* who) {
-    if (!w.built || (!w.cfg.static_geometry && w.built_version != w.pversion)) PSC_TRY(window_rebuild(w, s, tot, who));
-    if (w.moving && w.us_version != w.pversion) PSC_TRY(window_solid_velocity(w, s));
+    if (window_needs_rebuild(w)) PSC_TRY(window_rebuild(w, s, tot, who));
+    if (window_needs_solid_velocity(w)) PSC_TRY(window_solid_velocity(w, s));
     return PSC_OK;
 }
 
@@ -1358,7 +1368,14 @@ struct psc_batch {
     Lanes lanes;  // particle loads of the windows beside the post-stream reduction pass
     HArray<double> up_host;    // every window's particles, staged for one upload
     DArray<double> up_dev;
+    // The upload runs on its own stream beside the step kernels, which do not
+    // read particles: up_ready (on the main stream) orders it after every
+    // earlier reader of up_dev, up_done ends it.  Until the main stream has
+    // waited for up_done (up_pending), whatever reads particles waits first.
+    cudaStream_t up_stream = nullptr;
+    cudaEvent_t up_ready = nullptr;
     cudaEvent_t up_done = nullptr;
+    bool up_pending = false;
     // particle loads of all active windows in one launch sequence: job table
     // [LoadsJob x n][chunk bases n+1][particle bases n+1], as last uploaded
     std::vector<unsigned char> jobs_last;
@@ -1373,6 +1390,8 @@ struct psc_batch {
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
         if (up_done) cudaEventDestroy(up_done);
+        if (up_ready) cudaEventDestroy(up_ready);
+        if (up_stream) cudaStreamDestroy(up_stream);
     }
 };
 
@@ -1497,10 +1516,20 @@ int batch_launch(psc_batch& b, unsigned flags) {
                                b.stream);
 }
 
+// The main stream waits for a pending particle upload (psc_batch_set_particles_all):
+// everything queued on it afterwards, lanes forked from it included, sees the new state.
+int batch_upload_join(psc_batch& b, const char* who) {
+    if (!b.up_pending) return PSC_OK;
+    PSC_CUDA(cudaStreamWaitEvent(b.stream, b.up_done, 0), who);
+    b.up_pending = false;
+    return PSC_OK;
+}
+
 // Everything the next step reads is on the device and described by the tables.
 int batch_prepare(psc_batch& b, bool imb, bool moments) {
     for (size_t k = 0; k < b.w.size(); ++k) {
         Window& w = *b.w[k];
+        if (window_prepare_reads_particles(w)) PSC_TRY(batch_upload_join(b, "psc_batch_step"));
         PSC_TRY(window_prepare(w, b.stream, b.tot, "psc_batch_step"));
         if (imb) PSC_TRY(window_ensure_imb(w, b.stream));
         if (moments) PSC_TRY(window_ensure_moments(w, b.stream));
@@ -1656,6 +1685,8 @@ int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_lau
         if (e == cudaSuccess) e = b->host.ensure((int64_t)nwin * kOutLen);
         if (e == cudaSuccess) e = b->lanes.init(1);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->up_done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->up_ready, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->up_stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) st = cuda_fail(e, "psc_batch_create");
     }
@@ -1671,6 +1702,7 @@ int psc_batch_destroy(psc_batch* b) {
     if (!b) return PSC_OK;
     DeviceScope ds(b->device);
     cudaStreamSynchronize(b->stream);
+    if (b->up_stream) cudaStreamSynchronize(b->up_stream);
     cudaStream_t s = b->stream;
     bool own = b->own_stream;
     delete b;
@@ -1682,6 +1714,7 @@ int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, in
     if (!b || win < 0 || win >= (int)b->w.size()) return fail(PSC_E_INVALID, "psc_batch_set_particles: bad window");
     ErrorCapture errors_(b->last_error);
     DeviceScope ds(b->device);
+    PSC_TRY(batch_upload_join(*b, "psc_batch_set_particles"));
     return window_set_particles(*b->w[(size_t)win], h_particles, nparticles, b->stream, "psc_batch_set_particles");
 }
 
@@ -1744,11 +1777,15 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
         w.ext_particles = b->up_dev.p + off;
         off += (int64_t)P * 10;
     }
+    // after every kernel queued so far (they may read up_dev), on the upload stream
+    PSC_CUDA(cudaEventRecord(b->up_ready, b->stream), who);
+    PSC_CUDA(cudaStreamWaitEvent(b->up_stream, b->up_ready, 0), who);
     if (off > 0)
         PSC_CUDA(cudaMemcpyAsync(b->up_dev.p, b->up_host.p, (size_t)off * sizeof(double), cudaMemcpyHostToDevice,
-                                 b->stream),
+                                 b->up_stream),
                  who);
-    PSC_CUDA(cudaEventRecord(b->up_done, b->stream), who);
+    PSC_CUDA(cudaEventRecord(b->up_done, b->up_stream), who);
+    b->up_pending = true;
     return PSC_OK;
 }
 
@@ -1775,6 +1812,8 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
         // geometry only: on a lane, beside the reduction pass
         PSC_TRY(batch_loads_table(*b, "psc_batch_step"));
         PSC_CUDA(b->lanes.begin(b->stream), "psc_batch_step");
+        if (b->up_pending)  // the loads read the particles: after their upload
+            PSC_CUDA(cudaStreamWaitEvent(b->lanes.lane(0), b->up_done, 0), "psc_batch_step");
         PSC_CUDA(launch_particle_loads_multi(reinterpret_cast<const LoadsJob*>(b->jobs_dev.p), batch_chunk_base(*b),
                                              batch_particle_base(*b), b->jobs_n, b->jobs_chunks, b->jobs_particles,
                                              b->w[0]->field_type(), b->jobs_max_s, b->jobs_list_ready,
@@ -1817,6 +1856,7 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
     } else {
         PSC_CUDA(cudaGetLastError(), "psc_batch_step");
     }
+    PSC_TRY(batch_upload_join(*b, "psc_batch_step"));  // later calls see the main stream after the upload
     if (h_status)
         for (int k = 0; k < nwin; ++k) {
             h_status[k] = psc_status{};
@@ -1836,6 +1876,7 @@ int psc_batch_converge(psc_batch* b, double tol, int check_every, int max_steps,
     DeviceScope ds(b->device);
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_batch_converge: cudaSetDevice");
     const int nwin = (int)b->w.size();
+    PSC_TRY(batch_upload_join(*b, "psc_batch_converge"));
     PSC_TRY(batch_prepare(*b, false, false));
     std::vector<double> r1((size_t)nwin * PSC_NRED), r2((size_t)nwin * PSC_NRED);
     std::vector<int> conv((size_t)nwin, -1);
@@ -1920,6 +1961,7 @@ int psc_batch_get_fields(psc_batch* b, int win, int which, double* h_dst) {
     DeviceScope ds(b->device);
     Window& w = *b->w[(size_t)win];
     batch_sync_cur(*b);
+    PSC_TRY(batch_upload_join(*b, "psc_batch_get_fields"));
     return window_get_field(w, which, h_dst, b->stream, b->tot, "psc_batch_get_fields");
 }
 
