@@ -259,7 +259,8 @@ int psc_plan_row_tiles(struct psc_window* h_windows, int nwin, int rows, int ele
  * window needs an even nz (a cell pair never crosses a z row). */
 int psc_plan_pair_tiles(struct psc_window* h_windows, int nwin, int64_t* h_total_tiles);
 /* Device-side status word: non-zero after a kernel gave up a bounded wait
- * (0x101 producer, 0x102 drain, 0x103 consumer) or skipped a window it
+ * (0x101 producer, 0x102 drain, 0x103 consumer of the TMA kernel; 0x301 a
+ * load-chunk kernel's wait for a partial-sum slot) or skipped a window it
  * cannot run (0x201 odd nz, 0x202 tiles not planned for the pair kernel).
  * Synchronises. */
 int psc_device_status(int* h_status, int clear);

@@ -170,10 +170,11 @@ int psc_plan_row_tiles(psc_window* h_windows, int nwin, int rows, int elem_bytes
 
 int psc_device_status(int* h_status, int clear) {
     if (!h_status) return fail(PSC_E_INVALID, "psc_device_status: null output");
-    int tma = 0, pair = 0;
+    int tma = 0, pair = 0, loads = 0;
     cudaError_t e = read_device_status(&tma, clear != 0);
     if (e == cudaSuccess) e = read_pair_status(&pair, clear != 0);
-    *h_status = tma ? tma : pair;
+    if (e == cudaSuccess) e = read_loads_status(&loads, clear != 0);
+    *h_status = tma ? tma : (pair ? pair : loads);
     return e == cudaSuccess ? PSC_OK : cuda_fail(e, "psc_device_status");
 }
 

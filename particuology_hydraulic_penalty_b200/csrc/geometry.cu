@@ -314,34 +314,90 @@ __global__ void k_solid_velocity(psc_geometry g, O* us) {
     }
 }
 
-template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double (*s)[NV]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double x = v[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) s[warp][k] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double acc = 0.0;
-            for (int w = 0; w < nw; ++w) acc += s[w][k];
-            v[k] = acc;
-        }
+constexpr int LOAD_THREADS = 256;
+constexpr int LOAD_WARPS = LOAD_THREADS / 32;
+
+// Chunk sums without a block barrier per chunk.  Every warp of a block visits
+// the block's chunks in the same order (its threads' columns of each), adds
+// its 32 threads' sums by an xor-shuffle tree and leaves the warp sum in a
+// ring slot of the chunk; the warp that completes the slot's count adds the
+// LOAD_WARPS warp sums in warp order from 0.0 and writes the chunk row (the
+// order of a block reduction through shared memory by thread 0).  A warp runs up
+// to CHUNK_RING chunks ahead of the slowest warp of its block before it waits
+// for a slot.  The slowest warp never waits, so every wait ends; the wait is
+// bounded all the same (status 0x301, psc_device_status).
+//
+// With a barrier per chunk the block moved at the pace of its slowest warp
+// (threads own 0 to 16 list entries of a chunk, one or two staging passes)
+// and ncu counted 4.2 barrier stalls per issue on the list kernel; without
+// it the 24-window batch's list reduction took 318 us instead of 427.
+constexpr int CHUNK_RING = 4;
+__device__ int g_loads_status = 0;
+
+struct ChunkRing {
+    double v[CHUNK_RING][LOAD_WARPS][6];
+    int count[CHUNK_RING];
+    long long done[CHUNK_RING];  // block-local index of the chunk last written from the slot
+};
+
+__device__ __forceinline__ void chunk_ring_init(ChunkRing& r) {
+    if (threadIdx.x < CHUNK_RING) {
+        r.count[threadIdx.x] = 0;
+        r.done[threadIdx.x] = (long long)threadIdx.x - CHUNK_RING;
     }
     __syncthreads();
 }
 
-constexpr int LOAD_THREADS = 256;
+// Warp-level end of the block's j-th chunk: acc (this thread's sums) joins
+// the chunk's row once every warp of the block has finished the chunk.
+__device__ __forceinline__ void chunk_ring_finish(ChunkRing& r, long long j, double (&acc)[6], double* row) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = (int)(j % CHUNK_RING);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        double x = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        acc[k] = x;
+    }
+    if (lane == 0) {
+        volatile long long* done = r.done;
+        uint32_t spins = 0;
+        while (done[slot] != j - CHUNK_RING) {  // the slot's previous chunk is written out
+            if (++spins > (1u << 24)) {
+                atomicCAS(&g_loads_status, 0, 0x301);
+                break;
+            }
+            __nanosleep(64);
+        }
+        volatile double* v = &r.v[slot][warp][0];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = acc[k];
+        __threadfence_block();
+        if (atomicAdd(&r.count[slot], 1) == LOAD_WARPS - 1) {  // the chunk's last warp
+            __threadfence_block();
+            volatile const double* all = &r.v[slot][0][0];
+            double out[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                double s = 0.0;
+                for (int w = 0; w < LOAD_WARPS; ++w) s += all[w * 6 + k];
+                out[k] = s;
+            }
+#pragma unroll
+            for (int k = 0; k < 6; ++k) row[k] = out[k];
+            atomicExch(&r.count[slot], 0);
+            __threadfence_block();
+            done[slot] = j;
+        }
+    }
+    __syncwarp();
+}
 
 // Descriptor of one load-reduction chunk, computed by k_chunk_desc (one
 // thread per chunk, so the lookups of many chunks overlap) into the chunk's
-// own partial row (6 doubles); the chunk's block reads it before it
-// overwrites the row with its sums.
+// own partial row (6 doubles); every thread of the chunk's block reads it
+// before the chunk's last warp overwrites the row with the sums.
 struct ChunkDesc {
     int64_t e0, e1;       // entry range
     int32_t p;            // particle
@@ -535,7 +591,7 @@ __device__ __forceinline__ uint32_t chunk_thread_sums(const ChunkDesc& dsc, cons
 template <typename I>
 __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_chunks(psc_geometry g, const I* imb,
                                                                                  double* part) {
-    __shared__ double s[LOAD_THREADS / 32][6];
+    __shared__ ChunkRing rows;
     __shared__ LoadRing<I> ring;
     extern __shared__ double s_al[];  // S^3 + 1 entries (dynamic)
     const int64_t C = g.totals[1];
@@ -543,10 +599,10 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
     const int S3 = g.subsamples * g.subsamples * g.subsamples;
     const double S3d = (double)S3;
     for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
-    __syncthreads();
-    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
-        // every thread reads the chunk's descriptor; the block sum below (its barriers) comes before
-        // thread 0 overwrites the row with the chunk's sums
+    chunk_ring_init(rows);  // (its barrier also publishes s_al)
+    long long j = 0;
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x, ++j) {  // every warp, in this order
+        // every thread reads the chunk's descriptor before the chunk's last warp overwrites the row
         const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         const bool list = g.load_w && g.load_abk && g.load_n;  // write the loads list too
@@ -554,11 +610,7 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
             dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum, imb, N, (uint32_t)g.ny, (uint32_t)g.nz, s_al,
             ring, acc, list ? g.load_w : nullptr, g.load_abk, chunk * g.chunk_entries + threadIdx.x);
         if (list) g.load_n[chunk * LOAD_THREADS + threadIdx.x] = (uint8_t)listed;
-        block_sum<6>(acc, s);
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
-        }
+        chunk_ring_finish(rows, j, acc, part + chunk * 6);
     }
 }
 
@@ -659,13 +711,14 @@ __device__ __forceinline__ void list_chunk_sums(const ListCursor& cur, int64_t s
     }
 }
 
-// A chunk's list entries overlap the previous chunk's block sum: each thread
-// issues the next chunk's first list copy as soon as its own sums are done (its
-// stage slots are free then), before the barrier.
+// A chunk's list entries overlap the previous chunk's sums: each thread issues
+// the next chunk's first list copy as soon as its own sums are done (its stage
+// slots are free then), before its warp's sum.
 template <typename I>
-__global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list(psc_geometry g, const I* imb, double* part) {
-    __shared__ double s[LOAD_THREADS / 32][6];
+__global__ void __launch_bounds__(LOAD_THREADS, 3) k_loads_chunks_list(psc_geometry g, const I* imb, double* part) {
+    __shared__ ChunkRing rows;
     extern __shared__ __align__(16) unsigned char list_stage[];
+    chunk_ring_init(rows);
     const int64_t C = g.totals[1];
     const uint32_t N = (uint32_t)g.nx * g.ny * g.nz;
     ListCursor cur{};
@@ -676,7 +729,7 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list(psc_geometry
         list_issue(chunk * g.chunk_entries + threadIdx.x, g.load_w, g.load_abk, 0, list_pass_size(cur.n_t, 0),
                    list_stage);
     }
-    for (; chunk < C; chunk += gridDim.x) {  // block-uniform
+    for (long long j = 0; chunk < C; chunk += gridDim.x, ++j) {  // every warp, in this order
         // the next chunk's descriptor (its row is overwritten only when this block reduces it) and counts
         const int64_t nxt = chunk + gridDim.x;
         ListCursor nc{};
@@ -690,11 +743,7 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list(psc_geometry
         if (nxt < C)
             list_issue(nxt * g.chunk_entries + threadIdx.x, g.load_w, g.load_abk, 0, list_pass_size(nc.n_t, 0),
                        list_stage);
-        block_sum<6>(acc, s);
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
-        }
+        chunk_ring_finish(rows, j, acc, part + chunk * 6);
         cur = nc;
     }
 }
@@ -799,16 +848,19 @@ __global__ void __launch_bounds__(256) k_chunk_desc_multi(const LoadsJob* jobs, 
 template <typename I>
 __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS)
     k_loads_chunks_multi(const LoadsJob* jobs, const int64_t* chunk_base, int njobs, double* part) {
-    __shared__ double s[LOAD_THREADS / 32][6];
+    __shared__ ChunkRing rows;
     __shared__ LoadRing<I> ring;
     extern __shared__ double s_al[];  // S^3 + 1 entries for the largest S of the jobs (dynamic)
+    chunk_ring_init(rows);
     const int64_t C = chunk_base[njobs];
-    int cur_S = 0;  // S of the table in s_al (block-uniform)
-    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {  // block-uniform
+    int cur_S = 0;  // S of the table in s_al (the same in every warp: all visit the same chunks)
+    long long j = 0;
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x, ++j) {  // every warp, in this order
         const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
         const psc_geometry& g = jobs[dsc.pad].g;
         const int S = g.subsamples;
-        if (S != cur_S) {  // block-uniform; the previous chunk's reads of s_al ended before its block sum
+        if (S != cur_S) {  // every warp at the same chunk: the barriers are block-uniform
+            __syncthreads();  // no warp reads the old table any more
             const int S3 = S * S * S;
             const double S3d = (double)S3;
             for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
@@ -823,21 +875,18 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS)
             (uint32_t)g.nx * g.ny * g.nz, (uint32_t)g.ny, (uint32_t)g.nz, s_al, ring, acc,
             list ? g.load_w : nullptr, g.load_abk, local * g.chunk_entries + threadIdx.x);
         if (list) g.load_n[local * LOAD_THREADS + threadIdx.x] = (uint8_t)listed;
-        block_sum<6>(acc, s);
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
-        }
+        chunk_ring_finish(rows, j, acc, part + chunk * 6);
     }
 }
 
 // The list path for many windows: every job's loads list is current.
 template <typename I>
-__global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list_multi(const LoadsJob* jobs,
-                                                                        const int64_t* chunk_base, int njobs,
-                                                                        double* part) {
-    __shared__ double s[LOAD_THREADS / 32][6];
+__global__ void __launch_bounds__(LOAD_THREADS, 3) k_loads_chunks_list_multi(const LoadsJob* jobs,
+                                                                           const int64_t* chunk_base, int njobs,
+                                                                           double* part) {
+    __shared__ ChunkRing rows;
     extern __shared__ __align__(16) unsigned char list_stage[];
+    chunk_ring_init(rows);
     const int64_t C = chunk_base[njobs];
     ListCursor cur{};
     int64_t chunk = blockIdx.x;
@@ -849,7 +898,7 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list_multi(const 
         list_issue(local0 * g0.chunk_entries + threadIdx.x, g0.load_w, g0.load_abk, 0, list_pass_size(cur.n_t, 0),
                    list_stage);
     }
-    for (; chunk < C; chunk += gridDim.x) {  // block-uniform
+    for (long long j = 0; chunk < C; chunk += gridDim.x, ++j) {  // every warp, in this order
         const int64_t nxt = chunk + gridDim.x;
         ListCursor nc{};
         if (nxt < C) {
@@ -862,16 +911,12 @@ __global__ void __launch_bounds__(LOAD_THREADS) k_loads_chunks_list_multi(const 
         list_chunk_sums<I>(cur, local * J.g.chunk_entries + threadIdx.x, J.g.particles, J.g.load_w, J.g.load_abk,
                            reinterpret_cast<const I*>(J.imb), (uint32_t)J.g.nx * J.g.ny * J.g.nz, (uint32_t)J.g.ny,
                            (uint32_t)J.g.nz, list_stage, acc);
-        if (nxt < C) {  // the next chunk's first list copy, overlapping this chunk's block sum
+        if (nxt < C) {  // the next chunk's first list copy, overlapping this chunk's warp sums
             const psc_geometry& gn = jobs[nc.dsc.pad].g;
             list_issue((nxt - chunk_base[nc.dsc.pad]) * gn.chunk_entries + threadIdx.x, gn.load_w, gn.load_abk, 0,
                        list_pass_size(nc.n_t, 0), list_stage);
         }
-        block_sum<6>(acc, s);
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) part[chunk * 6 + k] = acc[k];
-        }
+        chunk_ring_finish(rows, j, acc, part + chunk * 6);
         cur = nc;
     }
 }
@@ -1000,6 +1045,13 @@ cudaError_t launch_geometry_build(const psc_geometry& g, cudaStream_t stream) {
     }
     k_geometry_final<<<grid_cap(N, 256), 256, 0, stream>>>(g);
     return cudaGetLastError();
+}
+
+cudaError_t read_loads_status(int* out, bool clear) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, g_loads_status, sizeof(int));
+    if (e != cudaSuccess || !clear) return e;
+    const int zero = 0;
+    return cudaMemcpyToSymbol(g_loads_status, &zero, sizeof(int));
 }
 
 cudaError_t launch_solid_velocity(const psc_geometry& g, int us_type, void* us, cudaStream_t stream) {

@@ -38,6 +38,7 @@ cudaError_t launch_step_pair(int store, const psc_window* d_windows, int nwin, i
                              bool moving, int grid_ctas, cudaStream_t stream);
 cudaError_t read_device_status(int* out, bool clear);
 cudaError_t read_pair_status(int* out, bool clear);
+cudaError_t read_loads_status(int* out, bool clear);
 cudaError_t launch_reduce_windows(const psc_window* d_windows, int nwin, double* out, cudaStream_t stream);
 cudaError_t launch_init_equilibrium(int store, double scale, void* f, int64_t ncells, cudaStream_t stream);
 // inlet = {rho, ux, uy, uz} when open_x (PSC_WIN_OPEN_X faces), else unused

@@ -106,3 +106,50 @@ def test_rebuilt_geometry_drops_its_loads_list():
     assert np.array_equal(Fa, Fb) and np.array_equal(Ta, Tb)
     a.close()
     b.close()
+
+
+def _device_status():
+    import ctypes
+
+    from particuology_hydraulic_penalty_b200 import _native as nat
+
+    v = ctypes.c_int(0)
+    nat.call("psc_device_status", ctypes.byref(v), 1)
+    return v.value
+
+
+def test_chunk_rows_with_many_chunks_per_block():
+    """The load-chunk kernels write a chunk's row from the warp that finishes the chunk last, through
+    a ring of four partial-sum slots per block; a warp may run ahead of the others by up to four
+    chunks.  On the 24 windows of the benchmark batch (about 15 000 chunks for 2368 blocks) every
+    block reuses its slots, in the whole-box pass (first step) and in the list pass (second step).
+    Each window's forces and torques equal those of the window run alone, where a block holds far
+    fewer chunks, bit for bit, and no kernel gave up a wait."""
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+    from particuology_hydraulic_penalty_b200.handle import BatchHandle, SolverHandle, make_config
+
+    _device_status()
+    wins = wgen.batched_windows(24, seed0=0)
+    cfgs = [make_config((w.n,) * 3, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=4, store=nat.STORE_F32)
+            for w in wins]
+    b = BatchHandle(cfgs, graph_steps=0)
+    b.set_particles_all([w.particles for w in wins])
+    b.step(1, nat.RUN_DIAG)
+    whole = [b.loads(k) for k in range(len(wins))]
+    b.step(1, nat.RUN_DIAG)
+    listed = [b.loads(k) for k in range(len(wins))]
+    assert _device_status() == 0
+    for k in (0, 1, 5, 11, 17, 23):
+        s = SolverHandle(cfgs[k])
+        s.set_particles(wins[k].particles)
+        s.step(1, nat.RUN_DIAG)
+        F1, T1 = s.loads()
+        s.step(1, nat.RUN_DIAG)
+        F2, T2 = s.loads()
+        s.close()
+        assert np.abs(F1).sum() > 0.0
+        assert np.array_equal(whole[k][0], F1) and np.array_equal(whole[k][1], T1)
+        assert np.array_equal(listed[k][0], F2) and np.array_equal(listed[k][1], T2)
+    assert _device_status() == 0
+    b.close()
