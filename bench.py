@@ -533,11 +533,14 @@ def perm_error_steady(tol: float = 1.0e-8, check_every: int = 200, max_steps: in
                     "run to its own steady state"}
 
 
+STORE_BYTES = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}  # bytes per stored population
 WORKLOADS = {
     "batch24": "batch24: 24 uneven periodic pore windows, edges {{48,64,96,128,160}}, S=4, BGK tau=0.8, "
                "F=1e-6 x, {prec} deviation storage, one persistent launch per step, CUDA graph",
     "window96x3": "window96x3: one seeded 96^3 window in its three geometries (skeleton, passive fines, "
                   "preloaded fines), S=4, BGK tau=0.8, F=1e-6 x, {prec} deviation storage, one launch per step",
+    "batch8": "batch8: the first 8 windows of batch24 (a profiling case: about 1.3 GB on the device, fields "
+              "larger than the L2), {prec} deviation storage, one persistent launch per step, CUDA graph",
 }
 
 
@@ -546,6 +549,8 @@ def make_windows(workload: str, rank: int):
 
     if workload == "batch24":
         return wgen.batched_windows(NWIN, seed0=NWIN * rank)
+    if workload == "batch8":
+        return wgen.batched_windows(NWIN, seed0=NWIN * rank)[:8]
     seed = 1000 + rank
     return [wgen.make_window(96, kind, seed) for kind in wgen.GEOMETRY_TYPES]
 
@@ -608,7 +613,8 @@ def run_ours(args):
         "data": "synthetic (seeded FCC skeleton / passive / preloaded pore windows; the reference's dumps are not shipped)",
         "config": {"workload": WORKLOADS[args.workload].format(prec=args.precision.upper()),
                    "windows_per_gpu": len(wins), "cells_per_gpu": cells_rank,
-                   "l2": "inputs (~5 GB/GPU) exceed the 126 MB L2; no flush", "parallelism": f"window-parallel x{world}",
+                   "l2": f"populations (~{2 * 19 * cells_rank * STORE_BYTES[args.precision] / 1e9:.1f} GB/GPU, two "
+                         f"buffers) exceed the 126 MB L2; no flush", "parallelism": f"window-parallel x{world}",
                    "graph_steps": args.graph_steps, "launch": batch.launch_config(),
                    "autotuned": tuned is not None,
                    "autotune": None if tuned is None else {
