@@ -560,12 +560,21 @@ const char* psc_batch_last_error(const psc_batch* b);
 int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, int nparticles);
 /* psc_batch_set_particles for every window in one call: h_particles[k] is window k's [P_k][10]
  * array (may be NULL when nparticles[k] is 0).  All windows are staged in one host buffer and
- * uploaded with one copy.  Every window is checked before any takes its new state: if one is
- * rejected (NaN / Inf, null array) the call returns the error and every window keeps its
- * previous state. */
+ * uploaded with one copy on the batch's own upload stream, beside the step kernels (they do not
+ * read particles); whatever does read them waits for the copy.  Every window is checked before
+ * any takes its new state: if one is rejected (NaN / Inf, null array) the call returns the error
+ * and every window keeps its previous state. */
 int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, const int* h_nparticles);
 /* nsteps steps of every active window.  PSC_RUN_DIAG: diagnostics and loads
- * of every window at the final step into h_status[nwin] (may be NULL). */
+ * of every window at the final step into h_status[nwin] (may be NULL).
+ * The post-stream sums of a PSC_RUN_DIAG call are the moment sums of the next
+ * step's pull.  With the pair kernel, without PSC_RUN_FIELDS and with the step
+ * inputs (geometry, solid velocity, descriptors, frozen set) unchanged since
+ * the previous PSC_RUN_DIAG call, the call runs that next step (into the other
+ * population buffer and a second IMB field per window; the current state is
+ * untouched) instead of a reduction-only pass, and the next call takes it as
+ * its first step if the inputs are still the same.  Results are the same bits
+ * either way. */
 int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_status);
 /* Step until every window's Darcy permeability changes by less than tol per
  * step, checked on a pair of consecutive steps every check_every steps; a

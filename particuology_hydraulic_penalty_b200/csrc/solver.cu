@@ -1395,6 +1395,7 @@ struct psc_batch {
     cudaEvent_t up_ready = nullptr;
     cudaEvent_t up_done = nullptr;
     bool up_pending = false;
+    std::vector<int64_t> staged;  // per window: offset of its accepted state in up_host, or -1
     // particle loads of all active windows in one launch sequence: job table
     // [LoadsJob x n][chunk bases n+1][particle bases n+1], as last uploaded
     // one table per buffer parity (a job names the IMB field of its window's current buffer)
@@ -1727,6 +1728,7 @@ int psc_batch_create(const psc_config* h_cfgs, int nwin, const psc_launch* h_lau
         if (st == PSC_OK) st = window_set_particles(*b->w.back(), nullptr, 0, b->stream, "psc_batch_create");
     }
     b->frozen.assign((size_t)nwin, -1);
+    b->staged.assign((size_t)nwin, -1);
     b->frozen_red.assign((size_t)nwin * PSC_NRED, 0.0);
     b->last.assign((size_t)nwin, psc_diag{});
     b->have_diag.assign((size_t)nwin, 0);
@@ -1769,6 +1771,7 @@ int psc_batch_set_particles(psc_batch* b, int win, const double* h_particles, in
     ErrorCapture errors_(b->last_error);
     DeviceScope ds(b->device);
     PSC_TRY(batch_upload_join(*b, "psc_batch_set_particles"));
+    b->staged[(size_t)win] = -1;  // the staging buffer no longer holds its accepted state
     return window_set_particles(*b->w[(size_t)win], h_particles, nparticles, b->stream, "psc_batch_set_particles");
 }
 
@@ -1786,7 +1789,13 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
     // one staging buffer and one host-to-device copy for all windows
     PSC_CUDA(cudaEventSynchronize(b->up_done), who);  // the previous upload has left the staging buffer
     const int64_t cap = b->up_dev.n < total ? total + total / 4 + 64 : b->up_dev.n;
+    const double* const host_before = b->up_host.p;
     PSC_CUDA(b->up_host.ensure(cap), who);
+    // where the staging buffer still holds a window's accepted state (the previous call's copy);
+    // unknown from here until this call succeeds
+    std::vector<int64_t> staged(nwin, -1);
+    if (b->up_host.p == host_before) staged.swap(b->staged);
+    b->staged.assign(nwin, -1);
     // pass 1: stage every window (an unchanged state is found in the same pass) and validate the
     // changed ones; one rejected window leaves every window as it was
     std::vector<int> known(nwin, 0);
@@ -1798,14 +1807,22 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
     }
     // window k: copy into the staging buffer, note whether it equals the accepted state, check a
     // changed one for NaN / Inf (known[k] = 1 same, 2 changed and finite, -1 non-finite)
+    // (where the buffer holds the accepted state at the same place, a read-only comparison: an
+    // unchanged state is not written again)
     auto stage = [&](int k) {
         const Window& w = *b->w[(size_t)k];
         const int P = h_nparticles[k];
         const size_t n10 = (size_t)P * 10;
         double* dst = b->up_host.p + offs[(size_t)k];
         bool same = P == 0 && w.P == 0 && w.hp.empty();  // (empty before and now)
-        if (P > 0 && P == w.P && w.hp.size() == n10) same = copy_same(dst, h_particles[k], w.hp.data(), n10);
-        else if (P > 0) std::memcpy(dst, h_particles[k], n10 * sizeof(double));
+        if (P > 0 && P == w.P && w.hp.size() == n10 && staged[(size_t)k] == offs[(size_t)k]) {
+            same = std::memcmp(dst, h_particles[k], n10 * sizeof(double)) == 0;
+            if (!same) std::memcpy(dst, h_particles[k], n10 * sizeof(double));
+        } else if (P > 0 && P == w.P && w.hp.size() == n10) {
+            same = copy_same(dst, h_particles[k], w.hp.data(), n10);
+        } else if (P > 0) {
+            std::memcpy(dst, h_particles[k], n10 * sizeof(double));
+        }
         known[(size_t)k] = same ? 1 : (particles_finite(h_particles[k], n10) ? 2 : -1);
     };
     for (size_t k = 0; k < nwin; ++k) stage((int)k);
@@ -1840,6 +1857,7 @@ int psc_batch_set_particles_all(psc_batch* b, const double* const* h_particles, 
                  who);
     PSC_CUDA(cudaEventRecord(b->up_done, b->up_stream), who);
     b->up_pending = true;
+    b->staged.assign(offs.begin(), offs.end() - 1);
     return PSC_OK;
 }
 
