@@ -615,8 +615,8 @@ double* diag_dev(Window& w) { return w.out.p + 2 * PSC_NRED; }
 
 int window_loads(Window& w, cudaStream_t s) {
     psc_geometry g = w.geometry();
-    PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
-                               w.forces.p, w.torques.p, diag_dev(w), s));
+    PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb_for(w.imb_par), w.chunk_partials.p,
+                               red_pre(w) + PSC_RED_IMBX, w.forces.p, w.torques.p, diag_dev(w), s));
     w.loads_enqueued();
     w.loads_ready = true;
     return PSC_OK;
@@ -830,9 +830,21 @@ struct psc_solver {
     // collide_stream_psc() call) as a CUDA graph per buffer parity, keyed by
     // every pointer, size and version its launches capture: captured on the
     // second call with an unchanged key, replayed while the key holds.
-    cudaGraphExec_t report_graph[2] = {nullptr, nullptr};
-    std::vector<unsigned char> report_key[2];   // key of report_graph[parity]
-    std::vector<unsigned char> report_seen[2];  // key of the last eager run of that parity
+    // One graph per buffer parity and kind of call (kReportAhead: the next step is run ahead;
+    // kReportCommit: this call's step was run ahead by the previous call).
+    cudaGraphExec_t report_graph[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
+    std::vector<unsigned char> report_key[2][4];   // key of report_graph[parity][kind]
+    std::vector<unsigned char> report_seen[2][4];  // key of the last eager run of that parity and kind
+    // The step run ahead: the post-stream sums of a reporting call are the moment sums of the next
+    // step's pull (the same per-cell arithmetic and tile rows in every kernel), so when the step
+    // inputs are those of the previous reporting call, the call runs the next step into the other
+    // buffer and IMB field instead of a reduction-only pass; the next reporting call takes it as
+    // its step when its inputs are still the same.  Every other call that steps or sets the state
+    // drops it (the current state is untouched by it).
+    DArray<double> ahead_red;             // reductions of the step run ahead
+    bool ahead_ready = false;
+    std::vector<uint64_t> ahead_inputs;   // step inputs it ran with
+    std::vector<uint64_t> report_inputs;  // step inputs of the last reporting call
     // device-side convergence (psc_converge): criterion state [kConvState] + reductions snapshot,
     // and two pinned status slots the host polls
     DArray<double> conv;
@@ -840,8 +852,9 @@ struct psc_solver {
     cudaEvent_t conv_ev[2] = {nullptr, nullptr};
 
     ~psc_solver() {
-        for (auto& g : report_graph)
-            if (g) cudaGraphExecDestroy(g);
+        for (auto& row : report_graph)
+            for (auto& g : row)
+                if (g) cudaGraphExecDestroy(g);
         for (auto& e : conv_ev)
             if (e) cudaEventDestroy(e);
     }
@@ -926,6 +939,7 @@ int solver_collide(psc_solver& h, bool imb) {
     }
     PSC_TRY(launch_solo(w, flags, s));
     w.cur ^= 1;
+    if (imb) w.imb_par = w.cur;
     w.stepped = true;
     w.moments_ready = false;
     w.loads_ready = false;
@@ -934,29 +948,35 @@ int solver_collide(psc_solver& h, bool imb) {
     return PSC_OK;
 }
 
+constexpr int kReportAhead = 1;   // the call runs the next step ahead (instead of a reduction pass)
+constexpr int kReportCommit = 2;  // the call's step was run ahead by the previous reporting call
+
 // Everything the launches of one reporting step from buffer parity `par`
 // capture: a graph recorded under one key replays correctly under the same key.
-std::vector<unsigned char> report_key(const psc_solver& h, int par) {
+std::vector<unsigned char> report_key(const psc_solver& h, int par, int kind) {
     const Window& w = h.w;
     struct Key {
         psc_geometry g;
         const void* desc[2];
-        const void* imb;
+        const void* imb[2];
         const void* out;
+        const void* ahead;
         const void* host;
         const void* chunks;
         const void* forces;
         const void* torques;
         uint64_t desc_version;
         int64_t tiles;
-        int32_t kernel, store, moving, par, field_type, pad;
+        int32_t kernel, store, moving, par, field_type, kind;
     } k;
     std::memset(&k, 0, sizeof(k));  // padding too: keys compare bytewise
     k.g = w.geometry();
     k.desc[0] = w.solo[0].p;
     k.desc[1] = w.solo[1].p;
-    k.imb = w.imb.p;
+    k.imb[0] = w.imb_for(0);
+    k.imb[1] = w.imb_for(1);
     k.out = w.out.p;
+    k.ahead = h.ahead_red.p;
     k.host = h.host_out.p;
     k.chunks = w.chunk_partials.p;
     k.forces = w.forces.p;
@@ -968,28 +988,51 @@ std::vector<unsigned char> report_key(const psc_solver& h, int par) {
     k.moving = w.moving ? 1 : 0;
     k.par = par;
     k.field_type = w.field_type();
+    k.kind = kind;
     const unsigned char* b = reinterpret_cast<const unsigned char*>(&k);
     return std::vector<unsigned char>(b, b + sizeof(k));
 }
 
+// Everything a step reads besides the populations.
+std::vector<uint64_t> solver_step_inputs(const psc_solver& h) {
+    const Window& w = h.w;
+    return {w.built_version, w.moving ? w.us_version : 0, w.desc_version, (uint64_t)(w.moving ? 1 : 0),
+            (uint64_t)w.solo_kernel, (uint64_t)w.solo_tiles};
+}
+
 // The GPU work of one reporting step from buffer parity `par` (the launches of
 // solver_collide(imb) + solver_report(loads, post) without their host-side
-// bookkeeping), ending with the read-back into host_out.
-int report_step_work(psc_solver& h, int par) {
+// bookkeeping), ending with the read-back into host_out.  kReportCommit: the
+// step from `par` is in place already (buffer par ^ 1, its IMB field and its
+// reductions in ahead_red).  kReportAhead: the post-stream sums come from the
+// next step, run from par ^ 1 into buffer par and IMB field par.
+int report_step_work(psc_solver& h, int par, int kind) {
     Window& w = h.w;
     cudaStream_t s = h.stream;
     const unsigned mv = w.moving ? PSC_STEP_MOVING : 0u;
     const psc_launch c = {0, 1, w.solo_kernel, 0, 0};
-    PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par].p, 1, w.solo_tiles,
-                                PSC_STEP_COLLIDE | PSC_STEP_IMB | PSC_STEP_REDUCE | mv, &c, s));
-    PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_pre(w), s));
+    const unsigned full = PSC_STEP_COLLIDE | PSC_STEP_IMB | PSC_STEP_REDUCE | mv;
+    if (kind & kReportCommit) {
+        PSC_CUDA(cudaMemcpyAsync(red_pre(w), h.ahead_red.p, PSC_NRED * sizeof(double), cudaMemcpyDeviceToDevice, s),
+                 "psc_step");
+    } else {
+        PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par].p, 1, w.solo_tiles, full, &c, s));
+        PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_pre(w), s));
+    }
     PSC_CUDA(h.lanes.begin(s), "psc_step");
     psc_geometry g = w.geometry();
-    PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb.p, w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
+    PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb_for(par ^ 1), w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
                                w.forces.p, w.torques.p, diag_dev(w), h.lanes.lane(0)));
     w.loads_enqueued();
-    PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par ^ 1].p, 1, w.solo_tiles, PSC_STEP_REDUCE | mv, &c, s));
-    PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_post(w), s));
+    if (kind & kReportAhead) {
+        PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par ^ 1].p, 1, w.solo_tiles, full, &c, s));
+        PSC_TRY(psc_reduce_windows(w.solo[par].p, 1, h.ahead_red.p, s));
+        PSC_CUDA(cudaMemcpyAsync(red_post(w), h.ahead_red.p, PSC_NRED * sizeof(double), cudaMemcpyDeviceToDevice, s),
+                 "psc_step");
+    } else {
+        PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par ^ 1].p, 1, w.solo_tiles, PSC_STEP_REDUCE | mv, &c, s));
+        PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_post(w), s));
+    }
     PSC_CUDA(h.lanes.end(s), "psc_step");
     PSC_CUDA(cudaMemcpyAsync(h.host_out.p, w.out.p, kOutLen * sizeof(double), cudaMemcpyDeviceToHost, s), "psc_step");
     return PSC_OK;
@@ -997,7 +1040,7 @@ int report_step_work(psc_solver& h, int par) {
 
 // One collide_stream_psc() step with its loads and diagnostics (the work of
 // solver_collide(imb) + solver_report(loads)), replayed from a CUDA graph
-// when nothing it captures has changed since the previous call.
+// when nothing it captures has changed since the previous call of its kind.
 int solver_report_step(psc_solver& h) {
     Window& w = h.w;
     cudaStream_t s = h.stream;
@@ -1005,46 +1048,61 @@ int solver_report_step(psc_solver& h) {
     PSC_TRY(window_ensure_imb(w, s));
     PSC_TRY(window_upload_solo(w, s));
     PSC_CUDA(h.host_out.ensure(kOutLen), "psc_step");
+    PSC_CUDA(h.ahead_red.ensure(PSC_NRED, true, s), "psc_step");
+    const std::vector<uint64_t> inputs = solver_step_inputs(h);
+    int kind = 0;
+    if (h.ahead_ready && inputs == h.ahead_inputs) kind |= kReportCommit;
+    if (inputs == h.report_inputs) kind |= kReportAhead;
+    h.ahead_ready = false;
     const int par = w.cur;
-    std::vector<unsigned char> key = report_key(h, par);
+    std::vector<unsigned char> key = report_key(h, par, kind);
+    cudaGraphExec_t& graph = h.report_graph[par][kind];
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     PSC_CUDA(cudaStreamIsCapturing(s, &cap), "psc_step");
     if (cap != cudaStreamCaptureStatusNone) {
-        PSC_TRY(report_step_work(h, par));  // the caller records this step into its own graph
-    } else if (h.report_graph[par] && key == h.report_key[par]) {
-        PSC_CUDA(cudaGraphLaunch(h.report_graph[par], s), "psc_step");
-    } else if (key == h.report_seen[par]) {
-        // the same launches as the previous call of this parity: record them once, then replay
-        if (h.report_graph[par]) {
-            cudaGraphExecDestroy(h.report_graph[par]);
-            h.report_graph[par] = nullptr;
-            h.report_key[par].clear();
+        kind = 0;  // the caller records this step into its own graph: no step run ahead
+        PSC_TRY(report_step_work(h, par, kind));
+    } else if (graph && key == h.report_key[par][kind]) {
+        PSC_CUDA(cudaGraphLaunch(graph, s), "psc_step");
+    } else if (key == h.report_seen[par][kind]) {
+        // the same launches as the previous call of this parity and kind: record them once, then replay
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+            h.report_key[par][kind].clear();
         }
         PSC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "psc_step");
-        const int st = report_step_work(h, par);
-        cudaGraph_t graph = nullptr;
-        const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+        const int st = report_step_work(h, par, kind);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s, &g);
         if (st != PSC_OK) {
-            if (graph) cudaGraphDestroy(graph);
+            if (g) cudaGraphDestroy(g);
             return st;
         }
         if (ec != cudaSuccess) return cuda_fail(ec, "psc_step: capturing the reporting step");
         cudaGraphExec_t exec = nullptr;
-        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
-        cudaGraphDestroy(graph);
+        const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
         if (ei != cudaSuccess) return cuda_fail(ei, "psc_step: instantiating the reporting step");
-        h.report_graph[par] = exec;
-        h.report_key[par] = key;
+        graph = exec;
+        h.report_key[par][kind] = key;
         PSC_CUDA(cudaGraphLaunch(exec, s), "psc_step");
     } else {
-        PSC_TRY(report_step_work(h, par));
-        h.report_seen[par] = std::move(key);
+        PSC_TRY(report_step_work(h, par, kind));
+        h.report_seen[par][kind] = std::move(key);
     }
     w.cur ^= 1;
+    w.imb_par = w.cur;
     w.stepped = true;
     w.moments_ready = false;
     w.loads_ready = true;
     PSC_CUDA(cudaStreamSynchronize(s), "psc_step");
+    if (kind & kReportAhead) {  // the step run ahead added its own IMB; a reduction pass adds none
+        for (int q = PSC_RED_IMBX; q <= PSC_RED_IMBZ; ++q) h.host_out.p[PSC_NRED + q] = 0.0;
+        h.ahead_ready = true;
+        h.ahead_inputs = inputs;
+    }
+    h.report_inputs = inputs;
     fill_diag(w, h.host_out.p, w.last);
     w.diag_ready = true;
     return PSC_OK;
@@ -1118,6 +1176,7 @@ int solver_converge(psc_solver& h, int nsteps, double tol, int min_steps, int ch
     st.steps_done = done;
     st.residual = cs[4];
     w.cur = start ^ (done & 1);
+    w.imb_par = w.cur;  // the last step that ran wrote its IMB field (a check step)
     w.stepped = true;
     w.moments_ready = false;
     w.loads_ready = false;
@@ -1154,6 +1213,7 @@ int psc_create(const psc_config* h_cfg, psc_solver** out) {
         PSC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "psc_create");
         h->own_stream = true;
     }
+    h->w.imb_dual = true;  // a reporting call may run the next step ahead (solver_report_step)
     int st = window_init(h->w, *h_cfg, h->stream, "psc_create");
     if (st == PSC_OK) {
         cudaError_t e = h->lanes.init(1);
@@ -1222,6 +1282,7 @@ int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status) {
         if (h_status) *h_status = st;
         return PSC_OK;
     }
+    if (nsteps > 0) h->ahead_ready = false;  // these steps overwrite the other buffer
     if (converge && nsteps > 0) {
         PSC_TRY(solver_converge(*h, nsteps, tol, min_steps, std::max(1, w.cfg.conv_check_every), fields, st));
         if (h_status) *h_status = st;
@@ -1250,6 +1311,7 @@ int psc_converge(psc_solver* h, int max_steps, double tol, int min_steps, int ch
     if (ds.err != cudaSuccess) return cuda_fail(ds.err, "psc_converge: cudaSetDevice");
     psc_status st{};
     st.residual = INFINITY;
+    h->ahead_ready = false;
     PSC_TRY(window_prepare(h->w, h->stream, h->tot, "psc_converge"));
     PSC_TRY(solver_converge(*h, max_steps, tol, std::max(1, min_steps), check_every, (flags & PSC_RUN_FIELDS) != 0,
                             st));
@@ -1268,6 +1330,7 @@ int psc_set_populations(psc_solver* h, const double* h_f) {
     if (!h) return fail(PSC_E_INVALID, "psc_set_populations: null handle");
     ErrorCapture errors_(h->last_error);
     DeviceScope ds(h->device);
+    h->ahead_ready = false;  // the state changes
     return window_set_populations(h->w, h_f, h->stream, "psc_set_populations");
 }
 

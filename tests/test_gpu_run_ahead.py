@@ -11,7 +11,10 @@ windows, one stepped with PSC_RUN_DIAG and one with PSC_RUN_DIAG |
 PSC_RUN_FIELDS, must report the same diagnostics, loads, populations and IMB
 fields bit for bit, through every way a call can use or drop the step run
 ahead: repeated reporting calls, moved particles (a rebuilt geometry), plain
-steps after a reporting call, and a convergence loop.
+steps after a reporting call, and a convergence loop.  The single-window
+handle (one psc_step(h, 1, PSC_RUN_DIAG) per collide_stream_psc() call) does
+the same in every kernel it runs: the exact FP64 kernel, the FP32 pair kernel
+and the one-cell kernel.
 """
 
 import numpy as np
@@ -123,3 +126,79 @@ def test_plain_steps_and_convergence_after_a_step_run_ahead():
     _same(nat, ahead, plain, len(wins))
     ahead.close()
     plain.close()
+
+
+# ---- single-window handle (the drop-in's collide_stream_psc() calls) -------------------------
+
+def _solo_pair(store_name, n, static=True):
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+    from particuology_hydraulic_penalty_b200.handle import SolverHandle, make_config
+
+    w = wgen.make_window(n, "preloaded", 11)
+    cfg = make_config((n,) * 3, tau=0.8, force=(1e-6, 0.0, 0.0), subsamples=4, store=getattr(nat, store_name),
+                      static_geometry=static)
+    a, b = SolverHandle(cfg), SolverHandle(cfg)
+    return nat, w, a, b
+
+
+def _solo_same(nat, a, b):
+    assert np.array_equal(_diag_tuple(a.step_diag), _diag_tuple(b.step_diag), equal_nan=True)
+    Fa, Ta = a.loads()
+    Fb, Tb = b.loads()
+    assert np.abs(Fa).sum() > 0.0
+    assert np.array_equal(Fa, Fb) and np.array_equal(Ta, Tb)
+
+
+def _solo_report(nat, h, particles, fields):
+    h.set_particles(particles)
+    h.step_diag = h.step(1, nat.RUN_DIAG | (nat.RUN_FIELDS if fields else 0)).diag
+
+
+@pytest.mark.parametrize("store_name,n", [("STORE_F64_EXACT", 24), ("STORE_F32", 32), ("STORE_F32", 27)])
+def test_solver_reporting_calls_run_ahead_equal_reduction_pass(store_name, n):
+    """FP64-exact (its own kernel), FP32 pair kernel (even nz) and FP32 one-cell kernel (odd nz)."""
+    nat, w, a, b = _solo_pair(store_name, n)
+    for _ in range(6):  # eager, captured and replayed calls of every kind
+        _solo_report(nat, a, w.particles, False)
+        _solo_report(nat, b, w.particles, True)
+        _solo_same(nat, a, b)
+    for which in (nat.FIELD_F, nat.FIELD_IMB_X, nat.FIELD_IMB_Z, nat.FIELD_UZ):
+        assert np.array_equal(a.field(which), b.field(which))
+    # a loads call on the current IMB field repeats the reporting call's loads
+    Fa, Ta = a.loads()
+    a.accumulate_loads()
+    Fc, Tc = a.loads()
+    assert np.array_equal(Fa, Fc) and np.array_equal(Ta, Tc)
+    a.close()
+    b.close()
+
+
+def test_solver_run_ahead_dropped_by_other_calls():
+    nat, w, a, b = _solo_pair("STORE_F32", 32, static=False)
+    for _ in range(3):
+        _solo_report(nat, a, w.particles, False)
+        _solo_report(nat, b, w.particles, True)
+    moved = w.particles.copy()
+    moved[:, 2] += 0.29  # a rebuilt geometry
+    for _ in range(3):
+        _solo_report(nat, a, moved, False)
+        _solo_report(nat, b, moved, True)
+        _solo_same(nat, a, b)
+    for h in (a, b):
+        h.step(3)  # plain steps overwrite the other buffer
+    _solo_report(nat, a, moved, False)
+    _solo_report(nat, b, moved, True)
+    _solo_same(nat, a, b)
+    _solo_report(nat, a, moved, False)
+    _solo_report(nat, b, moved, True)
+    f = a.field(nat.FIELD_F)
+    for h in (a, b):
+        h.set_populations(f)  # a new state
+    for _ in range(2):
+        _solo_report(nat, a, moved, False)
+        _solo_report(nat, b, moved, True)
+        _solo_same(nat, a, b)
+    assert np.array_equal(a.field(nat.FIELD_F), b.field(nat.FIELD_F))
+    a.close()
+    b.close()
