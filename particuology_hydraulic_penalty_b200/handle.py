@@ -171,6 +171,9 @@ class BatchHandle:
                  int(graph_steps), ctypes.byref(self._h))
         self._status = (nat.PscStatus * self.nwin)()
         self.P = [0] * self.nwin
+        # pointer and count arrays of the last set_particles_all, kept while the caller passes the
+        # same float64 C-contiguous array objects (their buffers cannot move while referenced here)
+        self._staged = None
 
     def close(self) -> None:
         if self._h is not None and self._h.value:
@@ -190,14 +193,21 @@ class BatchHandle:
         self.P[k] = int(arr.shape[0])
 
     def set_particles_all(self, arrays) -> None:
-        """Every window's (P_k, 10) particle array in one call."""
-        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrays]
-        if len(arrs) != self.nwin:
-            raise ValueError(f"expected {self.nwin} particle arrays")
-        ptrs = (_VP * self.nwin)(*[_addr(a) if a.size else None for a in arrs])
-        counts = (ctypes.c_int * self.nwin)(*[int(a.shape[0]) for a in arrs])
+        """Every window's (P_k, 10) particle array in one call (the contents are read every call)."""
+        arrays = list(arrays)
+        st = self._staged
+        if st is not None and len(arrays) == len(st[0]) and all(a is b for a, b in zip(arrays, st[0])):
+            ptrs, counts = st[1], st[2]
+        else:
+            arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrays]
+            if len(arrs) != self.nwin:
+                raise ValueError(f"expected {self.nwin} particle arrays")
+            ptrs = (_VP * self.nwin)(*[_addr(a) if a.size else None for a in arrs])
+            counts = (ctypes.c_int * self.nwin)(*[int(a.shape[0]) for a in arrs])
+            # reuse only when the caller's own arrays were passed on (no converted copies)
+            self._staged = (arrs, ptrs, counts) if all(a is b for a, b in zip(arrays, arrs)) else None
         nat.check(self._lib.psc_batch_set_particles_all(self._h, ptrs, counts), "psc_batch_set_particles_all")
-        self.P = [int(a.shape[0]) for a in arrs]
+        self.P = [int(c) for c in counts]
 
     def step(self, nsteps: int, flags: int = 0):
         nat.check(self._lib.psc_batch_step(self._h, int(nsteps), int(flags), self._status), "psc_batch_step")
