@@ -438,10 +438,12 @@ def run_e2e_dropin(windows, steps: int):
                    "static geometry", "steps": steps}
 
 
-def run_e2e_batch(windows, steps: int, graph_steps: int):
+def run_e2e_batch(windows, steps: int, graph_steps: int, world: int = 1):
     """MLUPS through the batched C ABI with host buffers: every step uploads each window's particle
     array (psc_batch_set_particles_all) and reads back every window's diagnostics (psc_batch_step with
-    PSC_RUN_DIAG: particle loads, post-stream reductions, Darcy K)."""
+    PSC_RUN_DIAG: particle loads, post-stream reductions, Darcy K).  With several ranks each rank runs
+    its own batch; the ranks start the timed loop together (barrier) and the job's rate is all ranks'
+    cells over the slowest rank's wall time; the copied bytes are summed over the ranks."""
     import torch
 
     from particuology_hydraulic_penalty_b200 import _native as nat
@@ -460,17 +462,21 @@ def run_e2e_batch(windows, steps: int, graph_steps: int):
         b.set_particles_all(arrays)
         b.step(1, nat.RUN_DIAG)
     k_sum = 0.0
+    barrier(world)
     t0 = time.perf_counter()
     for _ in range(steps):
         b.set_particles_all(arrays)
         st = b.step(1, nat.RUN_DIAG)
         k_sum += st[0].diag.permeability
-    wall = time.perf_counter() - t0
-    cells = sum(w.n ** 3 for w in windows)
+    wall = max_over_ranks(time.perf_counter() - t0, world)
+    cells = sum_over_ranks(float(sum(w.n ** 3 for w in windows)), world)
+    h2d = int(sum_over_ranks(float(h2d), world))
+    d2h = int(sum_over_ranks(float(d2h), world))
+    finite = sum_over_ranks(0.0 if np.isfinite(k_sum) else 1.0, world) == 0.0
     b.close()
     torch.cuda.empty_cache()
     return {"value": round(cells * steps / wall / 1e6, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "finite": bool(np.isfinite(k_sum)),
+            "d2h_bytes_per_step": d2h, "finite": bool(finite), "ranks": world,
             "api": "C ABI psc_batch_set_particles_all (every window) + psc_batch_step(1, PSC_RUN_DIAG) per step: "
                    "host particle arrays in, per-window diagnostics and Darcy K out, one persistent launch for "
                    "all windows", "steps": steps}
@@ -661,10 +667,11 @@ def run_ours(args):
             out["perm_error"] = {"bound": 1e-4, "batch_equal_steps": acc_equal, "steady_state": acc_steady,
                                  "within_bound": bool(acc_equal["max"] <= 1e-4 and
                                                       (acc_steady is None or acc_steady["max"] <= 1e-4))}
-    if rank == 0 and world == 1 and not args.no_e2e:
-        out["e2e"] = run_e2e_batch(wins, steps=args.e2e_steps, graph_steps=args.graph_steps)
-        out["e2e_dropin"] = run_e2e_dropin(wins, steps=max(3, args.e2e_steps // 4))
-    elif rank == 0:
+    if not args.no_e2e:  # every rank: its own batch through the C ABI, timed together
+        out["e2e"] = run_e2e_batch(wins, steps=args.e2e_steps, graph_steps=args.graph_steps, world=world)
+        if world == 1:
+            out["e2e_dropin"] = run_e2e_dropin(wins, steps=max(3, args.e2e_steps // 4))
+    else:
         out["e2e"] = None
     if cpu is not None:
         out["cpu_baseline"] = {"value": round(cpu["value"], 4), "unit": UNIT, "cores": cpu["cores"], "kind": "port",

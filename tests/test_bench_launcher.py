@@ -69,3 +69,58 @@ def test_bench_gpus2_reference_arm_spawns_ranks():
     out = json.loads(lines[0])
     assert out["impl"] == "reference" and out["value"] > 0.0
     assert out["e2e"]["h2d_bytes_per_step"] == 0
+
+
+# one rank of the end-to-end leg: the batch handle replaced by a stand-in (no GPU)
+E2E_STUB = textwrap.dedent("""
+    import json, sys, types
+    import numpy as np
+    sys.path.insert(0, {root!r})
+    import bench
+    from particuology_hydraulic_penalty_b200 import handle
+
+    class FakeBatch:
+        calls = 0
+        def __init__(self, cfgs, graph_steps=0):
+            self.n = len(cfgs)
+        def set_particles(self, k, arr):
+            pass
+        def set_particles_all(self, arrays):
+            assert len(arrays) == self.n
+        def step(self, nsteps, flags=0):
+            FakeBatch.calls += 1
+            d = types.SimpleNamespace(permeability=1.0)
+            return [types.SimpleNamespace(diag=d)]
+        def close(self):
+            pass
+
+    handle.BatchHandle = FakeBatch
+    world, rank, local = bench.dist_setup(backend="gloo")
+    wins = [types.SimpleNamespace(n=8 + 8 * rank, particles=np.zeros((3 + rank, 10)))]
+    out = bench.run_e2e_batch(wins, steps=4, graph_steps=0, world=world)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    import torch.distributed as dist
+    dist.barrier()
+    dist.destroy_process_group()
+""")
+
+
+def test_e2e_leg_runs_on_every_rank():
+    """Each rank runs its own batch through the (stand-in) C ABI; cells and copied bytes add up over
+    the ranks and the rate uses the slowest rank's wall time."""
+    stub = E2E_STUB.format(root=str(ROOT))
+    driver = textwrap.dedent(f"""
+        import sys
+        sys.path.insert(0, {str(ROOT)!r})
+        import bench
+        sys.exit(bench.spawn_ranks(2, [sys.executable, "-c", {stub!r}], timeout_s=120))
+    """)
+    p = subprocess.run([sys.executable, "-c", driver], capture_output=True, text=True, timeout=180)
+    assert p.returncode == 0, p.stderr
+    lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1, p.stdout
+    out = json.loads(lines[0])
+    assert out["ranks"] == 2 and out["finite"] is True
+    assert out["h2d_bytes_per_step"] == (3 + 4) * 10 * 8
+    assert out["value"] > 0.0
