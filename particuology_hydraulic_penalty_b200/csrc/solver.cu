@@ -1019,11 +1019,7 @@ int report_step_work(psc_solver& h, int par, int kind) {
         PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par].p, 1, w.solo_tiles, full, &c, s));
         PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_pre(w), s));
     }
-    PSC_CUDA(h.lanes.begin(s), "psc_step");
-    psc_geometry g = w.geometry();
-    PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb_for(par ^ 1), w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
-                               w.forces.p, w.torques.p, diag_dev(w), h.lanes.lane(0)));
-    w.loads_enqueued();
+    PSC_CUDA(h.lanes.begin(s), "psc_step");  // the loads on a lane; the main stream's kernel first
     if (kind & kReportAhead) {
         PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par ^ 1].p, 1, w.solo_tiles, full, &c, s));
         PSC_TRY(psc_reduce_windows(w.solo[par].p, 1, h.ahead_red.p, s));
@@ -1033,6 +1029,10 @@ int report_step_work(psc_solver& h, int par, int kind) {
         PSC_TRY(psc_step_windows_ex(w.cfg.store, w.solo[par ^ 1].p, 1, w.solo_tiles, PSC_STEP_REDUCE | mv, &c, s));
         PSC_TRY(psc_reduce_windows(w.solo[par ^ 1].p, 1, red_post(w), s));
     }
+    psc_geometry g = w.geometry();
+    PSC_TRY(psc_particle_loads(&g, w.field_type(), w.imb_for(par ^ 1), w.chunk_partials.p, red_pre(w) + PSC_RED_IMBX,
+                               w.forces.p, w.torques.p, diag_dev(w), h.lanes.lane(0)));
+    w.loads_enqueued();
     PSC_CUDA(h.lanes.end(s), "psc_step");
     PSC_CUDA(cudaMemcpyAsync(h.host_out.p, w.out.p, kOutLen * sizeof(double), cudaMemcpyDeviceToHost, s), "psc_step");
     return PSC_OK;
@@ -1966,10 +1966,21 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
             for (int k = 0; k < nwin; ++k)
                 if (b->frozen[(size_t)k] < 0) b->w[(size_t)k]->imb_par = b->w[(size_t)k]->cur;
         }
-        // the loads of every active window in one launch sequence; they read the IMB field and
-        // geometry only: on a lane, beside the post-stream reductions
+        // the loads of every active window in one launch sequence read the IMB field and geometry
+        // only: on a lane, beside the post-stream reductions, which come from the next step run
+        // ahead (it writes the other buffer and IMB field only) or from a reduction-only pass.  The
+        // main stream's kernel is launched first: the loads wait for the particle upload anyway.
         PSC_TRY(batch_loads_table(*b, "psc_batch_step"));
         PSC_CUDA(b->lanes.begin(b->stream), "psc_batch_step");
+        const bool ahead = batch_may_run_ahead(*b, fields, inputs);
+        const double* post_rows = ahead ? b->red_next.p : b->red_post.p;
+        if (ahead) {
+            PSC_TRY(batch_launch(*b, PSC_STEP_COLLIDE | PSC_STEP_IMB | PSC_STEP_REDUCE));
+            PSC_TRY(psc_reduce_windows(b->table[b->parity ^ 1].p, nwin, b->red_next.p, b->stream));
+        } else {
+            PSC_TRY(batch_launch(*b, PSC_STEP_REDUCE | (fields ? PSC_STEP_MOMENTS : 0u)));
+            PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_post.p, b->stream));
+        }
         if (b->up_pending)  // the loads read the particles: after their upload
             PSC_CUDA(cudaStreamWaitEvent(b->lanes.lane(0), b->up_done, 0), "psc_batch_step");
         PSC_CUDA(launch_particle_loads_multi(batch_jobs(*b), batch_chunk_base(*b),
@@ -1982,17 +1993,6 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
                 b->w[(size_t)k]->loads_enqueued();
                 b->w[(size_t)k]->loads_ready = true;
             }
-        // post-stream reductions: from the next step run ahead (it writes the other buffer and IMB
-        // field only), else from a reduction-only pass
-        const bool ahead = batch_may_run_ahead(*b, fields, inputs);
-        const double* post_rows = ahead ? b->red_next.p : b->red_post.p;
-        if (ahead) {
-            PSC_TRY(batch_launch(*b, PSC_STEP_COLLIDE | PSC_STEP_IMB | PSC_STEP_REDUCE));
-            PSC_TRY(psc_reduce_windows(b->table[b->parity ^ 1].p, nwin, b->red_next.p, b->stream));
-        } else {
-            PSC_TRY(batch_launch(*b, PSC_STEP_REDUCE | (fields ? PSC_STEP_MOMENTS : 0u)));
-            PSC_TRY(psc_reduce_windows(b->table[b->parity].p, nwin, b->red_post.p, b->stream));
-        }
         PSC_CUDA(b->lanes.end(b->stream), "psc_batch_step");
         double* host = b->host.p;
         PSC_CUDA(cudaMemcpyAsync(host, b->red_pre.p, rows * 8, cudaMemcpyDeviceToHost, b->stream), "psc_batch_step");
