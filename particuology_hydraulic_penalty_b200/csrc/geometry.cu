@@ -200,9 +200,46 @@ __device__ __forceinline__ double smooth_alpha(int32_t ix, int32_t iy, int32_t i
     return acc / (Sd * Sd * Sd);
 }
 
-__global__ void k_geometry_count(psc_geometry g) {
+// sample_count for a compile-time S: the same IEEE operations on the same
+// operands, with the sample offsets (k + 0.5) / S computed once per thread and
+// each axis's squared distances once per cell (S values per axis), so a
+// sample costs one addition and one comparison: (dx2 + dy2) + dz2 <= r^2.
+template <int S>
+__device__ __forceinline__ int sample_count_t(int32_t ix, int32_t iy, int32_t iz, double px, double py, double pz,
+                                              double rr, const double (&o)[S]) {
+    double dy2[S], dz2[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+        const double dy = xsub(xadd((double)iy, o[k]), py);
+        const double dz = xsub(xadd((double)iz, o[k]), pz);
+        dy2[k] = xmul(dy, dy);
+        dz2[k] = xmul(dz, dz);
+    }
+    int cnt = 0;
+#pragma unroll
+    for (int a = 0; a < S; ++a) {
+        const double dx = xsub(xadd((double)ix, o[a]), px);
+        const double dx2 = xmul(dx, dx);
+#pragma unroll
+        for (int b = 0; b < S; ++b) {
+            const double dxy = xadd(dx2, dy2[b]);
+#pragma unroll
+            for (int c = 0; c < S; ++c) cnt += xadd(dxy, dz2[c]) <= rr ? 1 : 0;
+        }
+    }
+    return cnt;
+}
+
+// Inside-sample count of every bbox entry (S: the subsample count as a
+// compile-time constant, or 0: the general loop) and the per-cell entry counts
+// of the cell lists.
+template <int S>
+__global__ void __launch_bounds__(256) k_geometry_count(psc_geometry g) {
     const int64_t E = min(g.totals[0], g.capacity_entries);
     const bool smooth = g.smooth_eps > 0.0;
+    double o[S > 0 ? S : 1];
+#pragma unroll
+    for (int k = 0; k < (S > 0 ? S : 1); ++k) o[k] = xdiv((double)k + 0.5, (double)(S > 0 ? S : 1));  // (k + 0.5) / S
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
         const EntryCell c = decode_entry(g, e);
         const double* q = g.particles + (size_t)c.p * PF;
@@ -211,6 +248,8 @@ __global__ void k_geometry_count(psc_geometry g) {
             const double al = smooth_alpha(c.ix, c.iy, c.iz, q[0], q[1], q[2], q[3], g.subsamples, g.smooth_eps);
             g.ent_alpha[e] = al;
             cnt = al > 0.0 ? 1 : 0;  // membership of the cell list
+        } else if constexpr (S > 0) {
+            cnt = sample_count_t<S>(c.ix, c.iy, c.iz, q[0], q[1], q[2], xmul(q[3], q[3]), o);
         } else {
             cnt = sample_count(c.ix, c.iy, c.iz, q[0], q[1], q[2], xmul(q[3], q[3]), g.subsamples);
         }
@@ -1034,7 +1073,16 @@ cudaError_t launch_geometry_build(const psc_geometry& g, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(g.cell_n, 0, (size_t)N * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     if (g.capacity_entries > 0) {
-        k_geometry_count<<<grid_cap(g.capacity_entries, 256), 256, 0, stream>>>(g);
+        const unsigned grid = grid_cap(g.capacity_entries, 256);
+        switch (g.smooth_eps > 0.0 ? 0 : g.subsamples) {  // the count kernel for a compile-time S
+            case 1: k_geometry_count<1><<<grid, 256, 0, stream>>>(g); break;
+            case 2: k_geometry_count<2><<<grid, 256, 0, stream>>>(g); break;
+            case 3: k_geometry_count<3><<<grid, 256, 0, stream>>>(g); break;
+            case 4: k_geometry_count<4><<<grid, 256, 0, stream>>>(g); break;
+            case 5: k_geometry_count<5><<<grid, 256, 0, stream>>>(g); break;
+            case 6: k_geometry_count<6><<<grid, 256, 0, stream>>>(g); break;
+            default: k_geometry_count<0><<<grid, 256, 0, stream>>>(g); break;
+        }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if ((e = scan_exclusive_i32(g.cell_n, g.cell_off, N, g.scan_tmp, stream)) != cudaSuccess) return e;
