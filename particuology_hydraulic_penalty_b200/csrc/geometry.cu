@@ -134,29 +134,6 @@ __device__ __forceinline__ int owner_of(const int64_t* off, int P, int64_t e) {
     return lo;
 }
 
-struct EntryCell {
-    int p;
-    int32_t ix, iy, iz;
-    uint32_t cell;
-};
-
-__device__ __forceinline__ EntryCell decode_entry(const psc_geometry& g, int64_t e) {
-    EntryCell c;
-    c.p = owner_of(g.ent_off, g.nparticles, e);
-    const int32_t* bb = g.bbox + (size_t)c.p * 6;
-    const int64_t local = e - g.ent_off[c.p];
-    const int64_t eyz = (int64_t)bb[4] * bb[5];
-    const int32_t a = (int32_t)(local / eyz);
-    const int64_t rem = local - (int64_t)a * eyz;
-    const int32_t b = (int32_t)(rem / bb[5]);
-    const int32_t k = (int32_t)(rem - (int64_t)b * bb[5]);
-    c.ix = bb[0] + a;
-    c.iy = bb[1] + b;
-    c.iz = bb[2] + k;
-    c.cell = ((uint32_t)c.ix * (uint32_t)g.ny + (uint32_t)c.iy) * (uint32_t)g.nz + (uint32_t)c.iz;
-    return c;
-}
-
 // Inside-sample count of one cell: offsets (k + 0.5)/S, d = (i + o) - c,
 // (dx*dx + dy*dy) + dz*dz <= r*r, every operation rounded once
 // (psc3d.py:72, :86-89).
@@ -200,6 +177,38 @@ __device__ __forceinline__ double smooth_alpha(int32_t ix, int32_t iy, int32_t i
     return acc / (Sd * Sd * Sd);
 }
 
+// Descriptor of one load-reduction chunk, computed by k_chunk_desc (one
+// thread per chunk, so the lookups of many chunks overlap) into the chunk's
+// own partial row (6 doubles); every thread of the chunk's block reads it
+// before the chunk's last warp overwrites the row with the sums.
+struct ChunkDesc {
+    int64_t e0, e1;       // entry range
+    int32_t p;            // particle
+    int32_t local0;       // e0 - ent_off[p]
+    int32_t x0, y0, z0;   // clipped box origin
+    int32_t ey, ez;       // box extents in y and z
+    int32_t pad;
+};
+static_assert(sizeof(ChunkDesc) == 6 * sizeof(double), "a chunk descriptor fills one partial row");
+
+__device__ __forceinline__ ChunkDesc make_chunk_desc(const psc_geometry& g, int64_t c) {
+    const int p = owner_of(g.chunk_off, g.nparticles, c);
+    const int64_t eb = g.ent_off[p];
+    ChunkDesc d;
+    d.e0 = eb + (c - g.chunk_off[p]) * g.chunk_entries;
+    d.e1 = min(d.e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
+    d.p = p;
+    d.local0 = (int32_t)(d.e0 - eb);
+    const int32_t* bb = g.bbox + (size_t)p * 6;
+    d.x0 = bb[0];
+    d.y0 = bb[1];
+    d.z0 = bb[2];
+    d.ey = bb[4];
+    d.ez = bb[5];
+    d.pad = 0;
+    return d;
+}
+
 // sample_count for a compile-time S: the same IEEE operations on the same
 // operands, with the sample offsets (k + 0.5) / S computed once per thread and
 // each axis's squared distances once per cell (S values per axis), so a
@@ -233,43 +242,104 @@ __device__ __forceinline__ int sample_count_t(int32_t ix, int32_t iy, int32_t iz
 // Inside-sample count of every bbox entry (S: the subsample count as a
 // compile-time constant, or 0: the general loop) and the per-cell entry counts
 // of the cell lists.
+//
+// One block per load chunk (its particle and entry range from the chunk
+// offsets, one lookup per chunk instead of one per entry); thread t takes the
+// chunk's entries t, t + blockDim.x, ... and steps their bbox-local
+// coordinates by a carry-add.
 template <int S>
-__global__ void __launch_bounds__(256) k_geometry_count(psc_geometry g) {
+__global__ void __launch_bounds__(256, 2) k_geometry_count(psc_geometry g) {
     const int64_t E = min(g.totals[0], g.capacity_entries);
+    const int64_t C = g.totals[1];
     const bool smooth = g.smooth_eps > 0.0;
     double o[S > 0 ? S : 1];
 #pragma unroll
     for (int k = 0; k < (S > 0 ? S : 1); ++k) o[k] = xdiv((double)k + 0.5, (double)(S > 0 ? S : 1));  // (k + 0.5) / S
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
-        const EntryCell c = decode_entry(g, e);
-        const double* q = g.particles + (size_t)c.p * PF;
-        int cnt;
-        if (smooth) {
-            const double al = smooth_alpha(c.ix, c.iy, c.iz, q[0], q[1], q[2], q[3], g.subsamples, g.smooth_eps);
-            g.ent_alpha[e] = al;
-            cnt = al > 0.0 ? 1 : 0;  // membership of the cell list
-        } else if constexpr (S > 0) {
-            cnt = sample_count_t<S>(c.ix, c.iy, c.iz, q[0], q[1], q[2], xmul(q[3], q[3]), o);
-        } else {
-            cnt = sample_count(c.ix, c.iy, c.iz, q[0], q[1], q[2], xmul(q[3], q[3]), g.subsamples);
+    const uint32_t ny = (uint32_t)g.ny, nz = (uint32_t)g.nz;
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {
+        const ChunkDesc dsc = make_chunk_desc(g, chunk);
+        const int64_t e1 = min(dsc.e1, E);
+        int64_t e = dsc.e0 + threadIdx.x;
+        if (e >= e1) continue;
+        const double* q = g.particles + (size_t)dsc.p * PF;
+        const double px = q[0], py = q[1], pz = q[2], r = q[3], rr = xmul(r, r);
+        const uint32_t ey = (uint32_t)dsc.ey, ez = (uint32_t)dsc.ez, eyz = ey * ez;
+        const uint32_t local = (uint32_t)dsc.local0 + threadIdx.x;
+        uint32_t a = local / eyz;
+        const uint32_t rem = local - a * eyz;
+        uint32_t b = rem / ez;
+        uint32_t k = rem - b * ez;
+        const uint32_t step_k = blockDim.x % ez;
+        const uint32_t step_q = blockDim.x / ez;
+        const uint32_t step_b = step_q % ey;
+        const uint32_t step_a = step_q / ey;
+        for (; e < e1; e += blockDim.x) {
+            const int32_t ix = dsc.x0 + (int32_t)a, iy = dsc.y0 + (int32_t)b, iz = dsc.z0 + (int32_t)k;
+            int cnt;
+            if (smooth) {
+                const double al = smooth_alpha(ix, iy, iz, px, py, pz, r, g.subsamples, g.smooth_eps);
+                g.ent_alpha[e] = al;
+                cnt = al > 0.0 ? 1 : 0;  // membership of the cell list
+            } else if constexpr (S > 0) {
+                cnt = sample_count_t<S>(ix, iy, iz, px, py, pz, rr, o);
+            } else {
+                cnt = sample_count(ix, iy, iz, px, py, pz, rr, g.subsamples);
+            }
+            g.ent_cnt[e] = (uint16_t)cnt;
+            if (cnt > 0) atomicAdd(g.cell_n + (((uint32_t)ix * ny + (uint32_t)iy) * nz + (uint32_t)iz), 1);
+            // next entry of this thread: (a, b, k) += (step_a, step_b, step_k) with carries
+            k += step_k;
+            const uint32_t ck = k >= ez;
+            k -= ck ? ez : 0u;
+            b += step_b + ck;
+            const uint32_t cb = b >= ey;
+            b -= cb ? ey : 0u;
+            a += step_a + cb;
         }
-        g.ent_cnt[e] = (uint16_t)cnt;
-        if (cnt > 0) atomicAdd(g.cell_n + c.cell, 1);
     }
 }
 
-__global__ void k_geometry_fill(psc_geometry g) {
+// The cell lists: every entry with a non-zero count appends (particle, count)
+// to its cell's list (the order within a list is fixed by k_geometry_final's
+// sort).  Walks the chunks as k_geometry_count does.
+__global__ void __launch_bounds__(256) k_geometry_fill(psc_geometry g) {
     const int64_t E = min(g.totals[0], g.capacity_entries);
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
-        const uint16_t cnt = g.ent_cnt[e];
-        if (cnt == 0) continue;
-        const EntryCell c = decode_entry(g, e);
-        const int32_t pos = atomicAdd(g.cell_n + c.cell, 1);
-        const int64_t idx = (int64_t)g.cell_off[c.cell] + pos;
-        if (idx < g.capacity_entries) {
-            g.cl_pid[idx] = c.p;
-            g.cl_cnt[idx] = cnt;
-            if (g.cl_ent) g.cl_ent[idx] = (int32_t)e;
+    const int64_t C = g.totals[1];
+    const uint32_t ny = (uint32_t)g.ny, nz = (uint32_t)g.nz;
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {
+        const ChunkDesc dsc = make_chunk_desc(g, chunk);
+        const int64_t e1 = min(dsc.e1, E);
+        int64_t e = dsc.e0 + threadIdx.x;
+        if (e >= e1) continue;
+        const uint32_t ey = (uint32_t)dsc.ey, ez = (uint32_t)dsc.ez, eyz = ey * ez;
+        const uint32_t local = (uint32_t)dsc.local0 + threadIdx.x;
+        uint32_t a = local / eyz;
+        const uint32_t rem = local - a * eyz;
+        uint32_t b = rem / ez;
+        uint32_t k = rem - b * ez;
+        const uint32_t step_k = blockDim.x % ez;
+        const uint32_t step_q = blockDim.x / ez;
+        const uint32_t step_b = step_q % ey;
+        const uint32_t step_a = step_q / ey;
+        for (; e < e1; e += blockDim.x) {
+            const uint16_t cnt = g.ent_cnt[e];
+            if (cnt != 0) {
+                const uint32_t cell = (((uint32_t)dsc.x0 + a) * ny + ((uint32_t)dsc.y0 + b)) * nz + ((uint32_t)dsc.z0 + k);
+                const int32_t pos = atomicAdd(g.cell_n + cell, 1);
+                const int64_t idx = (int64_t)g.cell_off[cell] + pos;
+                if (idx < g.capacity_entries) {
+                    g.cl_pid[idx] = dsc.p;
+                    g.cl_cnt[idx] = cnt;
+                    if (g.cl_ent) g.cl_ent[idx] = (int32_t)e;
+                }
+            }
+            k += step_k;
+            const uint32_t ck = k >= ez;
+            k -= ck ? ez : 0u;
+            b += step_b + ck;
+            const uint32_t cb = b >= ey;
+            b -= cb ? ey : 0u;
+            a += step_a + cb;
         }
     }
 }
@@ -431,38 +501,6 @@ __device__ __forceinline__ void chunk_ring_finish(ChunkRing& r, long long j, dou
         }
     }
     __syncwarp();
-}
-
-// Descriptor of one load-reduction chunk, computed by k_chunk_desc (one
-// thread per chunk, so the lookups of many chunks overlap) into the chunk's
-// own partial row (6 doubles); every thread of the chunk's block reads it
-// before the chunk's last warp overwrites the row with the sums.
-struct ChunkDesc {
-    int64_t e0, e1;       // entry range
-    int32_t p;            // particle
-    int32_t local0;       // e0 - ent_off[p]
-    int32_t x0, y0, z0;   // clipped box origin
-    int32_t ey, ez;       // box extents in y and z
-    int32_t pad;
-};
-static_assert(sizeof(ChunkDesc) == 6 * sizeof(double), "a chunk descriptor fills one partial row");
-
-__device__ __forceinline__ ChunkDesc make_chunk_desc(const psc_geometry& g, int64_t c) {
-    const int p = owner_of(g.chunk_off, g.nparticles, c);
-    const int64_t eb = g.ent_off[p];
-    ChunkDesc d;
-    d.e0 = eb + (c - g.chunk_off[p]) * g.chunk_entries;
-    d.e1 = min(d.e0 + (int64_t)g.chunk_entries, g.ent_off[p + 1]);
-    d.p = p;
-    d.local0 = (int32_t)(d.e0 - eb);
-    const int32_t* bb = g.bbox + (size_t)p * 6;
-    d.x0 = bb[0];
-    d.y0 = bb[1];
-    d.z0 = bb[2];
-    d.ey = bb[4];
-    d.ez = bb[5];
-    d.pad = 0;
-    return d;
 }
 
 __global__ void __launch_bounds__(256) k_chunk_desc(psc_geometry g, double* part) {
@@ -1073,7 +1111,7 @@ cudaError_t launch_geometry_build(const psc_geometry& g, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(g.cell_n, 0, (size_t)N * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     if (g.capacity_entries > 0) {
-        const unsigned grid = grid_cap(g.capacity_entries, 256);
+        const unsigned grid = grid_cap(g.capacity_entries, g.chunk_entries > 0 ? g.chunk_entries : 4096);  // ~ one block per chunk
         switch (g.smooth_eps > 0.0 ? 0 : g.subsamples) {  // the count kernel for a compile-time S
             case 1: k_geometry_count<1><<<grid, 256, 0, stream>>>(g); break;
             case 2: k_geometry_count<2><<<grid, 256, 0, stream>>>(g); break;
@@ -1088,7 +1126,8 @@ cudaError_t launch_geometry_build(const psc_geometry& g, cudaStream_t stream) {
     if ((e = scan_exclusive_i32(g.cell_n, g.cell_off, N, g.scan_tmp, stream)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(g.cell_n, 0, (size_t)N * sizeof(int32_t), stream)) != cudaSuccess) return e;
     if (g.capacity_entries > 0) {
-        k_geometry_fill<<<grid_cap(g.capacity_entries, 256), 256, 0, stream>>>(g);
+        k_geometry_fill<<<grid_cap(g.capacity_entries, g.chunk_entries > 0 ? g.chunk_entries : 4096), 256, 0,
+                          stream>>>(g);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     k_geometry_final<<<grid_cap(N, 256), 256, 0, stream>>>(g);
