@@ -478,10 +478,16 @@ int psc_rebuild_geometry(psc_solver* h);
  * NULL.  Without PSC_RUN_DIAG the intermediate steps skip the reductions
  * (they change no state); the IMB field of the final step is always written.
  * psc_step(h, 1, PSC_RUN_DIAG) (one drop-in call) replays its launches from a
- * CUDA graph, one per population buffer, recorded on the second call whose
- * launch arguments (buffers, sizes, kernel, descriptor version) match the
- * previous call's; on a stream the caller is capturing it runs its launches
- * directly, so they go into the caller's graph. */
+ * CUDA graph, one per population buffer and kind of call, recorded on the
+ * second call whose launch arguments (buffers, sizes, kernel, descriptor
+ * version) match the previous call's; on a stream the caller is capturing it
+ * runs its launches directly, so they go into the caller's graph.  Such a call
+ * takes its post-stream sums from the next step, run ahead into the other
+ * population buffer and a second IMB field, when the step inputs (geometry,
+ * solid velocity, descriptors) are those of the previous such call; the next
+ * such call takes that step as its own if the inputs still match, and any
+ * other stepping or state-setting call drops it.  Results are the same bits
+ * as with a reduction-only pass. */
 int psc_step(psc_solver* h, int nsteps, unsigned flags, psc_status* h_status);
 /* Field `which` (PSC_FIELD_*) as float64 into h_dst ([N], or [19][N] for PSC_FIELD_F). */
 int psc_get_fields(psc_solver* h, int which, double* h_dst);
