@@ -505,14 +505,22 @@ int window_set_particles(Window& w, const double* hp, int P, cudaStream_t s, con
     return PSC_OK;
 }
 
-int window_rebuild(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* who) {
+// A geometry rebuild in two halves, so that a batch reads the entry and chunk
+// counts of all its windows after one synchronisation: the plan (bounding
+// boxes, entry and chunk offsets, totals) with the totals copied into the
+// pinned slot tot4[0..3], then, once the copy has landed, the buffers grown
+// to the counts and the build enqueued.
+int window_rebuild_plan(Window& w, cudaStream_t s, int64_t* tot4, const char* who) {
     psc_geometry g = w.geometry();
+    w.built = false;  // the plan overwrites the current geometry's offsets
     PSC_TRY(psc_geometry_plan(&g, s));
-    PSC_CUDA(tot.ensure(4), who);
-    PSC_CUDA(cudaMemcpyAsync(tot.p, w.totals.p, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), who);
-    PSC_CUDA(cudaStreamSynchronize(s), who);
-    w.n_entries = tot.p[0];
-    w.n_chunks = tot.p[1];
+    PSC_CUDA(cudaMemcpyAsync(tot4, w.totals.p, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), who);
+    return PSC_OK;
+}
+
+int window_rebuild_finish(Window& w, cudaStream_t s, const int64_t* tot4, const char* who) {
+    w.n_entries = tot4[0];
+    w.n_chunks = tot4[1];
     if (w.n_entries >= (1ll << 31) - 1)
         return fail(PSC_E_CAPACITY, std::string(who) + ": too many bounding-box entries (>= 2^31) for one window");
     if (w.n_entries > w.cap_entries) {
@@ -536,8 +544,7 @@ int window_rebuild(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* 
         }
         w.cap_chunks = cap;
     }
-    w.built = false;  // until the build below is enqueued (the stored owner weights belong to the old one)
-    g = w.geometry();
+    psc_geometry g = w.geometry();
     PSC_TRY(psc_geometry_build(&g, s));
     w.built = true;
     w.built_version = w.pversion;
@@ -546,6 +553,13 @@ int window_rebuild(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* 
     w.loads_ready = false;
     w.diag_ready = false;
     return PSC_OK;
+}
+
+int window_rebuild(Window& w, cudaStream_t s, HArray<int64_t>& tot, const char* who) {
+    PSC_CUDA(tot.ensure(4), who);
+    PSC_TRY(window_rebuild_plan(w, s, tot.p, who));
+    PSC_CUDA(cudaStreamSynchronize(s), who);
+    return window_rebuild_finish(w, s, tot.p, who);
 }
 
 int window_solid_velocity(Window& w, cudaStream_t s) {
@@ -1523,8 +1537,9 @@ int batch_loads_table(psc_batch& b, const char* who) {
     const int t = b.parity;
     b.jobs_par = t;
     if (bytes == b.jobs_last[t]) return PSC_OK;
-    // kernels of earlier steps may still read the old table or partials, the copy the pinned buffer
-    PSC_CUDA(cudaStreamSynchronize(b.stream), who);
+    // No wait is needed before the rewrite: only reporting calls use the table, its pinned copy and
+    // the partials, and every reporting call ends with a stream synchronisation, so nothing of an
+    // earlier call still reads them (a buffer that grows is freed by cudaFree, which waits anyway).
     PSC_CUDA(b.loads_part.ensure(std::max<int64_t>(b.jobs_chunks, 1) * 6, false, b.stream), who);
     PSC_CUDA(b.jobs_dev[t].ensure((int64_t)bytes.size(), false, b.stream), who);
     PSC_CUDA(b.jobs_host[t].ensure((int64_t)bytes.size()), who);
@@ -1643,6 +1658,18 @@ int batch_upload_join(psc_batch& b, const char* who) {
 
 // Everything the next step reads is on the device and described by the tables.
 int batch_prepare(psc_batch& b, bool imb, bool moments) {
+    // geometry rebuilds: every window's plan, one synchronisation for all their counts, the builds
+    const char* who = "psc_batch_step";
+    std::vector<size_t> plan;
+    for (size_t k = 0; k < b.w.size(); ++k)
+        if (window_needs_rebuild(*b.w[k])) plan.push_back(k);
+    if (!plan.empty()) {
+        PSC_TRY(batch_upload_join(b, who));
+        PSC_CUDA(b.tot.ensure(4 * (int64_t)b.w.size()), who);
+        for (size_t k : plan) PSC_TRY(window_rebuild_plan(*b.w[k], b.stream, b.tot.p + 4 * k, who));
+        PSC_CUDA(cudaStreamSynchronize(b.stream), who);
+        for (size_t k : plan) PSC_TRY(window_rebuild_finish(*b.w[k], b.stream, b.tot.p + 4 * k, who));
+    }
     for (size_t k = 0; k < b.w.size(); ++k) {
         Window& w = *b.w[k];
         if (window_prepare_reads_particles(w)) PSC_TRY(batch_upload_join(b, "psc_batch_step"));
