@@ -395,16 +395,20 @@ def adjoint_check(n: int = 96, n_fines: int = 64, steps: int = 2000, every: int 
     p32 = problem("fp32")
     p32.forward(parts)  # untimed: first launches, buffers
     p32.backward()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    torch.cuda.synchronize()
-    ev[0].record()
-    K32 = p32.forward(parts)
-    ev[1].record()
-    g32 = per_sphere(p32.backward())
-    ev[2].record()
-    torch.cuda.synchronize()
-    t_fwd = ev[0].elapsed_time(ev[1]) * 1e-3  # CUDA events on the current stream (the handle synchronises)
-    t_bwd = ev[1].elapsed_time(ev[2]) * 1e-3
+    # two timed forward + backward passes, the faster of each kept (one pass is a few hundred launches,
+    # so host noise shows in a single measurement)
+    t_fwd = t_bwd = float("inf")
+    for _ in range(2):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record()
+        K32 = p32.forward(parts)
+        ev[1].record()
+        g32 = per_sphere(p32.backward())
+        ev[2].record()
+        torch.cuda.synchronize()
+        t_fwd = min(t_fwd, ev[0].elapsed_time(ev[1]) * 1e-3)  # CUDA events on the current stream (the handle
+        t_bwd = min(t_bwd, ev[1].elapsed_time(ev[2]) * 1e-3)  # synchronises)
     p64 = problem("fp64")
     K64 = p64.forward(parts)
     g64 = per_sphere(p64.backward())
