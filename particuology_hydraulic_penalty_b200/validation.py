@@ -395,7 +395,7 @@ def adjoint_check(n: int = 96, n_fines: int = 64, steps: int = 2000, every: int 
     p32 = problem("fp32")
     p32.forward(parts)  # untimed: first launches, buffers
     p32.backward()
-    # two timed forward + backward passes, the faster of each kept (one pass is a few hundred launches,
+    # two timed forward + backward passes, the faster of each kept (a pass is thousands of launches,
     # so host noise shows in a single measurement)
     t_fwd = t_bwd = float("inf")
     for _ in range(2):
