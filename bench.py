@@ -449,8 +449,9 @@ def run_e2e_batch(windows, steps: int, graph_steps: int, world: int = 1):
     from particuology_hydraulic_penalty_b200 import _native as nat
     from particuology_hydraulic_penalty_b200.handle import BatchHandle, make_config
 
-    cfgs = [make_config((w.n,) * 3, tau=TAU, force=FORCE, subsamples=SUBSAMPLES, store=nat.STORE_F32)
-            for w in windows]
+    dev = torch.cuda.current_device() if torch.cuda.is_available() else 0  # this rank's GPU
+    cfgs = [make_config((w.n,) * 3, tau=TAU, force=FORCE, subsamples=SUBSAMPLES, store=nat.STORE_F32,
+                        device_index=dev) for w in windows]
     b = BatchHandle(cfgs, graph_steps=graph_steps)
     for k, w in enumerate(windows):
         b.set_particles(k, w.particles)
