@@ -704,7 +704,7 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
 // entry of the thread (weight and cell), then the IMB momentum of those cells;
 // the next chunk's descriptor and counts are loaded meanwhile.  Two memory
 // round trips per chunk instead of one per dependent load.
-constexpr int LIST_STAGE_K = 8;  // list entries per thread staged at a time (a column holds up to 16: two passes)
+constexpr int LIST_STAGE_K = 6;  // list entries per thread staged at a time (a column holds up to 16: three passes)
 static_assert(LOAD_THREADS == PSC_LOAD_THREADS, "the loads list layout assumes PSC_LOAD_THREADS threads per chunk");
 
 template <typename I>
