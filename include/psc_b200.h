@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define PSC_ABI_VERSION 4
+#define PSC_ABI_VERSION 5
 
 /* ---- status codes ------------------------------------------------------- */
 #define PSC_OK 0
@@ -189,18 +189,20 @@ typedef struct psc_geometry {
     double* ent_alpha;        /* [capacity_entries] smooth alpha per entry (smooth mode) */
     int32_t* cl_ent;          /* [capacity_entries] entry index per cell-list slot (smooth mode) */
     /* Loads list, for a geometry used by more than one loads call (static
-     * particles).  Every load chunk is reduced by PSC_LOAD_THREADS threads, thread
-     * t taking the chunk's entries t, t + PSC_LOAD_THREADS, ...  The list keeps,
-     * per chunk and thread, that thread's entries with a non-zero sample count in
-     * their order: slot k of thread t of chunk c is c * chunk_entries +
-     * k * PSC_LOAD_THREADS + t, holding the entry's owner weight
-     * alpha_p / max(alpha_sum, 1e-14) (load_w) and its bbox-local cell a | b << 11
-     * | k << 22 (load_abk); load_n[c * PSC_LOAD_THREADS + t] counts them.  With the
-     * three arrays set and list_ready == 0, psc_particle_loads also writes the
-     * list; with list_ready == 1 it reduces from the list instead of the whole
-     * boxes (same sums, bit for bit: each thread adds the same entries in the same
-     * order).  The caller sets list_ready after a call on the same geometry.
-     * Needs chunk_entries a multiple of PSC_LOAD_THREADS, at most 16 of them, and
+     * particles).  Every load chunk is reduced by PSC_LOAD_THREADS threads (warps
+     * of 32).  Warp w owns the chunk's entries 32w + l + j * PSC_LOAD_THREADS
+     * (lane l, in order of j then l); its entries with a non-zero sample count are
+     * numbered c = 0, 1, ... in that order and dealt round-robin to its lanes:
+     * entry c is slot k = c / 32 of thread t = 32w + c % 32, at list index
+     * chunk * chunk_entries + k * PSC_LOAD_THREADS + t, holding the entry's owner
+     * weight alpha_p / max(alpha_sum, 1e-14) (load_w) and its bbox-local cell
+     * a | b << 11 | k << 22 (load_abk); load_n[chunk * PSC_LOAD_THREADS + t]
+     * counts thread t's slots.  With the three arrays set, psc_particle_loads
+     * reduces from the list, building it first when list_ready == 0 (so every
+     * call on a geometry gives the same sums, bit for bit); the caller sets
+     * list_ready after a call on the same geometry.  Without the arrays it
+     * reduces over the whole boxes (the same loads to round-off).  Needs
+     * chunk_entries a multiple of PSC_LOAD_THREADS, at most 16 of them, and
      * nx, ny <= 2048, nz <= 1024; NULL arrays = no list. */
     double* load_w;           /* [capacity_chunks * chunk_entries] or NULL */
     uint32_t* load_abk;       /* [capacity_chunks * chunk_entries] or NULL */

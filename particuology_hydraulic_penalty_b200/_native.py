@@ -14,7 +14,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libpscb200.so"
 HEADER_PATH = Path(__file__).resolve().parents[1] / "include" / "psc_b200.h"
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 # status codes
 PSC_OK = 0

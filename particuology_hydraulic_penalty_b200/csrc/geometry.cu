@@ -560,20 +560,16 @@ __device__ __forceinline__ void cp_async_wait() {
 // fixed mixed-radix stride with carries (one 32-bit division per chunk).
 // s_al holds count / S^3 for every count; cap_entries is the length of
 // ent_cnt (the count pairs are read as aligned 32-bit words inside it).
-//
-// With lw set, the thread's entries with a non-zero count also go into the
-// loads list (slots slot0, slot0 + blockDim.x, ...: owner weight and bbox-local
-// cell, in this order); returns how many.
+// (The path of a geometry without a loads list.)
 template <typename I>
-__device__ __forceinline__ uint32_t chunk_thread_sums(const ChunkDesc& dsc, const double* particles,
-                                                      const uint16_t* ent_cnt, int64_t cap_entries,
-                                                      const double* alpha_sum, const I* imb, uint32_t N, uint32_t ny,
-                                                      uint32_t nz, const double* s_al, LoadRing<I>& ring,
-                                                      double (&acc)[6], double* lw, uint32_t* labk, int64_t slot0) {
+__device__ __forceinline__ void chunk_thread_sums(const ChunkDesc& dsc, const double* particles,
+                                                  const uint16_t* ent_cnt, int64_t cap_entries,
+                                                  const double* alpha_sum, const I* imb, uint32_t N, uint32_t ny,
+                                                  uint32_t nz, const double* s_al, LoadRing<I>& ring,
+                                                  double (&acc)[6]) {
     const int64_t e0 = dsc.e0, e1 = dsc.e1;
     const int tid = threadIdx.x;
-    uint32_t listed = 0;
-    if (e0 + tid >= e1) return listed;
+    if (e0 + tid >= e1) return;
     const double* q = particles + (size_t)dsc.p * PF;
     const uint32_t ey = (uint32_t)dsc.ey, ez = (uint32_t)dsc.ez;
     // bbox-local coordinates of this thread's first entry, and the stride
@@ -628,12 +624,6 @@ __device__ __forceinline__ uint32_t chunk_thread_sums(const ChunkDesc& dsc, cons
             // owner weight alpha_p / max(alpha_sum, 1e-14)   (psc3d.py:386)
             const double al = s_al[cnt];
             const double ow = xdiv(al, as > 1.0e-14 ? as : 1.0e-14);
-            if (lw) {
-                const int64_t sl = slot0 + (int64_t)listed * blockDim.x;
-                lw[sl] = ow;
-                labk[sl] = a | (b << 11) | (k << 22);
-                ++listed;
-            }
             const double nfx = -xmul(ow, mx);
             const double nfy = -xmul(ow, my);
             const double nfz = -xmul(ow, mz);
@@ -661,7 +651,6 @@ __device__ __forceinline__ uint32_t chunk_thread_sums(const ChunkDesc& dsc, cons
         a += step_a + cb;
     }
     cp_async_wait<0>();  // nothing in flight into the ring when the next chunk starts
-    return listed;
 }
 
 // One block per chunk of one particle's bbox entries.
@@ -682,21 +671,16 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS) k_loads_ch
         // every thread reads the chunk's descriptor before the chunk's last warp overwrites the row
         const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        const bool list = g.load_w && g.load_abk && g.load_n;  // write the loads list too
-        const uint32_t listed = chunk_thread_sums<I>(
-            dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum, imb, N, (uint32_t)g.ny, (uint32_t)g.nz, s_al,
-            ring, acc, list ? g.load_w : nullptr, g.load_abk, chunk * g.chunk_entries + threadIdx.x);
-        if (list) g.load_n[chunk * LOAD_THREADS + threadIdx.x] = (uint8_t)listed;
+        chunk_thread_sums<I>(dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum, imb, N, (uint32_t)g.ny,
+                             (uint32_t)g.nz, s_al, ring, acc);
         chunk_ring_finish(rows, j, acc, part + chunk * 6);
     }
 }
 
-// The list path: the chunk's sums from the loads list a previous call on the
-// same geometry wrote.  Thread t reduces its own entries of the chunk (slots
-// slot0 + k * blockDim.x, k < its count) in the order chunk_thread_sums visits
-// them, with the same arithmetic on each, so the sums are bitwise the same;
-// gone are the zero-count entries, the count and alpha-sum gathers and the FP64
-// division.
+// The list path: the chunk's sums from its loads list (chunk_list_build, run
+// by the first loads call on a geometry).  Thread t reduces its slots
+// slot0 + k * blockDim.x, k < its count, in order; gone are the zero-count
+// entries, the count and alpha-sum gathers and the FP64 division.
 //
 // The gathers are latency-bound, so a chunk is staged in two asynchronous
 // copies into the thread's own shared-memory column (cp.async, no registers
@@ -825,6 +809,94 @@ __global__ void __launch_bounds__(LOAD_THREADS, 3) k_loads_chunks_list(psc_geome
     }
 }
 
+// The loads list of one chunk, built warp by warp.  Warp w of the block owns
+// the chunk's bbox entries 32w + l + PSC_LOAD_THREADS j (lane l, j <
+// chunk_entries / PSC_LOAD_THREADS), visited in that order; its entries with a
+// non-zero count are numbered c = 0, 1, ... in that order and dealt round-robin
+// to its lanes: entry c goes to slot k = c / 32 of lane c % 32, i.e. list slot
+// chunk * chunk_entries + k * PSC_LOAD_THREADS + 32w + c % 32, with its owner
+// weight alpha_p / max(alpha_sum, 1e-14) (psc3d.py:386) and its bbox-local
+// cell.  So neighbouring lanes reduce neighbouring cells (the IMB gathers of a
+// warp touch few lines) and a warp's lanes own counts that differ by at most one.
+__device__ __forceinline__ void chunk_list_build(const ChunkDesc& dsc, const uint16_t* ent_cnt, int64_t E,
+                                                 const double* alpha_sum, uint32_t ny, uint32_t nz,
+                                                 const double* s_al, int32_t chunk_entries, double* lw,
+                                                 uint32_t* labk, int64_t slot_chunk, uint8_t* load_n_chunk) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t ey = (uint32_t)dsc.ey, ez = (uint32_t)dsc.ez, eyz = ey * ez;
+    const int passes = chunk_entries / LOAD_THREADS;
+    const int64_t e1 = min(dsc.e1, E);
+    const uint32_t below = (1u << lane) - 1u;  // lanes before this one
+    uint32_t base = 0;                          // non-zero entries of the warp so far
+#pragma unroll 4
+    for (int j = 0; j < passes; ++j) {  // warp-uniform
+        const uint32_t off = warp * 32u + lane + (uint32_t)j * LOAD_THREADS;  // entry offset in the chunk
+        const int64_t e = dsc.e0 + off;
+        const uint32_t cnt = e < e1 ? (uint32_t)ent_cnt[e] : 0u;
+        const uint32_t mask = __ballot_sync(0xffffffffu, cnt != 0u);
+        if (cnt != 0u) {
+            const uint32_t local = (uint32_t)dsc.local0 + off;
+            const uint32_t a = local / eyz;
+            const uint32_t rem = local - a * eyz;
+            const uint32_t b = rem / ez;
+            const uint32_t k = rem - b * ez;
+            const uint32_t cell = (((uint32_t)dsc.x0 + a) * ny + ((uint32_t)dsc.y0 + b)) * nz + ((uint32_t)dsc.z0 + k);
+            const double as = alpha_sum[cell];
+            const double ow = xdiv(s_al[cnt], as > 1.0e-14 ? as : 1.0e-14);
+            const uint32_t c = base + __popc(mask & below);
+            const int64_t slot = slot_chunk + (int64_t)(c >> 5) * LOAD_THREADS + warp * 32u + (c & 31u);
+            lw[slot] = ow;
+            labk[slot] = a | (b << 11) | (k << 22);
+        }
+        base += __popc(mask);
+    }
+    load_n_chunk[warp * 32u + lane] = (uint8_t)(base > lane ? (base - lane + 31u) >> 5 : 0u);
+}
+
+// The loads list of every chunk of one geometry (descriptors in the partial rows).
+__global__ void __launch_bounds__(LOAD_THREADS) k_loads_list_build(const __grid_constant__ psc_geometry g,
+                                                                   const double* part) {
+    extern __shared__ double s_al[];  // S^3 + 1 entries (dynamic)
+    const int S3 = g.subsamples * g.subsamples * g.subsamples;
+    const double S3d = (double)S3;
+    for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
+    __syncthreads();
+    const int64_t C = g.totals[1];
+    const int64_t E = min(g.totals[0], g.capacity_entries);
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {
+        const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
+        chunk_list_build(dsc, g.ent_cnt, E, g.alpha_sum, (uint32_t)g.ny, (uint32_t)g.nz, s_al, g.chunk_entries,
+                         g.load_w, g.load_abk, chunk * g.chunk_entries, g.load_n + chunk * LOAD_THREADS);
+    }
+}
+
+// The loads lists of the jobs whose list is not current, in one launch.
+__global__ void __launch_bounds__(LOAD_THREADS) k_loads_list_build_multi(const LoadsJob* jobs,
+                                                                         const int64_t* chunk_base, int njobs,
+                                                                         const double* part) {
+    extern __shared__ double s_al[];  // S^3 + 1 entries for the largest S of the jobs (dynamic)
+    const int64_t C = chunk_base[njobs];
+    int cur_S = 0;  // S of the table in s_al (block-uniform: every thread visits the same chunks)
+    for (int64_t chunk = blockIdx.x; chunk < C; chunk += gridDim.x) {
+        const ChunkDesc dsc = *reinterpret_cast<const ChunkDesc*>(part + chunk * 6);
+        const psc_geometry& g = jobs[dsc.pad].g;
+        if (g.list_ready) continue;  // block-uniform
+        const int S = g.subsamples;
+        if (S != cur_S) {
+            __syncthreads();  // no thread reads the old table any more
+            const int S3 = S * S * S;
+            const double S3d = (double)S3;
+            for (int c = threadIdx.x; c <= S3; c += blockDim.x) s_al[c] = xdiv((double)c, S3d);
+            __syncthreads();
+            cur_S = S;
+        }
+        const int64_t local = chunk - chunk_base[dsc.pad];
+        chunk_list_build(dsc, g.ent_cnt, min(g.totals[0], g.capacity_entries), g.alpha_sum, (uint32_t)g.ny,
+                         (uint32_t)g.nz, s_al, g.chunk_entries, g.load_w, g.load_abk, local * g.chunk_entries,
+                         g.load_n + local * LOAD_THREADS);
+    }
+}
+
 // Per-particle sums of the chunk partials c0 .. c1-1: one warp per particle,
 // lane l sums chunks c0 + l, c0 + l + 32, ... in order, then a fixed shuffle tree.
 __device__ __forceinline__ void particle_sums(const double* part, int64_t c0, int64_t c1, double* force,
@@ -945,13 +1017,9 @@ __global__ void __launch_bounds__(LOAD_THREADS, PSC_LOADS_MIN_BLOCKS)
             cur_S = S;
         }
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        const int64_t local = chunk - chunk_base[dsc.pad];  // the chunk's index in its job
-        const bool list = g.load_w && g.load_abk && g.load_n;  // write the job's loads list too
-        const uint32_t listed = chunk_thread_sums<I>(
-            dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum, reinterpret_cast<const I*>(jobs[dsc.pad].imb),
-            (uint32_t)g.nx * g.ny * g.nz, (uint32_t)g.ny, (uint32_t)g.nz, s_al, ring, acc,
-            list ? g.load_w : nullptr, g.load_abk, local * g.chunk_entries + threadIdx.x);
-        if (list) g.load_n[local * LOAD_THREADS + threadIdx.x] = (uint8_t)listed;
+        chunk_thread_sums<I>(dsc, g.particles, g.ent_cnt, g.capacity_entries, g.alpha_sum,
+                             reinterpret_cast<const I*>(jobs[dsc.pad].imb), (uint32_t)g.nx * g.ny * g.nz,
+                             (uint32_t)g.ny, (uint32_t)g.nz, s_al, ring, acc);
         chunk_ring_finish(rows, j, acc, part + chunk * 6);
     }
 }
@@ -1186,14 +1254,15 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
         cudaError_t e0 = loads_smem_optin();
         if (e0 != cudaSuccess) return e0;
         k_chunk_desc<<<(unsigned)(cg < cap ? cg : cap), 256, 0, stream>>>(g, chunk_partials);
-        if (g.load_w && g.load_abk && g.load_n && g.list_ready) {  // this geometry's loads list is written
+        if (g.load_w && g.load_abk && g.load_n) {  // the list path: the list first, unless it is current
+            if (!g.list_ready) k_loads_list_build<<<grid, LOAD_THREADS, lut, stream>>>(g, chunk_partials);
             if (imb_type == 0)
                 k_loads_chunks_list<double><<<grid, LOAD_THREADS, list_stage_bytes<double>(), stream>>>(
                     g, reinterpret_cast<const double*>(imb), chunk_partials);
             else
                 k_loads_chunks_list<float><<<grid, LOAD_THREADS, list_stage_bytes<float>(), stream>>>(
                     g, reinterpret_cast<const float*>(imb), chunk_partials);
-        } else if (imb_type == 0) {  // (writes the loads list when its arrays are given)
+        } else if (imb_type == 0) {  // no loads list: the whole boxes
             k_loads_chunks<double><<<grid, LOAD_THREADS, lut, stream>>>(g, reinterpret_cast<const double*>(imb),
                                                                         chunk_partials);
         } else {
@@ -1215,7 +1284,7 @@ cudaError_t launch_particle_loads(const psc_geometry& g, int imb_type, const voi
 cudaError_t launch_particle_loads_multi(const LoadsJob* d_jobs, const int64_t* d_chunk_base,
                                         const int64_t* d_particle_base, int njobs, int64_t total_chunks,
                                         int64_t total_particles, int imb_type, int max_subsamples,
-                                        bool list_ready, double* part, cudaStream_t stream) {
+                                        bool all_lists, bool list_ready, double* part, cudaStream_t stream) {
     if (njobs <= 0) return cudaSuccess;
     const int64_t cap = (int64_t)sm_count() * 16;
     if (total_chunks > 0) {
@@ -1225,10 +1294,13 @@ cudaError_t launch_particle_loads_multi(const LoadsJob* d_jobs, const int64_t* d
         k_chunk_desc_multi<<<(unsigned)(cg < cap ? cg : cap), 256, 0, stream>>>(d_jobs, d_chunk_base, njobs, part);
         const unsigned grid = (unsigned)(total_chunks < cap ? total_chunks : cap);
         const size_t lut = (size_t)(max_subsamples * max_subsamples * max_subsamples + 1) * sizeof(double);
-        if (list_ready && imb_type == 0)
+        // every job has a loads list: the lists that are not current first, then the list path
+        if (all_lists && !list_ready)
+            k_loads_list_build_multi<<<grid, LOAD_THREADS, lut, stream>>>(d_jobs, d_chunk_base, njobs, part);
+        if (all_lists && imb_type == 0)
             k_loads_chunks_list_multi<double><<<grid, LOAD_THREADS, list_stage_bytes<double>(), stream>>>(
                 d_jobs, d_chunk_base, njobs, part);
-        else if (list_ready)
+        else if (all_lists)
             k_loads_chunks_list_multi<float><<<grid, LOAD_THREADS, list_stage_bytes<float>(), stream>>>(
                 d_jobs, d_chunk_base, njobs, part);
         else if (imb_type == 0)

@@ -66,13 +66,14 @@ struct LoadsJob {
 // Particle loads and load diagnostics of njobs windows in four launches.
 // d_chunk_base / d_particle_base: [njobs + 1] exclusive prefix sums of the
 // jobs' chunk and particle counts (the totals are their last entries, also
-// passed by value); part: total_chunks rows of 6 doubles.  list_ready: every
-// job's loads list is written (the list path); otherwise the loads are reduced
-// over the whole boxes and the lists are written where a job gives the arrays.
+// passed by value); part: total_chunks rows of 6 doubles.  all_lists: every
+// job gives loads-list arrays (the list path: the lists of the jobs whose list
+// is not current are built first); list_ready: every job's list is current.
+// Without all_lists the loads are reduced over the whole boxes.
 cudaError_t launch_particle_loads_multi(const LoadsJob* d_jobs, const int64_t* d_chunk_base,
                                         const int64_t* d_particle_base, int njobs, int64_t total_chunks,
                                         int64_t total_particles, int imb_type, int max_subsamples,
-                                        bool list_ready, double* part, cudaStream_t stream);
+                                        bool all_lists, bool list_ready, double* part, cudaStream_t stream);
 
 cudaError_t launch_adjoint_seed(const psc_adjoint_args& a, cudaStream_t stream);
 cudaError_t launch_adjoint_step(const psc_adjoint_args& a, cudaStream_t stream);

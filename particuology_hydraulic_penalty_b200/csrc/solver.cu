@@ -1483,7 +1483,8 @@ struct psc_batch {
     DArray<double> loads_part;  // chunk partials of all jobs
     int jobs_n = 0, jobs_max_s = 1;
     int64_t jobs_chunks = 0, jobs_particles = 0;
-    bool jobs_list_ready = false;  // every job's loads list is written (the list path of the loads)
+    bool jobs_list_ready = false;  // every job's loads list is current
+    bool jobs_all_lists = false;   // every job has loads-list arrays (the list path of the loads)
 
     ~psc_batch() {
         for (auto& g : graph)
@@ -1505,7 +1506,7 @@ int batch_loads_table(psc_batch& b, const char* who) {
     std::vector<LoadsJob> jobs;
     std::vector<int64_t> cb(1, 0), pb(1, 0);
     int max_s = 1;
-    bool ready = true;
+    bool ready = true, lists = true;
     for (int k = 0; k < nwin; ++k) {
         if (b.frozen[(size_t)k] >= 0) continue;
         const Window& w = *b.w[(size_t)k];
@@ -1513,6 +1514,7 @@ int batch_loads_table(psc_batch& b, const char* who) {
         std::memset(&j, 0, sizeof(j));  // padding too: the table is compared bytewise
         j.g = w.geometry();
         ready = ready && (w.P == 0 || j.g.list_ready);
+        lists = lists && (w.P == 0 || (j.g.load_w && j.g.load_abk && j.g.load_n));
         j.imb = w.imb_for(w.cur);
         j.imb_sums = b.red_pre.p + (size_t)k * PSC_NRED + PSC_RED_IMBX;
         j.forces = w.forces.p;
@@ -1534,6 +1536,7 @@ int batch_loads_table(psc_batch& b, const char* who) {
     b.jobs_chunks = cb.back();
     b.jobs_particles = pb.back();
     b.jobs_list_ready = ready;
+    b.jobs_all_lists = lists;
     const int t = b.parity;
     b.jobs_par = t;
     if (bytes == b.jobs_last[t]) return PSC_OK;
@@ -2012,7 +2015,8 @@ int psc_batch_step(psc_batch* b, int nsteps, unsigned flags, psc_status* h_statu
             PSC_CUDA(cudaStreamWaitEvent(b->lanes.lane(0), b->up_done, 0), "psc_batch_step");
         PSC_CUDA(launch_particle_loads_multi(batch_jobs(*b), batch_chunk_base(*b),
                                              batch_particle_base(*b), b->jobs_n, b->jobs_chunks, b->jobs_particles,
-                                             b->w[0]->field_type(), b->jobs_max_s, b->jobs_list_ready,
+                                             b->w[0]->field_type(), b->jobs_max_s, b->jobs_all_lists,
+                                             b->jobs_list_ready,
                                              b->loads_part.p, b->lanes.lane(0)),
                  "psc_batch_step: particle loads");
         for (int k = 0; k < nwin; ++k)

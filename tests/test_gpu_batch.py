@@ -70,8 +70,10 @@ def test_batch_loads_match_dropin():
                        force=(1e-6, 0.0, 0.0))
     for _ in range(6):
         s.collide_stream_psc()
-    assert np.array_equal(F, s.hydro_forces)
-    assert np.array_equal(T, s.hydro_torques)
+    # the drop-in reduces from its loads list, this batch over the whole boxes: the same sums in
+    # another order, equal to round-off
+    assert np.linalg.norm(F - s.hydro_forces) <= 1e-12 * np.linalg.norm(s.hydro_forces)
+    assert np.linalg.norm(T - s.hydro_torques) <= 1e-12 * np.linalg.norm(s.hydro_torques)
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64", "bf16"])

@@ -150,7 +150,9 @@ def test_batch_handle_matches_python_batch(precision):
         mom = py.velocity_field(k)
         assert np.array_equal(b.field(k, nat.FIELD_UX), mom[1].reshape(-1).astype(np.float64))
         F, T = b.loads(k)
-        assert np.array_equal(F, loads[k][0]) and np.array_equal(T, loads[k][1])
+        # the handle reduces from its loads list, PscBatch over the whole boxes: equal to round-off
+        assert np.linalg.norm(F - loads[k][0]) <= 1e-12 * np.linalg.norm(loads[k][0])
+        assert np.linalg.norm(T - loads[k][1]) <= 1e-12 * np.linalg.norm(loads[k][1])
 
 
 def test_batch_handle_tma_matches_direct():

@@ -1,14 +1,15 @@
-"""Particle loads from the loads list equal the whole-box path bit for bit.
+"""Particle loads through the loads list: the first call on a geometry and the later ones agree
+bit for bit.
 
-The first loads call on a geometry reduces every bbox entry, computing its owner
-weight alpha_p / max(alpha_sum, 1e-14) (psc3d.py:386), and writes the list of
-non-zero entries with their weights; later calls on the same geometry reduce
-from the list.  Two runs reach the same state: one takes two steps in one call
-(its only loads call reduces the whole boxes), the other takes two one-step
-calls (its second loads call reads the list).  Forces, torques and load
-diagnostics must agree exactly, for one window and for a batch, in FP32 and in
-the exact FP64 mode.  A geometry rebuilt for moved particles must not reuse the
-old list.
+The first loads call on a geometry builds its list -- the bbox entries with a
+non-zero count and their owner weights alpha_p / max(alpha_sum, 1e-14)
+(psc3d.py:386), dealt to the lanes of each warp -- and reduces from it; later
+calls on the same geometry reduce from the list without building it.  Two runs
+reach the same state: one takes two steps in one call (its only loads call
+builds the list), the other takes two one-step calls (its second loads call
+reuses the list).  Forces, torques and load diagnostics must agree exactly, for
+one window and for a batch, in FP32 and in the exact FP64 mode.  A geometry
+rebuilt for moved particles must not reuse the old list.
 """
 
 import numpy as np
@@ -122,9 +123,9 @@ def test_chunk_rows_with_many_chunks_per_block():
     """The load-chunk kernels write a chunk's row from the warp that finishes the chunk last, through
     a ring of four partial-sum slots per block; a warp may run ahead of the others by up to four
     chunks.  On the 24 windows of the benchmark batch (about 15 000 chunks for 2368 blocks) every
-    block reuses its slots, in the whole-box pass (first step) and in the list pass (second step).
-    Each window's forces and torques equal those of the window run alone, where a block holds far
-    fewer chunks, bit for bit, and no kernel gave up a wait."""
+    block reuses its slots, in the first step (list built, then reduced) and in the second (list
+    reused).  Each window's forces and torques equal those of the window run alone, where a block
+    holds far fewer chunks, bit for bit, and no kernel gave up a wait."""
     from particuology_hydraulic_penalty_b200 import _native as nat
     from particuology_hydraulic_penalty_b200 import windows as wgen
     from particuology_hydraulic_penalty_b200.handle import BatchHandle, SolverHandle, make_config
