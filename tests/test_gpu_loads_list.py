@@ -154,3 +154,74 @@ def test_chunk_rows_with_many_chunks_per_block():
         assert np.array_equal(listed[k][0], F2) and np.array_equal(listed[k][1], T2)
     assert _device_status() == 0
     b.close()
+
+
+def test_list_layout_is_the_documented_one():
+    """psc_particle_loads with the three list arrays and list_ready = 0 builds the list the header
+    documents (include/psc_b200.h, psc_geometry): warp w of chunk c owns the entries 32w + l + 256j,
+    numbers its non-zero ones in that order, and entry number n sits in slot
+    c * chunk_entries + (n / 32) * 256 + 32w + n % 32 with the owner weight
+    (count / S^3) / max(alpha_sum, 1e-14) and the packed bbox-local cell; load_n counts each
+    thread's slots.  Rebuilt here from the geometry's own counts and alpha sums, slot by slot."""
+    import ctypes
+
+    import torch
+
+    from particuology_hydraulic_penalty_b200 import _native as nat
+    from particuology_hydraulic_penalty_b200 import windows as wgen
+    from particuology_hydraulic_penalty_b200.engine import DeviceGeometry, LatticeWindow, stream_handle, vp
+
+    dev = torch.device("cuda", 0)
+    n, S = 32, 3
+    shape = (n, n, n)
+    w = wgen.make_window(n, "preloaded", 5)
+    with torch.cuda.device(dev):
+        geo = DeviceGeometry(shape, S, dev, want_level=True)
+        geo.set_particles(w.particles)
+        geo.rebuild()
+        win = LatticeWindow(shape, 0.8, (1e-6, 0.0, 0.0), S, nat.STORE_F32, None, dev)
+        win.bind_geometry(geo)
+        win.step(nat.STEP_IMB | nat.STEP_REDUCE)
+        win.reduce(win.red)
+        g = geo.struct()
+        CE, C, P = int(g.chunk_entries), int(g.capacity_chunks), int(g.nparticles)
+        lw = torch.full((C * CE,), float("nan"), dtype=torch.float64, device=dev)
+        labk = torch.zeros(C * CE, dtype=torch.int32, device=dev)
+        ln = torch.full((C * 256,), 255, dtype=torch.uint8, device=dev)
+        g.load_w, g.load_abk, g.load_n, g.list_ready = lw.data_ptr(), labk.data_ptr(), ln.data_ptr(), 0
+        F = torch.zeros((P, 3), dtype=torch.float64, device=dev)
+        T = torch.zeros((P, 3), dtype=torch.float64, device=dev)
+        D = torch.zeros(nat.NDIAG, dtype=torch.float64, device=dev)
+        nat.call("psc_particle_loads", ctypes.byref(g), 1, vp(win.imb), vp(geo.chunk_partials),
+                 vp(win.red[nat.RED_IMBX:]), vp(F), vp(T), vp(D), stream_handle(dev))
+        torch.cuda.synchronize()
+    cnt = geo.ent_cnt.cpu().numpy().view(np.uint16)
+    alpha = geo.alpha_sum.cpu().numpy()
+    bbox = geo.bbox.cpu().numpy().reshape(-1, 6)
+    ent_off = geo.ent_off.cpu().numpy()
+    chunk_off = geo.chunk_off.cpu().numpy()
+    lw_h, labk_h, ln_h = lw.cpu().numpy(), labk.cpu().numpy().view(np.uint32), ln.cpu().numpy()
+    S3 = np.float64(S ** 3)
+    listed = 0
+    for p in range(P):
+        x0, y0, z0, _, ey, ez = (int(v) for v in bbox[p])
+        for c in range(int(chunk_off[p]), int(chunk_off[p + 1])):
+            e0 = int(ent_off[p]) + (c - int(chunk_off[p])) * CE
+            e1 = min(e0 + CE, int(ent_off[p + 1]))
+            for warp in range(8):
+                mine = [e0 + 32 * warp + lane + 256 * j for j in range(CE // 256) for lane in range(32)]
+                nonzero = [e for e in mine if e < e1 and cnt[e] != 0]
+                for num, e in enumerate(nonzero):
+                    local = e - int(ent_off[p])
+                    a, rem = divmod(local, ey * ez)
+                    b, k = divmod(rem, ez)
+                    cell = ((x0 + a) * n + (y0 + b)) * n + (z0 + k)
+                    ow = (np.float64(cnt[e]) / S3) / max(alpha[cell], 1e-14)
+                    slot = c * CE + (num >> 5) * 256 + 32 * warp + (num & 31)
+                    assert lw_h[slot] == ow and labk_h[slot] == (a | (b << 11) | (k << 22))
+                    listed += 1
+                for lane in range(32):
+                    want = (len(nonzero) - lane + 31) // 32 if len(nonzero) > lane else 0
+                    assert ln_h[c * 256 + 32 * warp + lane] == want
+    assert listed > 1000
+    assert np.abs(F.cpu().numpy()).sum() > 0.0
